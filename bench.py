@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark of the banded pair-HMM path: DP cells/s of the batched FP32 form on the 256-read batch
+(seeded synthetic reads, reference spans ~U(2 kb, 20 kb), 6-mer ACGT Gaussian table, anchors every
+50 positions, diagonal expansion 50, threshold 0.01), with the plain FP64 one-read-per-launch form,
+the CPU oracle and accuracy against the oracle reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  A step is one pass of the hot path over the whole batch: the persistent
+FP32 launch over all 256 reads with inputs resident in HBM (`value`), or the full C-ABI call from
+host buffers (plan, upload, launch, download: `e2e`).  With N > 1 (torchrun) every rank aligns its
+own 256-read batch (weak scaling, no collective on the data path); times are the max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "dp_cells_per_sec"
+UNIT = "cells/s"
+FLOP_PER_CELL = 74.0   # forward + backward + posterior, FP32 form (per band cell)
+WORKLOAD = "256 reads x U(2kb,20kb) spans, 6-mer ACGT Gaussian table, expansion 50, threshold 0.01"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--reads", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--quick", action="store_true", help="skip the CPU baseline and accuracy legs")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def model_and_reads(n_reads, seed):
+    from oracle import formats
+    from signalalign_b200 import synth
+    cfg = synth.config1(seed=seed, n_reads=n_reads)
+    text = synth.model_text(cfg["alphabet"], cfg["k"], cfg["table"])
+    m = formats.parse_model_lines(*text.split("\n")[:3])
+    return cfg, m
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + ",".join(self.FIELDS),
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def time_oracle(m, reads, budget_s, threads):
+    """CPU oracle (FP64 restatement of the reference path) over a bounded sample of the reads, one read
+    per thread; returns (cells/s, cells, seconds, reads used)."""
+    from oracle import oracle as orc
+    p = orc.params(threshold=0.01, expansion=50)
+    oms = [orc.OracleModel(m, orc.EMIT_DESCALED, rd["scale"], rd["shift"], 1.0) for rd in reads]
+    cells = []
+    for rd in reads:
+        L, R = orc.band(rd["anchors"], len(rd["reference"]) - 5, len(rd["events"]), 50)
+        cells.append(int(np.sum((R - L) // 2 + 1)))
+    # the oracle runs ~2-3 M cells/s per thread: size the sample to the budget
+    per_thread = 2.5e6 * budget_s
+    order = np.argsort(cells)
+    chosen, tot = [], 0
+    for i in order:
+        if tot + cells[i] > per_thread * threads and chosen:
+            break
+        chosen.append(int(i))
+        tot += cells[i]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda i: orc.aligned_pairs(oms[i], reads[i]["reference"], reads[i]["events"],
+                                               reads[i]["anchors"], p), chosen))
+    dt = time.perf_counter() - t0
+    return tot / dt, tot, dt, len(chosen)
+
+
+def run_reference(args):
+    """`--impl reference`: the reference path on the host cores.  signalAlign's C sources need the
+    un-vendored sonLib library, so the reference arm is the FP64 CPU restatement (the oracle), which
+    follows the same recursion and reproduces the reference's golden outputs."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    cfg, m = model_and_reads(args.reads, args.seed)
+    threads = os.cpu_count() or 1
+    vals = []
+    for s in range(args.warmup + args.steps):
+        v, cells, dt, nr = time_oracle(m, cfg["reads"], 2.0, threads)
+        if s >= args.warmup:
+            vals.append((v, cells, dt, nr))
+    value = sum(c for _, c, _, _ in vals) / sum(d for _, _, d, _ in vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(d for _, _, d, _ in vals),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "global_batch": args.reads, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "%d reads per step (smallest bands first), one read per thread" % vals[0][3]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from signalalign_b200 import api
+
+    cfg, m = model_and_reads(args.reads, args.seed + 1000 * rank)
+    sm = api.StateMachine.from_tables("ACGT", 6, m["t"], m["match"], m["gapy"], m["gapx"], emission=api.EMIT_DESCALED,
+                                      device=local)
+    p = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=50, threshold=0.01)
+    reads = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                           scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    b = api.Batch(reads, p)
+    b.upload(sptr)
+    cells = b.cells
+    torch.cuda.synchronize()
+    for _ in range(max(3, args.warmup)):
+        b.run(sptr)
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = api.kernel_launch_count()
+    step_ms = []
+    barrier()
+    for _ in range(args.steps):
+        flush.fill_(1)                       # L2 flush between timed steps (outside the events)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.run(sptr)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    barrier()
+    launches = api.kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    t_local = sum(step_ms)
+    t = torch.tensor([t_local], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_max = float(t.item())
+    value = cells * args.steps * world / (t_max / 1e3)
+    reads_per_s = len(reads) * args.steps * world / (t_max / 1e3)
+
+    # e2e: the whole C-ABI call from host buffers (plan + upload + launch + download), wall clock
+    e2e_ms = []
+    h2d = d2h = 0
+    for i in range(max(2, min(args.steps, 3)) + 1):
+        barrier()
+        t0 = time.perf_counter()
+        bb = api.align_batch(reads, p, sptr)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) * 1e3
+        if i > 0:
+            e2e_ms.append(dt)
+        h2d, d2h = bb.transfer_bytes()
+        del bb
+    te = torch.tensor([statistics.mean(e2e_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = cells * world / (float(te.item()) / 1e3)
+
+    line = None
+    if rank == 0:
+        peak = api.measure_fp32_peak(local)
+        kernel_ms = t_max / args.steps
+        achieved = FLOP_PER_CELL * cells / (kernel_ms / 1e3) / 1e12
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", "batch_kernel_traffic.json")
+        if os.path.exists(prof):
+            with open(prof) as fh:
+                pj = json.load(fh)
+            traffic = pj.get("bytes_per_cell", 0) * cells
+        # plain FP64 form, one read per launch, on a sample of the batch
+        order = np.argsort([len(rd["events"]) for rd in cfg["reads"]])
+        sample = [int(i) for i in order[::max(1, len(order) // 8)][:8]]
+        sample_cells = 0
+        for i in sample:
+            rd = cfg["reads"][i]
+            L, R = api.band_construct(rd["anchors"], len(rd["reference"]) - 5, len(rd["events"]), 50)
+            sample_cells += int(np.sum((R - L) // 2 + 1))
+        sm64 = api.StateMachine.from_tables("ACGT", 6, m["t"], m["match"], m["gapy"], m["gapx"],
+                                            emission=api.EMIT_DESCALED, device=local)
+        api.getAlignedPairsUsingAnchors(sm64, cfg["reads"][sample[0]]["reference"][:300],
+                                        cfg["reads"][sample[0]]["events"][:400], [], p)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in sample:
+            rd = cfg["reads"][i]
+            sm64.set_scaling(rd["scale"], rd["shift"], 1.0)
+            api.getAlignedPairsUsingAnchors(sm64, rd["reference"], rd["events"], rd["anchors"], p)
+        plain_s = time.perf_counter() - t0
+        plain_value = sample_cells / plain_s
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": t_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "global_batch": args.reads * world, "regions": b.regions,
+                           "cells_per_step_per_gpu": cells, "parallelism": "dp%d (read sharding)" % world,
+                           "l2": "flushed between timed steps (256 MiB write); forward store >> L2"},
+                "reads_per_sec": reads_per_s,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "ms_per_step": float(te.item()),
+                        "includes": "host planning (bands, windows, k-mer ids), H2D, launch, D2H of all pairs"},
+                "plain_fp64": {"value": plain_value, "unit": UNIT, "sample": "%d reads, one launch per read" % len(sample),
+                               "batched_over_plain": value / world / plain_value},
+                "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                             "frac": achieved / peak, "traffic": traffic,
+                             "note": "%.0f FP32 FLOP per band cell (fwd+bwd+posterior); peak = FMA probe "
+                                     "measured in this run" % FLOP_PER_CELL},
+                "gpu_launches": launches, "clocks": clocks}
+    if world > 1:
+        dist.barrier()
+    if rank == 0 and not args.quick:
+        threads = os.cpu_count() or 1
+        v, ccells, dt, nr = time_oracle(m, cfg["reads"], 4.0, threads)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": "%d reads (%d cells, smallest bands first), one read per thread, %.1f s"
+                                          % (nr, ccells, dt)}
+        # accuracy of the batched FP32 form against the FP64 oracle on 4 reads
+        from oracle import oracle as orc
+        bb = api.align_batch(reads, p, sptr)
+        errs, llerr = [], []
+        for i in [int(j) for j in np.argsort([len(rd["events"]) for rd in cfg["reads"]])[:4]]:
+            rd = cfg["reads"][i]
+            om = orc.OracleModel(m, orc.EMIT_DESCALED, rd["scale"], rd["shift"], 1.0)
+            want, tps = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"],
+                                          orc.params(threshold=0.01, expansion=50), with_total_probs=True)
+            got = bb.pairs(i)
+            ma = {(int(r["x"]), int(r["y"])): r["score"] / 1e7 for r in want}
+            mg = {(int(r["x"]), int(r["y"])): r["score"] / 1e7 for r in got}
+            e = 0.0
+            for k in set(ma) | set(mg):
+                e = max(e, abs(ma.get(k, 0.0) - mg.get(k, 0.0)) if (k in ma and k in mg)
+                        else (ma.get(k) or mg.get(k)) - 0.01)
+            errs.append(e)
+            top = [v2 for d, v2 in tps if d == len(rd["reference"]) - 5 + len(rd["events"])]
+            if top:
+                llerr.append(abs(bb.log_likelihood(i) - top[0]))
+        line["accuracy"] = {"max_posterior_err": max(errs), "max_loglik_abs_err": max(llerr) if llerr else None,
+                            "reads": 4, "vs": "FP64 CPU oracle"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,237 @@
+/*
+ * sa_b200.h -- C ABI of the B200 banded pair-HMM engine (signalAlign's signal-to-reference
+ * posterior alignment).  Plain C types only: pointers, sizes, int64/double.  All entry points
+ * return an sa_status (0 = SA_OK) and never abort the process.
+ *
+ * Each declaration names the signalAlign routine it replaces (file:line in the signalAlign tree).
+ */
+#ifndef SA_B200_H_
+#define SA_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference aborts through st_errAbort / assert instead) ---- */
+typedef enum {
+    SA_OK = 0,
+    SA_E_ARG = 1,            /* bad argument (NULL pointer, negative length, bad parameters)            */
+    SA_E_ALPHABET = 2,       /* k-mer character outside the model alphabet (kmer_to_word exit,
+                                nanopore_hdp.c:375-388)                                                  */
+    SA_E_ANCHORS = 3,        /* anchors not strictly increasing / outside the matrix (band_construct
+                                asserts, pairwiseAligner.c:160-167; getSplitPoints asserts :1743-1746)  */
+    SA_E_NOMEM = 4,          /* host or device allocation failed                                        */
+    SA_E_CUDA = 5,           /* CUDA runtime error                                                      */
+    SA_E_OUTPUT = 6,         /* pair output buffer too small (re-run with a larger capacity)            */
+    SA_E_UNSUPPORTED = 7,    /* combination this engine does not run (e.g. 5-state machines)            */
+    SA_E_FILE = 8,           /* .model / .nhdp file missing or malformed (stateMachine.c:1339-1426,
+                                hdp.c:3047-3316)                                                         */
+    SA_E_TIMEOUT = 9,        /* a bounded device-side wait gave up                                      */
+    SA_E_DEVICE = 10,        /* device-side consistency check failed                                    */
+    SA_E_CAPACITY = 11       /* request larger than a fixed capacity of the entry point                 */
+} sa_status;
+
+/* ---- state machine (StateMachine / StateMachine3 / StateMachine3_HDP, inc/stateMachine.h:76-182) ---- */
+typedef enum {
+    SA_THREE_STATE = 2,      /* StateMachineType threeState (inc/stateMachine.h:30)                      */
+    SA_THREE_STATE_HDP = 7   /* StateMachineType threeStateHdp (inc/stateMachine.h:35)                   */
+} sa_machine_type;
+
+typedef enum {
+    SA_EMIT_PLAIN = 0,       /* emissions_signal_strawManGetKmerEventMatchProb (stateMachine.c:547-589),
+                                used by getStateMachine3 (stateMachine.c:1645-1653)                      */
+    SA_EMIT_DESCALED = 1,    /* ..._strawManGetKmerEventMatchProbWithDescaling (stateMachine.c:498-545),
+                                used by getStateMachine3_descaled (stateMachine.c:1627-1643)             */
+    SA_EMIT_HDP = 2          /* emissions_signal_getHdpKmerDensity (stateMachine.c:468-495), used by
+                                getHdpStateMachine (stateMachine.c:1655-1669)                            */
+} sa_emission;
+
+/* transition slots in log space, StateMachine3 field order (inc/stateMachine.h:153-163) */
+enum {
+    SA_T_MATCH_CONTINUE = 0, SA_T_MATCH_FROM_GAP_X, SA_T_MATCH_FROM_GAP_Y, SA_T_GAP_OPEN_X,
+    SA_T_GAP_OPEN_Y, SA_T_GAP_EXTEND_X, SA_T_GAP_EXTEND_Y, SA_T_GAP_SWITCH_TO_X, SA_T_GAP_SWITCH_TO_Y,
+    SA_N_TRANSITIONS
+};
+
+/* DegenerateType (inc/pairwiseAligner.h:50-56): which bases an 'X' in the reference may be */
+typedef enum {
+    SA_CYTOSINE_METHYLATION2 = 0,   /* "CE"   */
+    SA_CYTOSINE_METHYLATION3 = 1,   /* "CEO"  */
+    SA_ADENOSINE_METHYLATION = 2,   /* "AI"   */
+    SA_CANONICAL_VARIANTS = 3       /* "ACGT" */
+} sa_degenerate;
+
+typedef struct sa_state_machine sa_state_machine;   /* opaque; its tables live on the device */
+
+/* stateMachine3_loadFromFile (stateMachine.c:1328-1426) + getStateMachine3 / getStateMachine3_descaled /
+ * getHdpStateMachine (stateMachine.c:1627-1669).  For SA_THREE_STATE_HDP, nhdp_file is read as by
+ * deserialize_nhdp (nanopore_hdp.c:1071-1098); set_hdp_expected_values applies
+ * stateMachine3_setModelToHdpExpectedValues (stateMachine.c:1163-1192), as signalMachine does
+ * (signalMachine.c:709-711).  `device` is the CUDA device that holds the tables. */
+sa_status sa_stateMachine_loadFromFile(const char *model_file, sa_machine_type type, sa_emission emission,
+                                       const char *nhdp_file, int32_t set_hdp_expected_values, int32_t device,
+                                       sa_state_machine **out);
+
+/* Same state machine from in-memory tables.  match/gap_y: n_kmers x 5 doubles (level_mean, level_sd,
+ * noise_mean, noise_sd, noise_lambda) in k-mer-id order; gap_y's level_sd already multiplied by
+ * EXTRA_EVENT_NOISE_MULTIPLIER as the loader does (stateMachine.c:1418-1420); gap_x: n_kmers log
+ * probabilities (log 0.1 in the reference, stateMachine.c:1472-1474). */
+sa_status sa_stateMachine_fromTables(sa_machine_type type, sa_emission emission, const char *alphabet,
+                                     int32_t alphabet_size, int32_t kmer_length,
+                                     const double transitions[SA_N_TRANSITIONS], const double *match,
+                                     const double *gap_y, const double *gap_x, int32_t device,
+                                     sa_state_machine **out);
+
+/* HDP posterior-predictive tables (dir_proc_density, hdp.c:2583-2607): a uniform grid
+ * linspace(grid_start, grid_stop, grid_length) (hdp_math_utils.c:497-509), n_rows rows of density
+ * and knot slopes, and per k-mer the row of its nearest observed ancestor (-1: none). */
+sa_status sa_stateMachine_setHdp(sa_state_machine *sm, double grid_start, double grid_stop,
+                                 int64_t grid_length, int64_t n_rows, const double *density,
+                                 const double *slope, const int64_t *kmer_row);
+
+/* scale/shift/var of the StateMachine (inc/stateMachine.h:82-84, set at stateMachine.c:1633-1635). */
+sa_status sa_stateMachine_setScaling(sa_state_machine *sm, double scale, double shift, double var);
+
+/* emissions_signal_scaleModel (stateMachine.c:630-668) and emissions_signal_scaleNoise
+ * (stateMachine.c:607-628), applied to the state machine's tables in place. */
+sa_status sa_stateMachine_scaleModel(sa_state_machine *sm, double scale, double shift, double var,
+                                     double scale_sd, double var_sd);
+sa_status sa_stateMachine_scaleNoise(sa_state_machine *sm, double scale_sd, double var_sd);
+
+/* model facts and the interned, process-lifetime path k-mer string of a k-mer id (the reference puts
+ * the path's char* into element 3 of each aligned pair, pairwiseAligner.c:1239-1241). */
+int32_t sa_stateMachine_kmerLength(const sa_state_machine *sm);
+int64_t sa_stateMachine_numberOfKmers(const sa_state_machine *sm);
+const char *sa_stateMachine_kmerString(const sa_state_machine *sm, int64_t kmer_id);
+
+/* kmer_id (nanopore_hdp.c:388-393) over the state machine's sorted alphabet; -1 if a character is
+ * outside it. */
+int64_t sa_stateMachine_kmerId(const sa_state_machine *sm, const char *kmer);
+
+/* the model's tables back on the host (for checking a load): match/gap_y n x 5, gap_x n, t[9] */
+sa_status sa_stateMachine_getTables(const sa_state_machine *sm, double *match, double *gap_y, double *gap_x,
+                                    double *transitions);
+
+void sa_stateMachine_destruct(sa_state_machine *sm);
+
+/* ---- alignment parameters (PairwiseAlignmentParameters, inc/pairwiseAligner.h:123-134) ---- */
+typedef struct {
+    double threshold;                     /* posterior threshold, default 0.01 */
+    int64_t min_diags_between_traceback;  /* default 1000 */
+    int64_t traceback_diagonals;          /* default 40   */
+    int64_t diagonal_expansion;           /* default 20 in the library, 50 in signalMachine */
+    int64_t constraint_diagonal_trim;     /* default 14 (anchor preparation only) */
+    int64_t split_matrix_bigger_than_this;/* default 3000*3000 */
+} sa_params;
+
+/* pairwiseAlignmentBandingParameters_construct (pairwiseAligner.c:1843-1856) */
+void sa_params_default(sa_params *p);
+
+/* ---- one aligned pair: stIntTuple(4) of getAlignedPairsUsingAnchors (pairwiseAligner.c:1237-1241) ---- */
+typedef struct {
+    int64_t score;   /* floor(posterior * 10^7)  (PAIR_ALIGNMENT_PROB_1, inc/pairwiseAligner.h:27) */
+    int64_t x;       /* reference k-mer index */
+    int64_t y;       /* event index */
+    int64_t kmer;    /* path k-mer id; sa_stateMachine_kmerString gives its string */
+} sa_aligned_pair;
+
+/* ---- band geometry and split points (host, bit-exact with the reference) ---- */
+
+/* band_construct (pairwiseAligner.c:131-182): xmyL/xmyR of every anti-diagonal xay = 0..lX+lY.
+ * anchors: n_anchors (x, y) pairs in k-mer / event coordinates, strictly increasing. */
+sa_status sa_band_construct(const int64_t *anchors, int64_t n_anchors, int64_t lX, int64_t lY, int64_t expansion,
+                            int64_t *xmy_l, int64_t *xmy_r);
+
+/* getSplitPoints (pairwiseAligner.c:1730-1757): writes up to max_regions (x1, y1, x2, y2) tuples and
+ * their count. */
+sa_status sa_getSplitPoints(const int64_t *anchors, int64_t n_anchors, int64_t lX, int64_t lY,
+                            int64_t split_matrix_bigger_than_this, int32_t ragged_left, int32_t ragged_right,
+                            int64_t *regions, int64_t max_regions, int64_t *n_regions);
+
+/* ---- plain FP64 form: one read per launch ---- */
+
+/* getAlignedPairsUsingAnchors(sM, sX, sY, anchorPairs, p, diagonalCalculationPosteriorMatchProbs,
+ * raggedLeft, raggedRight) (pairwiseAligner.c:1871-1899), which splits at large anchor gaps
+ * (:1773-1837) and runs getPosteriorProbsWithBanding (:1282-1420) on each region.
+ *   reference: nucleotide string of reference_length chars (lX = reference_length - (k-1) k-mers),
+ *              'X' expands to the bases of `degenerate` (hdCell_construct, :605-650);
+ *   events: n_events x 4 doubles (mean, noise, duration, start; NB_EVENT_PARAMS, inc/nanopore.h:4);
+ *   anchors: n_anchors (x, y) pairs.
+ * The pairs come back in the reference's emission order.  *pairs is allocated with malloc; free it
+ * with sa_free_pairs.  Optional: log_likelihood receives the total probability of the last region's
+ * final refresh (the normaliser of its last posteriors). */
+sa_status sa_getAlignedPairsUsingAnchors(const sa_state_machine *sm, const char *reference,
+                                         int64_t reference_length, sa_degenerate degenerate,
+                                         const double *events, int64_t n_events, const int64_t *anchors,
+                                         int64_t n_anchors, const sa_params *p, int32_t ragged_left,
+                                         int32_t ragged_right, sa_aligned_pair **pairs, int64_t *n_pairs,
+                                         double *log_likelihood);
+
+void sa_free_pairs(sa_aligned_pair *pairs);
+
+/* ---- batched FP32 form: many reads, one persistent launch ---- */
+
+/* One read of a batch: the inputs of signalMachine's performSignalAlignment (signalMachine.c:333-354)
+ * after anchor remapping, plus the read's NanoporeReadAdjustmentParameters (inc/nanopore.h:11-19). */
+typedef struct {
+    const sa_state_machine *sm;   /* model; emission kind and tables come from it */
+    const char *reference;        /* nucleotide string */
+    int64_t reference_length;
+    const double *events;         /* n_events x 4 doubles */
+    int64_t n_events;
+    const int64_t *anchors;       /* n_anchors x (x, y) */
+    int64_t n_anchors;
+    double scale, shift, var;     /* used by SA_EMIT_DESCALED / SA_EMIT_HDP (descaleEventMean_JordanStyle) */
+    int32_t ragged_left, ragged_right;
+    int32_t degenerate;           /* sa_degenerate */
+    int32_t pad;
+} sa_read;
+
+typedef struct sa_batch sa_batch;   /* opaque: packed inputs, device buffers, results */
+
+/* Host-side planning of a batch: band geometry, traceback windows, k-mer ids, packing; allocates the
+ * batch's device buffers on the state machines' device.  The reads' arrays are copied; the caller
+ * may free them after this returns. */
+sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch **out);
+
+/* host -> device copy of the packed inputs on `stream` (a cudaStream_t, NULL = default stream) */
+sa_status sa_batch_upload(sa_batch *b, void *stream);
+
+/* the alignment itself on `stream`: one persistent FP32 launch over all regions (inputs resident) */
+sa_status sa_batch_run(sa_batch *b, void *stream);
+
+/* device -> host copy of pair counts, pairs and per-read status; synchronises `stream` */
+sa_status sa_batch_download(sa_batch *b, void *stream);
+
+/* all of the above in one call */
+sa_status sa_align_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, void *stream,
+                         sa_batch **out);
+
+/* results after download: per read status, pair count and pairs (reference emission order) */
+sa_status sa_batch_read_status(const sa_batch *b, int64_t read);
+int64_t sa_batch_pair_count(const sa_batch *b, int64_t read);
+const sa_aligned_pair *sa_batch_pairs(const sa_batch *b, int64_t read);
+/* the total probability of each read's last refresh (log-likelihood of its final window) */
+double sa_batch_log_likelihood(const sa_batch *b, int64_t read);
+/* batch facts: DP cells (sum of band widths over all regions) and regions */
+int64_t sa_batch_cells(const sa_batch *b);
+/* bytes the batch moves host->device on upload and device->host on download (after a download) */
+sa_status sa_batch_transfer_bytes(const sa_batch *b, int64_t *h2d, int64_t *d2h);
+int64_t sa_batch_regions(const sa_batch *b);
+void sa_batch_destroy(sa_batch *b);
+
+/* ---- diagnostics ---- */
+const char *sa_status_string(sa_status s);
+/* number of kernel launches this process has made through the library (all entry points) */
+int64_t sa_kernel_launch_count(void);
+/* FP32 FMA issue rate of `device` in TFLOP/s, measured by a short probe kernel (the denominator of
+ * the engine's compute roofline; no counterpart in signalAlign) */
+sa_status sa_measure_fp32_peak(int32_t device, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SA_B200_H_ */

@@ -1,0 +1,403 @@
+"""Python mirror of signalAlign's alignment interface over the C ABI of libsa_b200.so.
+
+Names follow the reference (getStateMachine3, getStateMachine3_descaled, getHdpStateMachine,
+pairwiseAlignmentBandingParameters_construct, band_construct, getSplitPoints,
+getAlignedPairsUsingAnchors); errors that the reference turns into an abort raise SAError here.
+There is no CPU fallback: every alignment runs on the GPU through the library, and importing this
+module fails if the library has not been built.
+"""
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsa_b200.so")
+
+THREE_STATE, THREE_STATE_HDP = 2, 7
+EMIT_PLAIN, EMIT_DESCALED, EMIT_HDP = 0, 1, 2
+CYTOSINE_METHYLATION2, CYTOSINE_METHYLATION3, ADENOSINE_METHYLATION, CANONICAL_VARIANTS = 0, 1, 2, 3
+PAIR_ALIGNMENT_PROB_1 = 10000000
+
+STATUS = {0: "ok", 1: "bad argument", 2: "k-mer character outside the model alphabet",
+          3: "anchors not strictly increasing or outside the matrix", 4: "out of memory", 5: "CUDA error",
+          6: "pair output buffer too small", 7: "unsupported state machine or input",
+          8: "model file missing or malformed", 9: "device wait timed out", 10: "device consistency check failed",
+          11: "request exceeds a fixed capacity"}
+
+
+class SAError(RuntimeError):
+    def __init__(self, status, where=""):
+        self.status = int(status)
+        super().__init__("%s: %s (status %d)" % (where, STATUS.get(self.status, "unknown"), self.status))
+
+
+class Params(C.Structure):
+    _fields_ = [("threshold", C.c_double), ("min_diags_between_traceback", C.c_int64),
+                ("traceback_diagonals", C.c_int64), ("diagonal_expansion", C.c_int64),
+                ("constraint_diagonal_trim", C.c_int64), ("split_matrix_bigger_than_this", C.c_int64)]
+
+
+class AlignedPair(C.Structure):
+    _fields_ = [("score", C.c_int64), ("x", C.c_int64), ("y", C.c_int64), ("kmer", C.c_int64)]
+
+
+PAIR_DTYPE = np.dtype([("score", np.int64), ("x", np.int64), ("y", np.int64), ("kmer", np.int64)])
+
+
+class Read(C.Structure):
+    _fields_ = [("sm", C.c_void_p), ("reference", C.c_char_p), ("reference_length", C.c_int64),
+                ("events", C.POINTER(C.c_double)), ("n_events", C.c_int64),
+                ("anchors", C.POINTER(C.c_int64)), ("n_anchors", C.c_int64),
+                ("scale", C.c_double), ("shift", C.c_double), ("var", C.c_double),
+                ("ragged_left", C.c_int32), ("ragged_right", C.c_int32), ("degenerate", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+_lib = None
+_i64p = C.POINTER(C.c_int64)
+_f64p = C.POINTER(C.c_double)
+
+
+def _bind(L):
+    vp = C.c_void_p
+    sig = {
+        "sa_stateMachine_loadFromFile": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int32, C.c_int32,
+                                                   C.POINTER(vp)]),
+        "sa_stateMachine_fromTables": (C.c_int, [C.c_int, C.c_int, C.c_char_p, C.c_int32, C.c_int32, _f64p, _f64p,
+                                                 _f64p, _f64p, C.c_int32, C.POINTER(vp)]),
+        "sa_stateMachine_setHdp": (C.c_int, [vp, C.c_double, C.c_double, C.c_int64, C.c_int64, _f64p, _f64p, _i64p]),
+        "sa_stateMachine_setScaling": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
+        "sa_stateMachine_scaleModel": (C.c_int, [vp] + [C.c_double] * 5),
+        "sa_stateMachine_scaleNoise": (C.c_int, [vp, C.c_double, C.c_double]),
+        "sa_stateMachine_kmerLength": (C.c_int32, [vp]),
+        "sa_stateMachine_numberOfKmers": (C.c_int64, [vp]),
+        "sa_stateMachine_kmerString": (C.c_char_p, [vp, C.c_int64]),
+        "sa_stateMachine_kmerId": (C.c_int64, [vp, C.c_char_p]),
+        "sa_stateMachine_getTables": (C.c_int, [vp, _f64p, _f64p, _f64p, _f64p]),
+        "sa_stateMachine_destruct": (None, [vp]),
+        "sa_params_default": (None, [C.POINTER(Params)]),
+        "sa_band_construct": (C.c_int, [_i64p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _i64p, _i64p]),
+        "sa_getSplitPoints": (C.c_int, [_i64p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
+                                        _i64p, C.c_int64, _i64p]),
+        "sa_getAlignedPairsUsingAnchors": (C.c_int, [vp, C.c_char_p, C.c_int64, C.c_int, _f64p, C.c_int64, _i64p,
+                                                     C.c_int64, C.POINTER(Params), C.c_int32, C.c_int32,
+                                                     C.POINTER(C.POINTER(AlignedPair)), _i64p, _f64p]),
+        "sa_free_pairs": (None, [vp]),
+        "sa_batch_create": (C.c_int, [C.POINTER(Read), C.c_int64, C.POINTER(Params), C.POINTER(vp)]),
+        "sa_batch_upload": (C.c_int, [vp, vp]),
+        "sa_batch_run": (C.c_int, [vp, vp]),
+        "sa_batch_download": (C.c_int, [vp, vp]),
+        "sa_align_batch": (C.c_int, [C.POINTER(Read), C.c_int64, C.POINTER(Params), vp, C.POINTER(vp)]),
+        "sa_batch_read_status": (C.c_int, [vp, C.c_int64]),
+        "sa_batch_pair_count": (C.c_int64, [vp, C.c_int64]),
+        "sa_batch_pairs": (C.POINTER(AlignedPair), [vp, C.c_int64]),
+        "sa_batch_log_likelihood": (C.c_double, [vp, C.c_int64]),
+        "sa_batch_cells": (C.c_int64, [vp]),
+        "sa_batch_regions": (C.c_int64, [vp]),
+        "sa_batch_transfer_bytes": (C.c_int, [vp, _i64p, _i64p]),
+        "sa_batch_destroy": (None, [vp]),
+        "sa_status_string": (C.c_char_p, [C.c_int]),
+        "sa_kernel_launch_count": (C.c_int64, []),
+        "sa_measure_fp32_peak": (C.c_int, [C.c_int32, _f64p]),
+    }
+    for name, (res, args) in sig.items():
+        if not hasattr(L, name):
+            continue
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+def lib():
+    """The loaded C-ABI library.  Raises if it was not built: there is no fallback path."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libsa_b200.so is not built (run `python -m signalalign_b200.build` or "
+                              "__graft_entry__.build())")
+        _lib = _bind(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def _check(st, where):
+    if st:
+        raise SAError(st, where)
+
+
+def _f64(a, cols=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    if cols is not None:
+        a = a.reshape(-1, cols)
+    return a
+
+
+def _anchors(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int64).reshape(-1, 2))
+
+
+def pairwiseAlignmentBandingParameters_construct(**overrides):
+    """pairwiseAlignmentBandingParameters_construct (pairwiseAligner.c:1843-1856)."""
+    p = Params()
+    lib().sa_params_default(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+class StateMachine:
+    """A 3-state signal state machine whose emission tables live on the GPU."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.sa_stateMachine_destruct(self._h)
+            self._h = C.c_void_p(0)
+
+    @classmethod
+    def load(cls, model_file, machine_type=THREE_STATE, emission=EMIT_DESCALED, nhdp_file=None,
+             set_hdp_expected_values=True, device=0):
+        h = C.c_void_p()
+        st = lib().sa_stateMachine_loadFromFile(model_file.encode(), machine_type, emission,
+                                                nhdp_file.encode() if nhdp_file else None,
+                                                int(set_hdp_expected_values), device, C.byref(h))
+        _check(st, "stateMachine3_loadFromFile(%s)" % model_file)
+        return cls(h.value)
+
+    @classmethod
+    def from_tables(cls, alphabet, kmer_length, transitions, match, gap_y, gap_x, emission=EMIT_DESCALED,
+                    device=0):
+        machine_type = THREE_STATE_HDP if emission == EMIT_HDP else THREE_STATE
+        t = _f64(transitions)
+        m, y, x = _f64(match, 5), _f64(gap_y, 5), _f64(gap_x)
+        h = C.c_void_p()
+        st = lib().sa_stateMachine_fromTables(machine_type, emission, alphabet.encode(), len(alphabet), kmer_length,
+                                              t.ctypes.data_as(_f64p), m.ctypes.data_as(_f64p),
+                                              y.ctypes.data_as(_f64p), x.ctypes.data_as(_f64p), device, C.byref(h))
+        _check(st, "stateMachine_fromTables")
+        return cls(h.value)
+
+    def set_hdp(self, grid_start, grid_stop, grid_length, density, slope, kmer_row):
+        d, s = _f64(density, grid_length), _f64(slope, grid_length)
+        r = np.ascontiguousarray(np.asarray(kmer_row, dtype=np.int64))
+        st = lib().sa_stateMachine_setHdp(self._h, grid_start, grid_stop, grid_length, len(d),
+                                          d.ctypes.data_as(_f64p), s.ctypes.data_as(_f64p), r.ctypes.data_as(_i64p))
+        _check(st, "stateMachine_setHdp")
+
+    def set_scaling(self, scale, shift, var):
+        _check(lib().sa_stateMachine_setScaling(self._h, scale, shift, var), "stateMachine_setScaling")
+
+    def scaleModel(self, scale, shift, var, scale_sd, var_sd):
+        _check(lib().sa_stateMachine_scaleModel(self._h, scale, shift, var, scale_sd, var_sd), "scaleModel")
+
+    def scaleNoise(self, scale_sd, var_sd):
+        _check(lib().sa_stateMachine_scaleNoise(self._h, scale_sd, var_sd), "scaleNoise")
+
+    @property
+    def kmer_length(self):
+        return lib().sa_stateMachine_kmerLength(self._h)
+
+    @property
+    def n_kmers(self):
+        return lib().sa_stateMachine_numberOfKmers(self._h)
+
+    def kmer_string(self, kmer_id):
+        s = lib().sa_stateMachine_kmerString(self._h, int(kmer_id))
+        return s.decode() if s is not None else None
+
+    def kmer_id(self, kmer):
+        return lib().sa_stateMachine_kmerId(self._h, kmer.encode())
+
+    def tables(self):
+        n = self.n_kmers
+        m, y, x, t = np.zeros((n, 5)), np.zeros((n, 5)), np.zeros(n), np.zeros(9)
+        _check(lib().sa_stateMachine_getTables(self._h, m.ctypes.data_as(_f64p), y.ctypes.data_as(_f64p),
+                                               x.ctypes.data_as(_f64p), t.ctypes.data_as(_f64p)), "getTables")
+        return dict(match=m, gapy=y, gapx=x, t=t)
+
+
+def getStateMachine3(model_file, device=0):
+    """getStateMachine3 (stateMachine.c:1645-1653): plain (not descaled) emissions."""
+    return StateMachine.load(model_file, THREE_STATE, EMIT_PLAIN, device=device)
+
+
+def getStateMachine3_descaled(model_file, scale, shift, var, scale_sd=1.0, var_sd=1.0, scale_noise=False, device=0):
+    """getStateMachine3_descaled (stateMachine.c:1627-1643)."""
+    sm = StateMachine.load(model_file, THREE_STATE, EMIT_DESCALED, device=device)
+    sm.set_scaling(scale, shift, var)
+    if scale_noise:
+        sm.scaleNoise(scale_sd, var_sd)
+    return sm
+
+
+def getHdpStateMachine(nhdp_file, model_file, scale, shift, var, set_expected_values=True, device=0):
+    """getHdpStateMachine (stateMachine.c:1655-1669), optionally followed by
+    stateMachine3_setModelToHdpExpectedValues as signalMachine does (signalMachine.c:709-711)."""
+    sm = StateMachine.load(model_file, THREE_STATE_HDP, EMIT_HDP, nhdp_file=nhdp_file,
+                           set_hdp_expected_values=set_expected_values, device=device)
+    sm.set_scaling(scale, shift, var)
+    return sm
+
+
+def band_construct(anchors, lX, lY, expansion):
+    """band_construct (pairwiseAligner.c:131-182): (xmyL, xmyR) for xay = 0..lX+lY."""
+    a = _anchors(anchors)
+    L, R = np.zeros(lX + lY + 1, np.int64), np.zeros(lX + lY + 1, np.int64)
+    _check(lib().sa_band_construct(a.ctypes.data_as(_i64p), len(a), lX, lY, expansion, L.ctypes.data_as(_i64p),
+                                   R.ctypes.data_as(_i64p)), "band_construct")
+    return L, R
+
+
+def getSplitPoints(anchors, lX, lY, split_matrix_bigger_than_this, ragged_left, ragged_right):
+    """getSplitPoints (pairwiseAligner.c:1730-1757): list of (x1, y1, x2, y2)."""
+    a = _anchors(anchors)
+    cap = len(a) + 2
+    out = np.zeros((cap, 4), np.int64)
+    n = C.c_int64(0)
+    _check(lib().sa_getSplitPoints(a.ctypes.data_as(_i64p), len(a), lX, lY, split_matrix_bigger_than_this,
+                                   int(ragged_left), int(ragged_right), out.ctypes.data_as(_i64p), cap, C.byref(n)),
+           "getSplitPoints")
+    return [tuple(int(v) for v in r) for r in out[:n.value]]
+
+
+def getAlignedPairsUsingAnchors(sm, reference, events, anchors, p, ragged_left=True, ragged_right=True,
+                                degenerate=CYTOSINE_METHYLATION3, as_tuples=False, with_log_likelihood=False):
+    """getAlignedPairsUsingAnchors (pairwiseAligner.c:1871-1899) on the plain FP64 GPU form.
+
+    Returns a structured array (score, x, y, kmer id) in the reference's emission order, or a list
+    of (score, x, y, path k-mer string) tuples like the reference's stIntTuple list."""
+    ev = _f64(events, 4)
+    a = _anchors(anchors)
+    out = C.POINTER(AlignedPair)()
+    n = C.c_int64(0)
+    ll = C.c_double(0)
+    ref = reference.encode()
+    st = lib().sa_getAlignedPairsUsingAnchors(sm.handle, ref, len(ref), degenerate, ev.ctypes.data_as(_f64p), len(ev),
+                                              a.ctypes.data_as(_i64p), len(a), C.byref(p), int(ragged_left),
+                                              int(ragged_right), C.byref(out), C.byref(n), C.byref(ll))
+    _check(st, "getAlignedPairsUsingAnchors")
+    try:
+        arr = np.ctypeslib.as_array(C.cast(out, C.POINTER(C.c_int64)), shape=(n.value * 4,)).copy() \
+            if n.value else np.zeros(0, np.int64)
+    finally:
+        lib().sa_free_pairs(C.cast(out, C.c_void_p))
+    pairs = arr.view(PAIR_DTYPE).reshape(-1)
+    if as_tuples:
+        pairs = [(int(r["score"]), int(r["x"]), int(r["y"]), sm.kmer_string(r["kmer"])) for r in pairs]
+    if with_log_likelihood:
+        return pairs, ll.value
+    return pairs
+
+
+@dataclass
+class ReadInput:
+    """One read of a batch (the inputs of performSignalAlignment, signalMachine.c:333-354)."""
+    sm: StateMachine
+    reference: str
+    events: np.ndarray
+    anchors: np.ndarray
+    scale: float = 1.0
+    shift: float = 0.0
+    var: float = 1.0
+    ragged_left: bool = True
+    ragged_right: bool = True
+    degenerate: int = CYTOSINE_METHYLATION3
+
+
+class Batch:
+    """A planned batch on the device: upload / run / download, or all at once with align()."""
+
+    def __init__(self, reads, p):
+        self._keep = []
+        arr = (Read * len(reads))()
+        for i, r in enumerate(reads):
+            ev = _f64(r.events, 4)
+            a = _anchors(r.anchors)
+            ref = r.reference.encode()
+            self._keep += [ev, a, ref]
+            arr[i].sm = r.sm.handle.value
+            arr[i].reference = ref
+            arr[i].reference_length = len(ref)
+            arr[i].events = ev.ctypes.data_as(_f64p)
+            arr[i].n_events = len(ev)
+            arr[i].anchors = a.ctypes.data_as(_i64p)
+            arr[i].n_anchors = len(a)
+            arr[i].scale, arr[i].shift, arr[i].var = r.scale, r.shift, r.var
+            arr[i].ragged_left, arr[i].ragged_right = int(r.ragged_left), int(r.ragged_right)
+            arr[i].degenerate = r.degenerate
+        self._reads = arr
+        self.n = len(reads)
+        self._sms = [r.sm for r in reads]
+        h = C.c_void_p()
+        _check(lib().sa_batch_create(arr, len(reads), C.byref(p), C.byref(h)), "batch_create")
+        self._h = h
+        self._keep = []   # the library copied the inputs
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.sa_batch_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def upload(self, stream=None):
+        _check(lib().sa_batch_upload(self._h, stream), "batch_upload")
+
+    def run(self, stream=None):
+        _check(lib().sa_batch_run(self._h, stream), "batch_run")
+
+    def download(self, stream=None):
+        _check(lib().sa_batch_download(self._h, stream), "batch_download")
+
+    @property
+    def cells(self):
+        return lib().sa_batch_cells(self._h)
+
+    @property
+    def regions(self):
+        return lib().sa_batch_regions(self._h)
+
+    def transfer_bytes(self):
+        h, d = C.c_int64(0), C.c_int64(0)
+        _check(lib().sa_batch_transfer_bytes(self._h, C.byref(h), C.byref(d)), "batch_transfer_bytes")
+        return h.value, d.value
+
+    def status(self, i):
+        return lib().sa_batch_read_status(self._h, i)
+
+    def log_likelihood(self, i):
+        return lib().sa_batch_log_likelihood(self._h, i)
+
+    def pairs(self, i):
+        n = lib().sa_batch_pair_count(self._h, i)
+        if n <= 0:
+            return np.zeros(0, PAIR_DTYPE)
+        ptr = lib().sa_batch_pairs(self._h, i)
+        arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_int64)), shape=(n * 4,)).copy()
+        return arr.view(PAIR_DTYPE).reshape(-1)
+
+
+def align_batch(reads, p, stream=None):
+    """Batched FP32 form: plan, upload, one persistent launch, download."""
+    b = Batch(reads, p)
+    b.upload(stream)
+    b.run(stream)
+    b.download(stream)
+    return b
+
+
+def kernel_launch_count():
+    return lib().sa_kernel_launch_count()
+
+
+def measure_fp32_peak(device=0):
+    """FP32 FMA issue rate of the device in TFLOP/s (probe kernel)."""
+    v = C.c_double(0)
+    _check(lib().sa_measure_fp32_peak(device, C.byref(v)), "measure_fp32_peak")
+    return v.value

@@ -1,0 +1,136 @@
+// Internal declarations shared by the host planner (sa_host.cpp) and the CUDA kernels
+// (sa_fp64.cu, sa_fp32.cu).  Nothing here is part of the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "sa_b200.h"
+
+namespace sa {
+
+constexpr int kEventParams = 4;                 // NB_EVENT_PARAMS (inc/nanopore.h:4)
+constexpr double kPairProb1 = 10000000.0;       // PAIR_ALIGNMENT_PROB_1 (inc/pairwiseAligner.h:27)
+constexpr double kLogPointOne = -2.3025850929940455;  // gap-X emission, stateMachine.c:1282, :1472-1474
+constexpr int kMaxK = 12;
+
+// ----------------------------------------------------------------------------------------------
+// state machine: host copy of the reference tables, device copies for both kernel forms
+// ----------------------------------------------------------------------------------------------
+struct HdpTables {
+    bool present = false;
+    double grid_start = 0, grid_stop = 0;
+    int64_t grid_length = 0;
+    int64_t n_rows = 0;
+    std::vector<double> grid;       // linspace (hdp_math_utils.c:497-509)
+    std::vector<double> density;    // n_rows x grid_length
+    std::vector<double> slope;      // n_rows x grid_length
+    std::vector<int64_t> kmer_row;  // n_kmers
+    std::vector<char> kmer_observed;  // n_kmers: the k-mer's own DP is observed (hdp_check_for_observed)
+};
+
+// FP32 per-k-mer emission constants (one 32-byte record per k-mer), derived on the host in FP64
+// from the reference tables:
+//   mu, 1/sd_match, 1/sd_gapy, k_m = -log(2 pi) - log(sd_match) + 0.5 log(lambda),
+//   k_y = -log(2 pi) - log(sd_gapy) + 0.5 log(lambda), 1/noise_mean, lambda/2
+struct __align__(16) KmerConst32 {
+    float mu, inv_sd_m, inv_sd_y, k_m;
+    float k_y, inv_nu, half_lambda, pad;
+};
+
+struct DeviceModel {
+    int device = 0;
+    // FP64 tables (reference layout)
+    double *match = nullptr, *gapy = nullptr, *gapx = nullptr;
+    double *hdp_grid = nullptr, *hdp_density = nullptr, *hdp_slope = nullptr;
+    int64_t *hdp_kmer_row = nullptr;
+    // FP32 tables
+    KmerConst32 *kc32 = nullptr;
+    float *gapx32 = nullptr;
+    float2 *hdp_knots32 = nullptr;   // n_rows x grid_length (density, slope)
+    int32_t *hdp_row32 = nullptr;
+};
+
+}  // namespace sa
+
+struct sa_state_machine {
+    sa_machine_type type;
+    sa_emission emission;
+    std::string alphabet;            // sorted (sequence_prepareAlphabet, pairwiseAligner.c:294-323)
+    int32_t kmer_length = 0;
+    int64_t n_kmers = 0;
+    double t[SA_N_TRANSITIONS];
+    double scale = 1.0, shift = 0.0, var = 1.0;
+    std::vector<double> match, gapy, gapx;
+    sa::HdpTables hdp;
+    std::vector<std::string> kmer_strings;   // interned path k-mers, built on first use
+    sa::DeviceModel dev;
+    bool dev_dirty = true;
+};
+
+namespace sa {
+
+// ----------------------------------------------------------------------------------------------
+// host planning
+// ----------------------------------------------------------------------------------------------
+struct Window {
+    int32_t T;      // traced back to (exclusive lower end of the posterior range)
+    int32_t D;      // traceback diagonal (backward end point)
+    int32_t from;   // last diagonal whose posteriors this window emits
+    int32_t at_end;
+};
+
+struct Region {
+    int64_t x1 = 0, y1 = 0;          // offset of the region in read coordinates
+    int64_t lX = 0, lY = 0;          // k-mers, events
+    int32_t ragged_left = 0, ragged_right = 0;
+    std::vector<int32_t> xmy_l, xmy_r;   // per anti-diagonal 0..lX+lY
+    std::vector<Window> windows;
+    int64_t cells = 0;
+    int32_t max_width = 0;
+};
+
+// band_construct (pairwiseAligner.c:131-182); returns SA_E_ANCHORS on bad anchors
+sa_status band_construct(const int64_t *anchors, int64_t n_anchors, int64_t lX, int64_t lY, int64_t expansion,
+                         int64_t *xmy_l, int64_t *xmy_r);
+
+// getSplitPoints (pairwiseAligner.c:1730-1757)
+sa_status split_points(const int64_t *anchors, int64_t n_anchors, int64_t lX, int64_t lY, int64_t limit,
+                       bool ragged_left, bool ragged_right, std::vector<int64_t> &regions);
+
+// getPosteriorProbsWithBandingSplittingAlignmentsByLargeGaps (pairwiseAligner.c:1773-1837) minus the DP:
+// region geometry, band, traceback windows (getPosteriorProbsWithBanding :1319-1333, :1350)
+sa_status plan_regions(const int64_t *anchors, int64_t n_anchors, int64_t lX, int64_t lY, const sa_params &p,
+                       bool ragged_left, bool ragged_right, std::vector<Region> &regions);
+
+sa_status check_params(const sa_params &p);
+
+// path k-mers of one reference: per column x (1..lX) the ids of its paths (single id when no 'X')
+struct PathTable {
+    int64_t lX = 0;
+    bool multi = false;              // some column has more than one path
+    std::vector<int32_t> first;      // lX + 1 entries; column x's paths are ids[first[x] .. first[x+1])
+    std::vector<int32_t> ids;        // k-mer ids; column 0 holds the NULL path (-1)
+    std::vector<char> kmers;         // k chars per path (for the legality test)
+};
+
+const char *degenerate_options(int32_t degenerate);
+sa_status build_paths(const sa_state_machine *sm, const char *reference, int64_t lX, int32_t degenerate,
+                      PathTable &pt);
+
+// device model upload (both kernel forms)
+sa_status ensure_device_model(sa_state_machine *sm);
+void free_device_model(sa_state_machine *sm);
+
+void count_launch(int64_t n = 1);
+
+#define SA_CUDA_TRY(expr)                                   \
+    do {                                                    \
+        cudaError_t _e = (expr);                            \
+        if (_e != cudaSuccess) return SA_E_CUDA;            \
+    } while (0)
+
+}  // namespace sa

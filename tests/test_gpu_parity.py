@@ -1,0 +1,230 @@
+"""GPU parity: both kernel forms against the FP64 CPU oracle on the same seeded inputs.
+
+Tolerances:
+* plain FP64 form: posterior error <= 1e-5 absolute; pair sets identical except pairs whose
+  posterior lies within 1e-5 of the threshold.
+* batched FP32 form: posterior error <= 1e-4 absolute (pairs missing on one side count with
+  posterior 0 there, so a pair may only be missing if its posterior is within 1e-4 of the
+  threshold); log-likelihood within 1e-3 relative.
+"""
+import numpy as np
+import pytest
+
+from oracle import formats
+from oracle import oracle as orc
+from signalalign_b200 import synth
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-5
+FP32_TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from signalalign_b200 import api as a
+    return a
+
+
+@pytest.fixture(scope="module")
+def cfg0():
+    return synth.config0()
+
+
+def _p(api, **kw):
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    p.diagonal_expansion = kw.get("expansion", 50)
+    p.threshold = kw.get("threshold", 0.01)
+    if "split" in kw:
+        p.split_matrix_bigger_than_this = kw["split"]
+    if "min_diags" in kw:
+        p.min_diags_between_traceback = kw["min_diags"]
+    return p
+
+
+def _op(p):
+    return orc.params(threshold=p.threshold, expansion=p.diagonal_expansion, min_diags=p.min_diags_between_traceback,
+                      traceback=p.traceback_diagonals, split=p.split_matrix_bigger_than_this)
+
+
+def _fp64_case(api, m, emission, rd, p, ragged=(True, True), hdp=None):
+    om = W.oracle_model(m, emission, rd, hdp)
+    sm = W.gpu_model(api, m, emission, rd, hdp)
+    want = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], _op(p), ragged[0], ragged[1])
+    got = api.getAlignedPairsUsingAnchors(sm, rd["reference"], rd["events"], rd["anchors"], p, ragged[0], ragged[1])
+    return want, got
+
+
+def _assert_fp64(want, got, thr):
+    assert W.max_posterior_error(want, got, thr) <= FP64_TOL
+    # away from the threshold the two pair lists are identical, in the same (reference) order
+    keep_w = [tuple(r) for r in want[["x", "y", "kmer"]].tolist()]
+    keep_g = [tuple(r) for r in got[["x", "y", "kmer"]].tolist()]
+    if len(want) == len(got):
+        assert keep_w == keep_g
+    else:
+        near = lambda s: abs(s / 1e7 - thr) <= FP64_TOL
+        assert [k for k, s in zip(keep_w, want["score"]) if not near(s)] == \
+               [k for k, s in zip(keep_g, got["score"]) if not near(s)]
+
+
+def test_fp64_config0(api, cfg0):
+    m = W.gaussian_model(cfg0)
+    rd = cfg0["reads"][0]
+    p = _p(api)
+    want, got = _fp64_case(api, m, orc.EMIT_DESCALED, rd, p)
+    assert len(want) > 500
+    _assert_fp64(want, got, p.threshold)
+
+
+@pytest.mark.parametrize("ragged", [(False, False), (True, False), (False, True)])
+def test_fp64_ragged_ends(api, cfg0, ragged):
+    m = W.gaussian_model(cfg0)
+    rd = cfg0["reads"][0]
+    p = _p(api, threshold=0.05)
+    want, got = _fp64_case(api, m, orc.EMIT_DESCALED, rd, p, ragged=ragged)
+    _assert_fp64(want, got, p.threshold)
+
+
+def test_fp64_split_regions_and_windows(api, cfg0):
+    """small split limit forces getSplitPoints regions; small traceback spacing forces many windows"""
+    m = W.gaussian_model(cfg0)
+    rd = cfg0["reads"][0]
+    p = _p(api, split=150 * 150, min_diags=120)
+    assert len(api.getSplitPoints(rd["anchors"], len(rd["reference"]) - 5, len(rd["events"]),
+                                  p.split_matrix_bigger_than_this, 1, 1)) > 1
+    want, got = _fp64_case(api, m, orc.EMIT_DESCALED, rd, p)
+    _assert_fp64(want, got, p.threshold)
+
+
+def test_fp64_plain_scaled_model_zymo(api):
+    """The Zymo read of the reference's tests, R7.3 model scaled with the read's parameters
+    (emissions_signal_scaleModel), no anchors: the band is the full 892 x 799 matrix."""
+    from golden_models import load_fixture, model_from_fixture
+    fx = load_fixture("zymo")
+    tp = fx["template_params"]
+    m = formats.scale_model(model_from_fixture(fx), tp["scale"], tp["shift"], tp["var"], tp["scale_sd"],
+                            tp["var_sd"])
+    rd = dict(reference=fx["sequence"], events=np.array(fx["events"]), anchors=np.zeros((0, 2), np.int64),
+              scale=1.0, shift=0.0)
+    p = _p(api, expansion=2)
+    want, got = _fp64_case(api, m, orc.EMIT_PLAIN, rd, p, ragged=(False, False))
+    assert len(want) > 900
+    _assert_fp64(want, got, p.threshold)
+
+
+def test_fp64_hdp_small(api):
+    cfg = W.small_hdp_config()
+    n = len(cfg["alphabet"]) ** cfg["k"]
+    hdp = W.hdp_dict(cfg["hdp"], n)
+    text = synth.model_text(cfg["alphabet"], cfg["k"], cfg["table"])
+    m = formats.parse_model_lines(*text.split("\n")[:3])
+    p = _p(api)
+    for rd in cfg["reads"]:
+        want, got = _fp64_case(api, m, orc.EMIT_HDP, rd, p, hdp=hdp)
+        assert len(want) > 50
+        _assert_fp64(want, got, p.threshold)
+
+
+def test_fp64_edge_cases(api, cfg0):
+    m = W.gaussian_model(cfg0)
+    rd = cfg0["reads"][0]
+    p = _p(api)
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED, rd)
+    # no events: every cell is on y = 0, no pair can be emitted
+    got = api.getAlignedPairsUsingAnchors(sm, rd["reference"], np.zeros((0, 4)), [], p)
+    assert len(got) == 0
+    # empty reference and no events: trivial
+    got = api.getAlignedPairsUsingAnchors(sm, "", np.zeros((0, 4)), [], p)
+    assert len(got) == 0
+    # a reference shorter than k is rejected like sequence_correctSeqLength would make it negative
+    with pytest.raises(api.SAError):
+        api.getAlignedPairsUsingAnchors(sm, "ACG", rd["events"][:5], [], p)
+    # out-of-alphabet character
+    with pytest.raises(api.SAError) as ei:
+        api.getAlignedPairsUsingAnchors(sm, "ACGTNACGTACGT", rd["events"][:10], [], p)
+    assert ei.value.status == 2
+    # non-monotone anchors
+    with pytest.raises(api.SAError) as ei:
+        api.getAlignedPairsUsingAnchors(sm, rd["reference"], rd["events"], [(50, 80), (40, 90)], p)
+    assert ei.value.status == 3
+    # tiny read without anchors matches the oracle
+    small = dict(rd, reference=rd["reference"][:40], events=rd["events"][:50], anchors=np.zeros((0, 2), np.int64))
+    want, got = _fp64_case(api, m, orc.EMIT_DESCALED, small, p)
+    _assert_fp64(want, got, p.threshold)
+
+
+# ------------------------------------------------------------------------------------------------
+# batched FP32 form
+# ------------------------------------------------------------------------------------------------
+def _batch_vs_oracle(api, m, emission, reads, p, hdp=None):
+    sms = [W.gpu_model(api, m, emission, None, hdp)]
+    inputs = [api.ReadInput(sm=sms[0], reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                            scale=rd["scale"], shift=rd["shift"], var=rd.get("var", 1.0)) for rd in reads]
+    b = api.align_batch(inputs, p)
+    errs, llerr = [], []
+    for i, rd in enumerate(reads):
+        assert b.status(i) == 0
+        om = W.oracle_model(m, emission, rd, hdp)
+        want, tps = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], _op(p), True, True,
+                                      with_total_probs=True)
+        got = b.pairs(i)
+        errs.append(W.max_posterior_error(want, got, p.threshold))
+        top = [v for d, v in tps if d == len(rd["reference"]) - m["kmer_length"] + 1 + len(rd["events"])]
+        if top:
+            llerr.append(abs(b.log_likelihood(i) - top[0]) / abs(top[0]))
+    return max(errs), (max(llerr) if llerr else 0.0), b
+
+
+def test_fp32_config0(api, cfg0):
+    m = W.gaussian_model(cfg0)
+    p = _p(api)
+    err, llerr, b = _batch_vs_oracle(api, m, orc.EMIT_DESCALED, cfg0["reads"], p)
+    assert b.cells > 150000
+    assert err <= FP32_TOL, err
+    assert llerr <= 1e-3
+
+
+def test_fp32_mixed_lengths(api):
+    cfg = synth.config1(seed=11, n_reads=6, span=(200, 2500))
+    m = W.gaussian_model(cfg)
+    p = _p(api)
+    err, llerr, _ = _batch_vs_oracle(api, m, orc.EMIT_DESCALED, cfg["reads"], p)
+    assert err <= FP32_TOL, err
+    assert llerr <= 1e-3
+
+
+def test_fp32_hdp_small(api):
+    cfg = W.small_hdp_config()
+    n = len(cfg["alphabet"]) ** cfg["k"]
+    hdp = W.hdp_dict(cfg["hdp"], n)
+    text = synth.model_text(cfg["alphabet"], cfg["k"], cfg["table"])
+    m = formats.parse_model_lines(*text.split("\n")[:3])
+    err, llerr, _ = _batch_vs_oracle(api, m, orc.EMIT_HDP, cfg["reads"], _p(api), hdp=hdp)
+    assert err <= FP32_TOL, err
+    assert llerr <= 1e-3
+
+
+def test_fp32_splits_and_windows(api, cfg0):
+    m = W.gaussian_model(cfg0)
+    p = _p(api, split=150 * 150, min_diags=120)
+    err, _, b = _batch_vs_oracle(api, m, orc.EMIT_DESCALED, cfg0["reads"], p)
+    assert b.regions > 1
+    assert err <= FP32_TOL, err
+
+
+def test_fp32_result_independent_of_batch(api, cfg0):
+    """a read's pairs are the same alone and inside a larger batch"""
+    cfg = synth.config1(seed=12, n_reads=5, span=(300, 1500))
+    m = W.gaussian_model(cfg)
+    p = _p(api)
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED)
+    mk = lambda rd: api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                                  scale=rd["scale"], shift=rd["shift"])
+    alone = api.align_batch([mk(cfg["reads"][2])], p).pairs(0)
+    mixed = api.align_batch([mk(rd) for rd in cfg["reads"]], p).pairs(2)
+    assert np.array_equal(alone, mixed)
