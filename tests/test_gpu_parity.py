@@ -94,7 +94,7 @@ def test_fp64_split_regions_and_windows(api, cfg0):
     """small split limit forces getSplitPoints regions; small traceback spacing forces many windows"""
     m = W.gaussian_model(cfg0)
     rd = cfg0["reads"][0]
-    p = _p(api, split=150 * 150, min_diags=120)
+    p = _p(api, split=2000, min_diags=120)
     assert len(api.getSplitPoints(rd["anchors"], len(rd["reference"]) - 5, len(rd["events"]),
                                   p.split_matrix_bigger_than_this, 1, 1)) > 1
     want, got = _fp64_case(api, m, orc.EMIT_DESCALED, rd, p)
@@ -211,7 +211,7 @@ def test_fp32_hdp_small(api):
 
 def test_fp32_splits_and_windows(api, cfg0):
     m = W.gaussian_model(cfg0)
-    p = _p(api, split=150 * 150, min_diags=120)
+    p = _p(api, split=2000, min_diags=120)
     err, _, b = _batch_vs_oracle(api, m, orc.EMIT_DESCALED, cfg0["reads"], p)
     assert b.regions > 1
     assert err <= FP32_TOL, err
