@@ -29,470 +29,13 @@ namespace fp32 {
 
 using namespace dp32;
 
-constexpr int kThreads = 128;
-constexpr int kWarps = kThreads / 32;
+}  // namespace fp32
+}  // namespace sa
 
-enum { T_MC = 0, T_MFGX, T_MFGY, T_OX, T_OY, T_EX, T_EY, T_SX, T_SY };
+#include "sa_fp32_kernel.cuh"
 
-struct ModelDesc {
-    const KmerConst32 *kc;
-    const float *gapx;
-    Hdp32 hdp;
-    int32_t emission;
-    int32_t pad;
-    float t[9];
-    float pad2;
-};
-
-struct RegionDesc {
-    int32_t n, lX, lY, read;
-    int32_t n_windows, model;
-    int32_t ragged_left, ragged_right;
-    int64_t diag_base;    // first anti-diagonal of this region in the per-anti-diagonal arrays
-    int64_t cell_base;    // first cell of this region in the forward store
-    int64_t win_base;
-    int64_t kmer_base;    // k-mer id of column x >= 1 is kmer[kmer_base + x - 1]
-    int64_t event_base;   // event of row y >= 1 is events[event_base + y - 1]
-    int64_t out_base, out_cap;
-    int64_t x1, y1;
-};
-
-struct Args {
-    const RegionDesc *regions;
-    const int32_t *order;
-    int64_t n_regions;
-    const ModelDesc *models;
-    const ReadScale32 *read_scale;
-    const int32_t *xl, *xr;        // per anti-diagonal band
-    const int64_t *coff;           // per anti-diagonal first cell (region-relative)
-    const Window *windows;
-    const int32_t *kmer;
-    const Event32 *events;
-    float *F;                      // forward store
-    double *base;                  // per anti-diagonal FP64 base of the forward store
-    float *fmax;                   // per anti-diagonal largest stored forward value
-    sa_aligned_pair *out;
-    int64_t *out_count;            // per region
-    double *loglik;                // per region: total probability at its last anti-diagonal
-    int32_t *status;               // per read
-    unsigned int *queue;
-    float threshold;
-    int32_t cpt;                   // cells per thread
-};
-
-struct Shared {
-    float4 la[4];
-    float wmax[2][kWarps];
-    int32_t wcnt[8][kWarps];
-    float pval;
-};
-
-__device__ __forceinline__ float warp_max(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-// Sequential logAdd over vals[0..n) in index order, exactly as a one-thread loop would fold it
-// (dpDiagonal_dotProduct, pairwiseAligner.c:1014-1027), run by one warp: a value can only change the
-// running result if it exceeds the running maximum minus 7.5 (the running result never falls below
-// the running maximum), so only those values are folded, in order.
-__device__ float ordered_fold(const float4 *tab, const float *vals, int n) {
-    const int lane = threadIdx.x & 31;
-    float r = kNegInf, carry = kNegInf;
-    for (int b = 0; b < n; b += 32) {
-        const float v = b + lane < n ? vals[b + lane] : kNegInf;
-        float incl = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const float t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl = fmaxf(incl, t);
-        }
-        incl = fmaxf(incl, carry);
-        float excl = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) excl = carry;
-        unsigned mask = __ballot_sync(0xffffffffu, v > excl - 7.6f);
-        while (mask) {
-            const int bit = __ffs(mask) - 1;
-            mask &= mask - 1;
-            r = log_add(tab, r, __shfl_sync(0xffffffffu, v, bit));
-        }
-        carry = __shfl_sync(0xffffffffu, incl, 31);
-    }
-    return r;
-}
-
-__global__ void prep_events(const double2 *raw, Event32 *out, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
-        const double2 e = raw[i];
-        Event32 v;
-        v.mean = (float) e.x;
-        v.noise = (float) e.y;
-        v.c_noise = (float) (-1.5 * log(e.y));
-        v.inv_noise = (float) (1.0 / e.y);
-        out[i] = v;
-    }
-}
-
-struct Ctx {
-    const Args *A;
-    RegionDesc Rv;
-    const RegionDesc *R;   // points at Rv
-    int32_t region_index;
-    const ModelDesc *M;
-    ReadScale32 rs;
-    Shared *sh;
-    float *fring;     // [3 slots][3 states][wmax]
-    float *bring;     // [3 slots][3 states][wmax]
-    float *chain;     // [2][wmax]
-    int wmax;
-};
-
-__device__ __forceinline__ int32_t kmer_of(const Ctx &c, int32_t x) {
-    return x > 0 ? __ldg(c.A->kmer + c.R->kmer_base + x - 1) : -1;
-}
-
-__device__ __forceinline__ void emissions(const Ctx &c, int32_t kid, int32_t y_event, float &em, float &ey) {
-    const Event32 ev = c.A->events[c.R->event_base + y_event];
-    if (kid < 0) { em = ey = kNegInf; return; }
-    const KmerConst32 k = c.M->kc[kid];
-    if (c.M->emission == SA_EMIT_HDP) {
-        em = ey = emit_hdp(c.M->hdp, k, kid, ev, c.rs);
-    } else {
-        emit_gauss(k, ev, c.rs, em, ey);
-    }
-}
-
-__device__ __forceinline__ float emission_gapx(const Ctx &c, int32_t kid) {
-    if (c.M->emission == SA_EMIT_HDP) return (float) kLogPointOne;
-    return kid < 0 ? kNegInf : __ldg(c.M->gapx + kid);
-}
-
-__device__ __forceinline__ float *ring(float *r, int wmax, int slot, int state) { return r + (slot * 3 + state) * wmax; }
-
-// total probability of anti-diagonal d (diagonalCalculationTotalProbability, pairwiseAligner.c:
-// 1182-1200) relative to base(F_d) + base(B_d).  fs/bs: slots of F_d (global) and B_d, B_{d+1} (ring).
-__device__ float total_probability(Ctx &c, int32_t d, bool have_next, int slot_d, int slot_n, float fmax_prev,
-                                   float bmax_next) {
-    const Args &A = *c.A;
-    const RegionDesc &R = *c.R;
-    const float4 *tab = c.sh->la;
-    const float *t = c.M->t;
-    const int tid = threadIdx.x;
-    const int32_t L = A.xl[R.diag_base + d], W = (A.xr[R.diag_base + d] - L) / 2 + 1;
-    const float *Fd = A.F + 3 * (R.cell_base + A.coff[R.diag_base + d]);
-    const float *bM = ring(c.bring, c.wmax, slot_d, 0), *bX = ring(c.bring, c.wmax, slot_d, 1),
-                *bY = ring(c.bring, c.wmax, slot_d, 2);
-    for (int i = tid; i < W; i += kThreads) {
-        float s = Fd[i] + bM[i];
-        s = log_add(tab, s, Fd[W + i] + bX[i]);
-        s = log_add(tab, s, Fd[2 * W + i] + bY[i]);
-        c.chain[i] = s;
-    }
-    int32_t Wn = 0;
-    if (have_next && d >= 1) {
-        const int32_t dn = d + 1;
-        const int32_t Ln = A.xl[R.diag_base + dn];
-        Wn = (A.xr[R.diag_base + dn] - Ln) / 2 + 1;
-        const int32_t Lp = A.xl[R.diag_base + d - 1], Rp = A.xr[R.diag_base + d - 1];
-        const int32_t Wp = (Rp - Lp) / 2 + 1;
-        const float *Fp = A.F + 3 * (R.cell_base + A.coff[R.diag_base + d - 1]);
-        const float *nM = ring(c.bring, c.wmax, slot_n, 0);
-        const float shift = -fmax_prev - bmax_next;
-        for (int i = tid; i < Wn; i += kThreads) {
-            const int32_t xmy = Ln + 2 * i;
-            float m = kNegInf;
-            if (xmy >= Lp && xmy <= Rp) {
-                const int32_t x = (dn + xmy) >> 1, y = (dn - xmy) >> 1;
-                const int32_t im = (xmy - Lp) >> 1;
-                float em, ey;
-                emissions(c, kmer_of(c, x), y - 1, em, ey);
-                m = Fp[im] + (em + t[T_MC]);
-                m = log_add(tab, m, Fp[Wp + im] + (em + t[T_MFGX]));
-                m = log_add(tab, m, Fp[2 * Wp + im] + (em + t[T_MFGY]));
-            }
-            c.chain[c.wmax + i] = m + nM[i] + shift;
-        }
-    }
-    __syncthreads();
-    if (tid < 32) {
-        float p = ordered_fold(tab, c.chain, W);
-        if (Wn > 0) p = log_add(tab, p, ordered_fold(tab, c.chain + c.wmax, Wn));
-        if (tid == 0) c.sh->pval = p;
-    }
-    __syncthreads();
-    return c.sh->pval;
-}
-
-__device__ void run_region(Ctx &c) {
-    const Args &A = *c.A;
-    const RegionDesc &R = *c.R;
-    const ModelDesc &M = *c.M;
-    const float *t = M.t;
-    const float4 *tab = c.sh->la;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int64_t db = R.diag_base;
-    const int cpt = A.cpt;
-
-    // anti-diagonal 0: startStateProb / raggedStartStateProb (stateMachine.c:1022-1032)
-    if (tid == 0) {
-        const float s0 = R.ragged_left ? kNegInf : 0.0f, s1 = R.ragged_left ? 0.0f : kNegInf;
-        float *F0 = A.F + 3 * (R.cell_base + A.coff[db]);
-        F0[0] = s0; F0[1] = s1; F0[2] = s1;
-        ring(c.fring, c.wmax, 0, 0)[0] = s0;
-        ring(c.fring, c.wmax, 0, 1)[0] = s1;
-        ring(c.fring, c.wmax, 0, 2)[0] = s1;
-        A.base[db] = 0.0;
-        A.fmax[db] = 0.0f;
-    }
-    __syncthreads();
-    double fbase = 0.0;        // base of the anti-diagonal being computed
-    float m1 = 0.0f, m2 = 0.0f;  // largest stored value of anti-diagonals d-1, d-2
-    int32_t Lp = A.xl[db], Rp = A.xr[db], Lpp = 0, Rpp = -1;
-    int32_t wi = 0;
-    Window W = A.windows[R.win_base];
-    int64_t n_out = 0;
-    double ll = 0.0;
-    for (int32_t d = 1; d <= R.n; ++d) {
-        fbase += (double) m1;
-        const int32_t L = A.xl[db + d], Rr = A.xr[db + d], Wd = (Rr - L) / 2 + 1;
-        const int slot = d % 3, s1 = (d + 2) % 3, s2 = (d + 1) % 3;
-        float *Fd = A.F + 3 * (R.cell_base + A.coff[db + d]);
-        float lmax = kNegInf;
-        for (int j = 0; j < cpt; ++j) {
-            const int i = tid + j * kThreads;
-            if (i >= Wd) break;
-            const int32_t xmy = L + 2 * i, x = (d + xmy) >> 1, y = (d - xmy) >> 1;
-            const int32_t kid = kmer_of(c, x);
-            float vM = kNegInf, vX = kNegInf, vY = kNegInf;
-            const bool lower = xmy - 1 >= Lp && xmy - 1 <= Rp;
-            const bool upper = xmy + 1 >= Lp && xmy + 1 <= Rp;
-            const bool middle = d >= 2 && xmy >= Lpp && xmy <= Rpp;
-            if (lower) {
-                const int il = (xmy - 1 - Lp) >> 1;
-                const float e = emission_gapx(c, kid) - m1;
-                vX = ring(c.fring, c.wmax, s1, 0)[il] + (e + t[T_OX]);
-                vX = log_add(tab, vX, ring(c.fring, c.wmax, s1, 1)[il] + (e + t[T_EX]));
-                vX = log_add(tab, vX, ring(c.fring, c.wmax, s1, 2)[il] + (e + t[T_SX]));
-            }
-            if (middle || upper) {
-                float em, ey;
-                emissions(c, kid, y - 1, em, ey);
-                if (middle) {
-                    const int im = (xmy - Lpp) >> 1;
-                    const float e = em - m2 - m1;
-                    vM = ring(c.fring, c.wmax, s2, 0)[im] + (e + t[T_MC]);
-                    vM = log_add(tab, vM, ring(c.fring, c.wmax, s2, 1)[im] + (e + t[T_MFGX]));
-                    vM = log_add(tab, vM, ring(c.fring, c.wmax, s2, 2)[im] + (e + t[T_MFGY]));
-                }
-                if (upper) {
-                    const int iu = (xmy + 1 - Lp) >> 1;
-                    const float e = ey - m1;
-                    vY = ring(c.fring, c.wmax, s1, 0)[iu] + (e + t[T_OY]);
-                    vY = log_add(tab, vY, ring(c.fring, c.wmax, s1, 2)[iu] + (e + t[T_EY]));
-                }
-            }
-            ring(c.fring, c.wmax, slot, 0)[i] = vM;
-            ring(c.fring, c.wmax, slot, 1)[i] = vX;
-            ring(c.fring, c.wmax, slot, 2)[i] = vY;
-            Fd[i] = vM;
-            Fd[Wd + i] = vX;
-            Fd[2 * Wd + i] = vY;
-            lmax = fmaxf(lmax, fmaxf(vM, fmaxf(vX, vY)));
-        }
-        lmax = warp_max(lmax);
-        if (lane == 0) c.sh->wmax[d & 1][warp] = lmax;
-        __syncthreads();
-        float md = c.sh->wmax[d & 1][0];
-#pragma unroll
-        for (int w = 1; w < kWarps; ++w) md = fmaxf(md, c.sh->wmax[d & 1][w]);
-        if (!(md > kNegInf)) md = 0.0f;
-        if (tid == 0) {
-            A.base[db + d] = fbase;
-            A.fmax[db + d] = md;
-        }
-        m2 = m1; m1 = md;
-        Lpp = Lp; Rpp = Rp; Lp = L; Rp = Rr;
-        if (d != W.D) continue;
-
-        // ---------------- backward sweep of the window (T, D] with fused posteriors -------------
-        __threadfence_block();
-        const bool ragged_end = W.at_end && R.ragged_right;
-        const float e0 = ragged_end ? (t[T_OX] + t[T_OY]) / 2.0f : t[T_MC];
-        const float e1 = ragged_end ? t[T_EX] : t[T_MFGX];
-        const float e2 = ragged_end ? t[T_EY] : t[T_MFGY];
-        {
-            const int sl = d % 3;
-            for (int i = tid; i < Wd; i += kThreads) {
-                ring(c.bring, c.wmax, sl, 0)[i] = e0;
-                ring(c.bring, c.wmax, sl, 1)[i] = e1;
-                ring(c.bring, c.wmax, sl, 2)[i] = e2;
-            }
-        }
-        float bm_end = fmaxf(e0, fmaxf(e1, e2));
-        if (!(bm_end > kNegInf)) bm_end = 0.0f;
-        double bbase = 0.0;            // base of B on the anti-diagonal being processed
-        float b1 = bm_end, b2 = 0.0f;  // largest stored B value on d2+1, d2+2
-        int32_t BLn = L, BRn = Rr, BLnn = 0, BRnn = -1;   // band of d2+1, d2+2
-        double pref = 0.0;             // latest refresh total probability (absolute)
-        int32_t k = 0;
-        __syncthreads();
-        for (int32_t d2 = W.D; d2 > W.T; --d2) {
-            const int sl = d2 % 3, sn = (d2 + 1) % 3, snn = (d2 + 2) % 3;
-            const int32_t BL = A.xl[db + d2], BR = A.xr[db + d2], BW = (BR - BL) / 2 + 1;
-            float bmd = bm_end;
-            if (d2 < W.D) {
-                bbase += (double) b1;
-                float lm = kNegInf;
-                for (int j = 0; j < cpt; ++j) {
-                    const int i = tid + j * kThreads;
-                    if (i >= BW) break;
-                    const int32_t xmy = BL + 2 * i, x = (d2 + xmy) >> 1, y = (d2 - xmy) >> 1;
-                    float vM = kNegInf, vX = kNegInf, vY = kNegInf;
-                    const bool mid = d2 + 2 <= W.D && xmy >= BLnn && xmy <= BRnn;
-                    const bool up = xmy - 1 >= BLn && xmy - 1 <= BRn;
-                    const bool lo = xmy + 1 >= BLn && xmy + 1 <= BRn;
-                    if (mid) {
-                        float em, ey;
-                        emissions(c, kmer_of(c, x + 1), y, em, ey);
-                        const float bmv = ring(c.bring, c.wmax, snn, 0)[(xmy - BLnn) >> 1];
-                        const float e = em - b2 - b1;
-                        vM = bmv + (e + t[T_MC]);
-                        vX = bmv + (e + t[T_MFGX]);
-                        vY = bmv + (e + t[T_MFGY]);
-                    }
-                    if (up) {
-                        float em, ey;
-                        emissions(c, kmer_of(c, x), y, em, ey);
-                        const float buv = ring(c.bring, c.wmax, sn, 2)[(xmy - 1 - BLn) >> 1];
-                        const float e = ey - b1;
-                        vM = log_add(tab, vM, buv + (e + t[T_OY]));
-                        vY = log_add(tab, vY, buv + (e + t[T_EY]));
-                    }
-                    if (lo) {
-                        const float blv = ring(c.bring, c.wmax, sn, 1)[(xmy + 1 - BLn) >> 1];
-                        const float e = emission_gapx(c, kmer_of(c, x + 1)) - b1;
-                        vM = log_add(tab, vM, blv + (e + t[T_OX]));
-                        vX = log_add(tab, vX, blv + (e + t[T_EX]));
-                        vY = log_add(tab, vY, blv + (e + t[T_SX]));
-                    }
-                    ring(c.bring, c.wmax, sl, 0)[i] = vM;
-                    ring(c.bring, c.wmax, sl, 1)[i] = vX;
-                    ring(c.bring, c.wmax, sl, 2)[i] = vY;
-                    lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
-                }
-                lm = warp_max(lm);
-                if (lane == 0) c.sh->wmax[d2 & 1][warp] = lm;
-                __syncthreads();
-                bmd = c.sh->wmax[d2 & 1][0];
-#pragma unroll
-                for (int w = 1; w < kWarps; ++w) bmd = fmaxf(bmd, c.sh->wmax[d2 & 1][w]);
-                if (!(bmd > kNegInf)) bmd = 0.0f;
-            }
-            if (d2 <= W.from) {
-                const double fb = A.base[db + d2];
-                if (k++ % 10 == 0) {
-                    const bool have_next = d2 < W.D;
-                    const float fmp = d2 >= 1 ? A.fmax[db + d2 - 1] : 0.0f;
-                    const float pt = total_probability(c, d2, have_next, sl, sn, fmp, b1);
-                    pref = (double) pt + fb + bbase;
-                    if (d2 == R.n) ll = pref;
-                }
-                const float kd = (float) (fb + bbase - pref);
-                const float *Fm = A.F + 3 * (R.cell_base + A.coff[db + d2]);
-                const float *bM = ring(c.bring, c.wmax, sl, 0);
-                unsigned flags = 0;
-                float pv[8];
-                for (int j = 0; j < cpt && j < 8; ++j) {
-                    const int i = tid + j * kThreads;
-                    pv[j] = 0.0f;
-                    if (i < BW) {
-                        const int32_t xmy = BL + 2 * i, x = (d2 + xmy) >> 1, y = (d2 - xmy) >> 1;
-                        if (x > 0 && y > 0) {
-                            const float p = __expf(Fm[i] + bM[i] + kd);
-                            if (p >= A.threshold) { flags |= 1u << j; pv[j] = p; }
-                        }
-                    }
-                    const unsigned bal = __ballot_sync(0xffffffffu, (flags >> j) & 1u);
-                    if (lane == 0) c.sh->wcnt[j][warp] = __popc(bal);
-                }
-                __syncthreads();
-                int64_t before = 0;
-                for (int j = 0; j < cpt && j < 8; ++j) {
-                    int32_t tot = 0, pre = 0;
-#pragma unroll
-                    for (int w = 0; w < kWarps; ++w) {
-                        const int32_t cw = c.sh->wcnt[j][w];
-                        if (w < warp) pre += cw;
-                        tot += cw;
-                    }
-                    const unsigned mine = __ballot_sync(0xffffffffu, (flags >> j) & 1u);
-                    if ((flags >> j) & 1u) {
-                        const int rank = __popc(mine & ((1u << lane) - 1u));
-                        const int64_t slot64 = n_out + before + pre + rank;
-                        const int i = tid + j * kThreads;
-                        const int32_t xmy = BL + 2 * i, x = (d2 + xmy) >> 1, y = (d2 - xmy) >> 1;
-                        if (slot64 < R.out_cap) {
-                            sa_aligned_pair o;
-                            const float p = fminf(pv[j], 1.0f);
-                            o.score = (int64_t) floor((double) p * 10000000.0);
-                            o.x = R.x1 + x - 1;
-                            o.y = R.y1 + y - 1;
-                            o.kmer = kmer_of(c, x);
-                            A.out[R.out_base + slot64] = o;
-                        } else {
-                            atomicMax(A.status + R.read, (int32_t) SA_E_OUTPUT);
-                        }
-                    }
-                    before += tot;
-                }
-                n_out += before;
-            }
-            b2 = b1; b1 = bmd;
-            BLnn = BLn; BRnn = BRn; BLn = BL; BRn = BR;
-        }
-        __syncthreads();
-        if (W.at_end) break;
-        W = A.windows[R.win_base + (++wi)];
-    }
-    if (tid == 0) {
-        A.out_count[c.region_index] = n_out;
-        A.loglik[c.region_index] = ll;
-    }
-}
-
-__global__ void __launch_bounds__(kThreads) batch_kernel(const __grid_constant__ Args A, int wmax) {
-    extern __shared__ float4 smem_raw[];
-    Shared *sh = reinterpret_cast<Shared *>(smem_raw);
-    float *fring = reinterpret_cast<float *>(sh + 1);
-    float *bring = fring + 9 * wmax;
-    float *chain = bring + 9 * wmax;
-    if (threadIdx.x < 4) {
-        const LogAddTable lt = log_add_table();
-        sh->la[threadIdx.x] = lt.c[threadIdx.x];
-    }
-    __shared__ int32_t next;
-    for (;;) {
-        __syncthreads();
-        if (threadIdx.x == 0) next = (int32_t) atomicAdd(A.queue, 1u);
-        __syncthreads();
-        const int32_t qi = next;
-        if (qi >= A.n_regions) break;
-        Ctx c;
-        c.A = &A;
-        c.region_index = A.order[qi];
-        c.Rv = A.regions[c.region_index];
-        c.R = &c.Rv;
-        c.M = A.models + c.Rv.model;
-        c.rs = A.read_scale[c.R->read];
-        c.sh = sh;
-        c.fring = fring;
-        c.bring = bring;
-        c.chain = chain;
-        c.wmax = wmax;
-        run_region(c);
-    }
-}
+namespace sa {
+namespace fp32 {
 
 // FP32 issue-rate probe for the roofline denominator: 8 independent FMA chains per thread.
 __global__ void __launch_bounds__(256) fma_probe(float *sink, int iters, float seed) {
@@ -546,7 +89,7 @@ struct sa_batch {
     Window *d_windows = nullptr;
     double2 *d_events_raw = nullptr;
     Event32 *d_events = nullptr;
-    float *d_F = nullptr, *d_fmax = nullptr;
+    float *d_F = nullptr, *d_fshift = nullptr;
     double *d_base = nullptr, *d_loglik = nullptr;
     sa_aligned_pair *d_out = nullptr;
     unsigned int *d_queue = nullptr;
@@ -579,7 +122,7 @@ void free_batch_device(sa_batch *b) {
     cudaFree(b->d_regions); cudaFree(b->d_order); cudaFree(b->d_models); cudaFree(b->d_read_scale);
     cudaFree(b->d_xl); cudaFree(b->d_xr); cudaFree(b->d_kmer); cudaFree(b->d_status); cudaFree(b->d_coff);
     cudaFree(b->d_out_count); cudaFree(b->d_windows); cudaFree(b->d_events_raw); cudaFree(b->d_events);
-    cudaFree(b->d_F); cudaFree(b->d_fmax); cudaFree(b->d_base); cudaFree(b->d_loglik); cudaFree(b->d_out);
+    cudaFree(b->d_F); cudaFree(b->d_fshift); cudaFree(b->d_base); cudaFree(b->d_loglik); cudaFree(b->d_out);
     cudaFree(b->d_queue);
 }
 
@@ -675,7 +218,7 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
         }
         b->read_n_regions[r] = (int64_t) b->regions.size() - b->read_first_region[r];
     }
-    if (b->max_width > 8 * kThreads) {
+    if (b->max_width > kMaxCpt * kGroup) {
         delete b;
         return SA_E_CAPACITY;
     }
@@ -712,7 +255,7 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
     if (!st) st = dalloc(&b->d_events, b->events.size());
     if (!st) st = dalloc(&b->d_F, 3 * (size_t) b->cells);
     if (!st) st = dalloc(&b->d_base, nd);
-    if (!st) st = dalloc(&b->d_fmax, nd);
+    if (!st) st = dalloc(&b->d_fshift, nd);
     if (!st) st = dalloc(&b->d_out, (size_t) b->out_total);
     if (!st) st = dalloc(&b->d_out_count, b->regions.size());
     if (!st) st = dalloc(&b->d_loglik, b->regions.size());
@@ -740,7 +283,6 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
         ModelDesc &m = md[i];
         std::memset(&m, 0, sizeof(m));
         m.kc = sm->dev.kc32;
-        m.gapx = sm->dev.gapx32;
         m.emission = sm->emission;
         for (int j = 0; j < 9; ++j) m.t[j] = (float) sm->t[j];
         if (sm->emission == SA_EMIT_HDP) {
@@ -803,24 +345,30 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         a.events = b->d_events;
         a.F = b->d_F;
         a.base = b->d_base;
-        a.fmax = b->d_fmax;
+        a.fshift = b->d_fshift;
         a.out = b->d_out;
         a.out_count = b->d_out_count;
         a.loglik = b->d_loglik;
         a.status = b->d_status;
         a.queue = b->d_queue;
         a.threshold = b->threshold;
-        const int cpt = (b->max_width + kThreads - 1) / kThreads;
-        a.cpt = std::max(1, cpt);
-        const int wmax = a.cpt * kThreads;
-        const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) (9 * wmax * 2 + 2 * wmax);
+        const int cpt = std::max(1, (b->max_width + kGroup - 1) / kGroup);
+        const int cpt_pow2 = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
+        a.wmax = cpt_pow2 * kGroup;
+        a.spin_limit = 20000000000LL;   // ~10 s at 2 GHz: far beyond any window's forward time
+        const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) (20 * a.wmax);
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-        if (smem > 48 * 1024) cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, kThreads, smem);
-        int64_t grid = (int64_t) std::max(1, sms) * std::max(1, per_sm);
-        grid = std::min<int64_t>(grid, (int64_t) b->regions.size());
-        batch_kernel<<<(unsigned) grid, kThreads, smem, s>>>(a, wmax);
+        auto launch = [&](auto kern) {
+            if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+            int64_t grid = (int64_t) std::max(1, sms) * std::max(1, per_sm);
+            grid = std::min<int64_t>(grid, (int64_t) b->regions.size());
+            kern<<<(unsigned) grid, kThreads, smem, s>>>(a);
+        };
+        if (cpt_pow2 == 1) launch(batch_kernel<1>);
+        else if (cpt_pow2 == 2) launch(batch_kernel<2>);
+        else launch(batch_kernel<4>);
         count_launch();
         if (cudaGetLastError() != cudaSuccess) st = SA_E_CUDA;
     }

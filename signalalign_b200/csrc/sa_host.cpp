@@ -565,7 +565,7 @@ sa_status ensure_device_model(sa_state_machine *sm) {
         c.k_y = (float) (-1.8378770664093453 - std::log(y[1]) + half_log_lambda);
         c.inv_nu = (float) (1.0 / m[2]);
         c.half_lambda = (float) (0.5 * m[4]);
-        c.pad = 0.0f;
+        c.gapx = (float) sm->gapx[i];
         gx[i] = (float) sm->gapx[i];
     }
     if (!st) st = upload(&d.match, sm->match.data(), sm->match.size());

@@ -35,10 +35,10 @@ struct HdpTables {
 // FP32 per-k-mer emission constants (one 32-byte record per k-mer), derived on the host in FP64
 // from the reference tables:
 //   mu, 1/sd_match, 1/sd_gapy, k_m = -log(2 pi) - log(sd_match) + 0.5 log(lambda),
-//   k_y = -log(2 pi) - log(sd_gapy) + 0.5 log(lambda), 1/noise_mean, lambda/2
+//   k_y = -log(2 pi) - log(sd_gapy) + 0.5 log(lambda), 1/noise_mean, lambda/2, gap-X log probability
 struct __align__(16) KmerConst32 {
     float mu, inv_sd_m, inv_sd_y, k_m;
-    float k_y, inv_nu, half_lambda, pad;
+    float k_y, inv_nu, half_lambda, gapx;
 };
 
 struct DeviceModel {
