@@ -75,6 +75,7 @@ struct sa_batch {
     std::vector<int64_t> coff;
     std::vector<Window> windows;
     std::vector<int32_t> kmer;
+    std::vector<float> gapx;
     std::vector<double2> events;
     int64_t cells = 0, out_total = 0;
     int32_t max_width = 0;
@@ -85,6 +86,7 @@ struct sa_batch {
     ModelDesc *d_models = nullptr;
     ReadScale32 *d_read_scale = nullptr;
     int32_t *d_xl = nullptr, *d_xr = nullptr, *d_kmer = nullptr, *d_status = nullptr;
+    float *d_gapx = nullptr;
     int64_t *d_coff = nullptr, *d_out_count = nullptr;
     Window *d_windows = nullptr;
     double2 *d_events_raw = nullptr;
@@ -120,7 +122,7 @@ sa_status h2d(T *dst, const std::vector<T> &src, cudaStream_t s) {
 
 void free_batch_device(sa_batch *b) {
     cudaFree(b->d_regions); cudaFree(b->d_order); cudaFree(b->d_models); cudaFree(b->d_read_scale);
-    cudaFree(b->d_xl); cudaFree(b->d_xr); cudaFree(b->d_kmer); cudaFree(b->d_status); cudaFree(b->d_coff);
+    cudaFree(b->d_xl); cudaFree(b->d_xr); cudaFree(b->d_kmer); cudaFree(b->d_gapx); cudaFree(b->d_status); cudaFree(b->d_coff);
     cudaFree(b->d_out_count); cudaFree(b->d_windows); cudaFree(b->d_events_raw); cudaFree(b->d_events);
     cudaFree(b->d_F); cudaFree(b->d_fshift); cudaFree(b->d_base); cudaFree(b->d_loglik); cudaFree(b->d_out);
     cudaFree(b->d_queue);
@@ -179,7 +181,11 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
         rs.inv_var = (float) (1.0 / var);
         rs.log_inv_var = (float) std::log(1.0 / var);
         const int64_t kmer_base = (int64_t) b->kmer.size();
-        for (int64_t x = 1; x <= lX; ++x) b->kmer.push_back(pt.ids[pt.first[x]]);
+        for (int64_t x = 1; x <= lX; ++x) {
+            const int32_t kid = pt.ids[pt.first[x]];
+            b->kmer.push_back(kid);
+            b->gapx.push_back(sm->emission == SA_EMIT_HDP ? (float) kLogPointOne : (float) sm->gapx[kid]);
+        }
         const int64_t event_base = (int64_t) b->events.size();
         for (int64_t y = 0; y < rd.n_events; ++y)
             b->events.push_back(make_double2(rd.events[y * kEventParams], rd.events[y * kEventParams + 1]));
@@ -251,9 +257,10 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
     if (!st) st = dalloc(&b->d_coff, nd);
     if (!st) st = dalloc(&b->d_windows, b->windows.size());
     if (!st) st = dalloc(&b->d_kmer, b->kmer.size());
+    if (!st) st = dalloc(&b->d_gapx, b->gapx.size());
     if (!st) st = dalloc(&b->d_events_raw, b->events.size());
     if (!st) st = dalloc(&b->d_events, b->events.size());
-    if (!st) st = dalloc(&b->d_F, 3 * (size_t) b->cells);
+    if (!st) st = dalloc(&b->d_F, (size_t) kStoreStride * (size_t) b->cells);
     if (!st) st = dalloc(&b->d_base, nd);
     if (!st) st = dalloc(&b->d_fshift, nd);
     if (!st) st = dalloc(&b->d_out, (size_t) b->out_total);
@@ -306,6 +313,7 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
     if (!st) st = h2d(b->d_coff, b->coff, s);
     if (!st) st = h2d(b->d_windows, b->windows, s);
     if (!st) st = h2d(b->d_kmer, b->kmer, s);
+    if (!st) st = h2d(b->d_gapx, b->gapx, s);
     if (!st) st = h2d(b->d_events_raw, b->events, s);
     if (!st && !b->events.empty()) {
         const int64_t n = (int64_t) b->events.size();
@@ -342,6 +350,7 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         a.coff = b->d_coff;
         a.windows = b->d_windows;
         a.kmer = b->d_kmer;
+        a.gapx = b->d_gapx;
         a.events = b->d_events;
         a.F = b->d_F;
         a.base = b->d_base;
@@ -465,7 +474,7 @@ sa_status sa_batch_transfer_bytes(const sa_batch *b, int64_t *h2d, int64_t *d2h)
     if (!b || !h2d || !d2h) return SA_E_ARG;
     auto bytes = [](const auto &v) { return (int64_t) (v.size() * sizeof(v[0])); };
     *h2d = bytes(b->regions) + bytes(b->order) + (int64_t) (b->models.size() * sizeof(ModelDesc)) +
-           bytes(b->read_scale) + bytes(b->xl) + bytes(b->xr) + bytes(b->coff) + bytes(b->windows) + bytes(b->kmer) +
+           bytes(b->read_scale) + bytes(b->xl) + bytes(b->xr) + bytes(b->coff) + bytes(b->windows) + bytes(b->kmer) + bytes(b->gapx) +
            bytes(b->events);
     int64_t pairs = 0;
     for (const auto &rp : b->read_pairs) pairs += (int64_t) rp.size();
