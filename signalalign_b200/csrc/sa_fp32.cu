@@ -71,8 +71,8 @@ struct sa_batch {
     std::vector<int32_t> read_status;       // host planning status per read
     std::vector<int64_t> read_first_region, read_n_regions;
     std::vector<ReadScale32> read_scale;
-    std::vector<int32_t> xl, xr;
-    std::vector<int64_t> coff;
+    std::vector<int2> meta;
+    std::vector<int32_t> window_off;
     std::vector<Window> windows;
     std::vector<int32_t> kmer;
     std::vector<float> gapx;
@@ -85,9 +85,10 @@ struct sa_batch {
     int32_t *d_order = nullptr;
     ModelDesc *d_models = nullptr;
     ReadScale32 *d_read_scale = nullptr;
-    int32_t *d_xl = nullptr, *d_xr = nullptr, *d_kmer = nullptr, *d_status = nullptr;
+    int2 *d_meta = nullptr;
+    int32_t *d_window_off = nullptr, *d_kmer = nullptr, *d_status = nullptr;
     float *d_gapx = nullptr;
-    int64_t *d_coff = nullptr, *d_out_count = nullptr;
+    int64_t *d_out_count = nullptr;
     Window *d_windows = nullptr;
     double2 *d_events_raw = nullptr;
     Event32 *d_events = nullptr;
@@ -122,7 +123,7 @@ sa_status h2d(T *dst, const std::vector<T> &src, cudaStream_t s) {
 
 void free_batch_device(sa_batch *b) {
     cudaFree(b->d_regions); cudaFree(b->d_order); cudaFree(b->d_models); cudaFree(b->d_read_scale);
-    cudaFree(b->d_xl); cudaFree(b->d_xr); cudaFree(b->d_kmer); cudaFree(b->d_gapx); cudaFree(b->d_status); cudaFree(b->d_coff);
+    cudaFree(b->d_meta); cudaFree(b->d_window_off); cudaFree(b->d_kmer); cudaFree(b->d_gapx); cudaFree(b->d_status);
     cudaFree(b->d_out_count); cudaFree(b->d_windows); cudaFree(b->d_events_raw); cudaFree(b->d_events);
     cudaFree(b->d_F); cudaFree(b->d_fshift); cudaFree(b->d_base); cudaFree(b->d_loglik); cudaFree(b->d_out);
     cudaFree(b->d_queue);
@@ -200,7 +201,7 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
             d.model = model;
             d.ragged_left = rg.ragged_left;
             d.ragged_right = rg.ragged_right;
-            d.diag_base = (int64_t) b->xl.size();
+            d.diag_base = (int64_t) b->meta.size();
             d.cell_base = b->cells;
             d.win_base = (int64_t) b->windows.size();
             d.kmer_base = kmer_base + rg.x1;
@@ -210,13 +211,23 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
             d.out_cap = 4 * (int64_t) d.n + 256;
             d.out_base = b->out_total;
             b->out_total += d.out_cap;
+            // per anti-diagonal meta: band start, width, window end / refresh / stored gap states
+            std::vector<int32_t> flags(d.n + 2, 0);
+            for (const Window &w : rg.windows) {
+                flags[w.D] |= kFlagWindowEnd;
+                for (int32_t r = w.from; r > w.T; r -= 10) flags[r] |= kFlagRefresh;
+            }
+            std::vector<int64_t> off(d.n + 1, 0);
             int64_t acc = 0;
             for (int32_t dd = 0; dd <= d.n; ++dd) {
-                b->xl.push_back(rg.xmy_l[dd]);
-                b->xr.push_back(rg.xmy_r[dd]);
-                b->coff.push_back(acc);
-                acc += (rg.xmy_r[dd] - rg.xmy_l[dd]) / 2 + 1;
+                const int32_t w = (rg.xmy_r[dd] - rg.xmy_l[dd]) / 2 + 1;
+                int32_t f = flags[dd];
+                if ((flags[dd] | flags[dd + 1]) & kFlagRefresh) f |= kFlagStoreGaps;
+                b->meta.push_back(make_int2(rg.xmy_l[dd], w | f));
+                off[dd] = acc;
+                acc += w;
             }
+            for (const Window &w : rg.windows) b->window_off.push_back((int32_t) off[w.D]);
             b->cells += acc;
             b->max_width = std::max(b->max_width, rg.max_width);
             b->windows.insert(b->windows.end(), rg.windows.begin(), rg.windows.end());
@@ -246,15 +257,14 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
         st = ensure_device_model(sm);
         if (st) { cudaSetDevice(prev); delete b; return st; }
     }
-    const size_t nd = b->xl.size();
+    const size_t nd = b->meta.size();
     st = SA_OK;
     if (!st) st = dalloc(&b->d_regions, b->regions.size());
     if (!st) st = dalloc(&b->d_order, b->order.size());
     if (!st) st = dalloc(&b->d_models, b->models.size());
     if (!st) st = dalloc(&b->d_read_scale, b->read_scale.size());
-    if (!st) st = dalloc(&b->d_xl, nd);
-    if (!st) st = dalloc(&b->d_xr, nd);
-    if (!st) st = dalloc(&b->d_coff, nd);
+    if (!st) st = dalloc(&b->d_meta, nd);
+    if (!st) st = dalloc(&b->d_window_off, b->window_off.size());
     if (!st) st = dalloc(&b->d_windows, b->windows.size());
     if (!st) st = dalloc(&b->d_kmer, b->kmer.size());
     if (!st) st = dalloc(&b->d_gapx, b->gapx.size());
@@ -308,9 +318,8 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
     if (!st) st = h2d(b->d_order, b->order, s);
     if (!st) st = h2d(b->d_models, md, s);
     if (!st) st = h2d(b->d_read_scale, b->read_scale, s);
-    if (!st) st = h2d(b->d_xl, b->xl, s);
-    if (!st) st = h2d(b->d_xr, b->xr, s);
-    if (!st) st = h2d(b->d_coff, b->coff, s);
+    if (!st) st = h2d(b->d_meta, b->meta, s);
+    if (!st) st = h2d(b->d_window_off, b->window_off, s);
     if (!st) st = h2d(b->d_windows, b->windows, s);
     if (!st) st = h2d(b->d_kmer, b->kmer, s);
     if (!st) st = h2d(b->d_gapx, b->gapx, s);
@@ -345,9 +354,8 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         a.n_regions = (int64_t) b->regions.size();
         a.models = b->d_models;
         a.read_scale = b->d_read_scale;
-        a.xl = b->d_xl;
-        a.xr = b->d_xr;
-        a.coff = b->d_coff;
+        a.meta = b->d_meta;
+        a.window_off = b->d_window_off;
         a.windows = b->d_windows;
         a.kmer = b->d_kmer;
         a.gapx = b->d_gapx;
@@ -365,7 +373,7 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         const int cpt_pow2 = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
         a.wmax = cpt_pow2 * kGroup;
         a.spin_limit = 20000000000LL;   // ~10 s at 2 GHz: far beyond any window's forward time
-        const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) (20 * a.wmax);
+        const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) (18 * (a.wmax + 2) + 2 * a.wmax);
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
         auto launch = [&](auto kern) {
@@ -474,7 +482,7 @@ sa_status sa_batch_transfer_bytes(const sa_batch *b, int64_t *h2d, int64_t *d2h)
     if (!b || !h2d || !d2h) return SA_E_ARG;
     auto bytes = [](const auto &v) { return (int64_t) (v.size() * sizeof(v[0])); };
     *h2d = bytes(b->regions) + bytes(b->order) + (int64_t) (b->models.size() * sizeof(ModelDesc)) +
-           bytes(b->read_scale) + bytes(b->xl) + bytes(b->xr) + bytes(b->coff) + bytes(b->windows) + bytes(b->kmer) + bytes(b->gapx) +
+           bytes(b->read_scale) + bytes(b->meta) + bytes(b->window_off) + bytes(b->windows) + bytes(b->kmer) + bytes(b->gapx) +
            bytes(b->events);
     int64_t pairs = 0;
     for (const auto &rp : b->read_pairs) pairs += (int64_t) rp.size();

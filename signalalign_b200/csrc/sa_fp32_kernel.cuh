@@ -14,17 +14,21 @@
 // The hand-off is a window counter in shared memory; the backward group's wait on it is bounded
 // (it gives up with SA_E_TIMEOUT), and the forward group never waits on the backward group.
 //
-// Both sweeps software-pipeline everything that does not depend on the recursion: band bounds
-// three anti-diagonals ahead, k-mer ids and events two ahead, k-mer constants one ahead and
-// emissions one anti-diagonal early (forward); stored emissions, forward values and bases one
-// anti-diagonal ahead (backward).
+// The recursion is bound by instruction issue and latency, so the inner loops are branch-free:
+// the rings carry a -inf cell on each side and every slot beyond the anti-diagonal's width holds
+// -inf, so an absent neighbour is a clamped index that reads -inf (logAdd and the sums then behave
+// exactly like the reference's skipped transitions).  Per-anti-diagonal facts (band start, width,
+// window end, refresh, which forward values to store) come packed from the host.  Everything that
+// does not depend on the recursion is software-pipelined: band facts three anti-diagonals ahead,
+// k-mer ids and events two ahead, k-mer constants one ahead and emissions one anti-diagonal early
+// (forward); stored emissions, forward values and bases one anti-diagonal ahead (backward).
 //
 // Values are log probabilities relative to a per-anti-diagonal FP64 base.  The base of d is the
 // base of d-2 plus the largest value stored on d-2 (a lagged renormalisation, so the max reduction
 // is off the critical path); the recorded bases are built from the same float shifts the kernel
 // applies, so they describe the stored values exactly.
 //
-// Forward store layout per anti-diagonal d (region-relative float offset 5*coff[d], W = width):
+// Forward store layout per anti-diagonal d (region-relative float offset 5 * first cell, W = width):
 //   [ match | match emission | extra-event emission | gap-X | gap-Y ], W floats each; the last two
 //   blocks are written only where a refresh needs them.
 #pragma once
@@ -42,6 +46,12 @@ constexpr int kBarForward = 1;
 constexpr int kBarBackward = 2;
 constexpr int kStoreStride = 5;
 enum { ST_M = 0, ST_EM = 1, ST_EY = 2, ST_X = 3, ST_Y = 4 };
+
+// per-anti-diagonal meta: x = xmy of the first cell, y = width | flags
+constexpr int32_t kWidthMask = (1 << 20) - 1;
+constexpr int32_t kFlagWindowEnd = 1 << 20;   // a traceback window closes here
+constexpr int32_t kFlagStoreGaps = 1 << 21;   // a refresh reads this anti-diagonal's gap states
+constexpr int32_t kFlagRefresh = 1 << 22;     // total-probability refresh in its posterior window
 
 enum { T_MC = 0, T_MFGX, T_MFGY, T_OX, T_OY, T_EX, T_EY, T_SX, T_SY };
 
@@ -73,9 +83,9 @@ struct Args {
     int64_t n_regions;
     const ModelDesc *models;
     const ReadScale32 *read_scale;
-    const int32_t *xl, *xr;        // per anti-diagonal band
-    const int64_t *coff;           // per anti-diagonal first cell (region-relative)
+    const int2 *meta;              // per anti-diagonal {xmy of first cell, width | flags}
     const Window *windows;
+    const int32_t *window_off;     // per window: region-relative first cell of its traceback anti-diagonal
     const int32_t *kmer;
     const float *gapx;             // per k-mer position: skip emission of that k-mer
     const Event32 *events;
@@ -88,7 +98,7 @@ struct Args {
     int32_t *status;               // per read
     unsigned int *queue;
     float threshold;
-    int32_t wmax;
+    int32_t wmax;                  // ring width (cells); rings hold wmax + 2 floats per state
     long long spin_limit;          // clock cycles the backward group may wait for a window
 };
 
@@ -137,15 +147,45 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
-// Sequential logAdd over vals[0..n) in index order, exactly as dpDiagonal_dotProduct folds a
-// diagonal one cell at a time (pairwiseAligner.c:1014-1027), run by one warp.  The running result
-// never falls below the running maximum, so a value at least 7.5 below the maximum of the values
-// before it is dropped by logAdd unchanged; only the others are folded, in index order (after being
-// compacted into consecutive lanes so their broadcasts do not depend on the running result).
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sequential logAdd over vals[0..n) in index order, as dpDiagonal_dotProduct folds an
+// anti-diagonal one cell at a time (pairwiseAligner.c:1014-1027), run by one warp.
+//  * The running result never falls below the running maximum, so a value at least 7.5 below the
+//    maximum of the values before it leaves the result unchanged: only the others are folded, in
+//    index order (compacted into consecutive lanes first).
+//  * Values before the first one within kSeedGap of the overall maximum M enter as one exact
+//    log-sum-exp seed: the final result depends on the running result at that point with weight
+//    at most exp(-(kSeedGap - 0.7)) < 1e-6, so the reference's approximation error there (< 1e-3)
+//    cannot reach the final total.
+constexpr float kSeedGap = 15.0f;
+
 __device__ float ordered_fold(const float4 *tab, const float *vals, int n) {
     const int lane = threadIdx.x & 31;
-    float r = kNegInf, carry = kNegInf;
+    float mall = kNegInf;
+    for (int b = 0; b < n; b += 32) mall = fmaxf(mall, b + lane < n ? vals[b + lane] : kNegInf);
+    mall = warp_max(mall);
+    if (!(mall > kNegInf)) return kNegInf;
+    // first index within kSeedGap of the maximum
+    int start = n;
     for (int b = 0; b < n; b += 32) {
+        const unsigned m = __ballot_sync(0xffffffffu, b + lane < n && vals[b + lane] >= mall - kSeedGap);
+        if (m) { start = b + __ffs(m) - 1; break; }
+    }
+    float seed = 0.0f, carry = kNegInf;
+    for (int b = 0; b < start; b += 32) {
+        const float v = b + lane < start ? vals[b + lane] : kNegInf;
+        seed += v > kNegInf ? __expf(v - mall) : 0.0f;
+        carry = fmaxf(carry, v);
+    }
+    seed = warp_sum(seed);
+    carry = warp_max(carry);
+    float r = seed > 0.0f ? mall + __logf(seed) : kNegInf;
+    for (int b = start; b < n; b += 32) {
         const float v = b + lane < n ? vals[b + lane] : kNegInf;
         float incl = v;
 #pragma unroll
@@ -226,29 +266,35 @@ __device__ __forceinline__ void emit_event_pair(const Ctx &c, int32_t kid, const
     }
 }
 
-__device__ __forceinline__ float *slot_ptr(float *ring, int wmax, int slot, int state) {
-    return ring + (slot * 3 + state) * wmax;
+__device__ __forceinline__ int32_t clampi(int32_t v, int32_t lo, int32_t hi) { return min(max(v, lo), hi); }
+
+struct Meta {
+    int32_t L, W, flags;
+};
+
+__device__ __forceinline__ Meta load_meta(const Args &A, int64_t db, int32_t d, int32_t n) {
+    if (d < 0 || d > n) return Meta{0, 0, 0};
+    const int2 m = __ldg(A.meta + db + d);
+    return Meta{m.x, m.y & kWidthMask, m.y & ~kWidthMask};
 }
 
-__device__ __forceinline__ int32_t width_of(int32_t L, int32_t R) { return R >= L ? ((R - L) >> 1) + 1 : 0; }
-
-// is anti-diagonal d a total-probability refresh of its posterior window (pairwiseAligner.c:1370)?
-// The posterior range of window w is (from[w-1], from[w]]; refreshes are from[w], from[w] - 10, ...
-struct RefreshTracker {
-    const Window *win;
-    int32_t n_windows, w, from;
-    __device__ void init(const Window *ws, int32_t nw) {
-        win = ws;
-        n_windows = nw;
-        w = 0;
-        from = nw > 0 ? ws[0].from : 0;
-    }
-    // d must be visited in increasing order
-    __device__ bool is_refresh(int32_t d) {
-        while (d > from && w + 1 < n_windows) from = win[++w].from;
-        return d > 0 && d <= from && (from - d) % 10 == 0;
+// ring: 3 slots x 3 states x (wmax + 2) floats; slot pointers point at cell 0 (cell -1 is a pad)
+struct Ring {
+    float *s[3];   // s[0] = anti-diagonal d (being written), s[1] = d -/+ 1, s[2] = d -/+ 2
+    int stride;    // wmax + 2
+    __device__ float *st(int k, int state) const { return s[k] + state * stride; }
+    __device__ void rotate() {
+        float *t = s[2];
+        s[2] = s[1];
+        s[1] = s[0];
+        s[0] = t;
     }
 };
+
+__device__ __forceinline__ void ring_init(float *base, int wmax, int tid) {
+    const int total = 9 * (wmax + 2);
+    for (int i = tid; i < total; i += kGroup) base[i] = kNegInf;
+}
 
 // ------------------------------------------------------------------------------------------------
 // forward group
@@ -263,28 +309,30 @@ __device__ void forward_region(const Ctx &c, Shared *sh, float *fring) {
     const int wmax = A.wmax;
     const int64_t db = R.diag_base;
     const int32_t n = R.n;
-    float *Freg = A.F + kStoreStride * R.cell_base;
-    auto band_l = [&](int32_t d) -> int32_t { return d <= n ? __ldg(A.xl + db + d) : 0; };
-    auto band_r = [&](int32_t d) -> int32_t { return d <= n ? __ldg(A.xr + db + d) : -2; };
-    const Window *wins = A.windows + R.win_base;
-    RefreshTracker rt;
-    rt.init(wins, R.n_windows);
+    float *Fd = A.F + kStoreStride * R.cell_base;     // store of the anti-diagonal being computed
+
+    ring_init(fring, wmax, tid);
+    group_bar(kBarForward);
+    Ring rg;
+    rg.stride = wmax + 2;
+    // slot of d = 1 is s[0]; s[1] holds d = 0, s[2] holds d = -1 (all -inf)
+    rg.s[1] = fring + 1;
+    rg.s[2] = fring + 3 * rg.stride + 1;
+    rg.s[0] = fring + 6 * rg.stride + 1;
 
     // anti-diagonal 0: startStateProb / raggedStartStateProb (stateMachine.c:1022-1032)
     const float s0 = R.ragged_left ? kNegInf : 0.0f, s1 = R.ragged_left ? 0.0f : kNegInf;
     if (tid == 0) {
-        Freg[ST_M] = s0; Freg[ST_EM] = kNegInf; Freg[ST_EY] = kNegInf; Freg[ST_X] = s1; Freg[ST_Y] = s1;
-        slot_ptr(fring, wmax, 0, 0)[0] = s0;
-        slot_ptr(fring, wmax, 0, 1)[0] = s1;
-        slot_ptr(fring, wmax, 0, 2)[0] = s1;
+        Fd[ST_M] = s0; Fd[ST_EM] = kNegInf; Fd[ST_EY] = kNegInf; Fd[ST_X] = s1; Fd[ST_Y] = s1;
+        rg.st(1, 0)[0] = s0;
+        rg.st(1, 1)[0] = s1;
+        rg.st(1, 2)[0] = s1;
         A.base[db] = 0.0;
         A.fshift[db] = 0.0f;
     }
-    bool ref_cur = rt.is_refresh(0), ref_next = rt.is_refresh(1);
-    // band bounds: d-2, d-1, d, d+1, d+2
-    int32_t L2 = 0, R2 = -2, L1 = band_l(0), R1 = band_r(0);
-    int32_t L0 = band_l(1), R0 = band_r(1), Ln = band_l(2), Rn = band_r(2), Lnn = band_l(3), Rnn = band_r(3);
-    int32_t off0 = 1;   // anti-diagonal 0 has one cell
+    Fd += kStoreStride;   // anti-diagonal 0 has one cell
+    Meta m2{0, 0, 0}, m1 = load_meta(A, db, 0, n), m0 = load_meta(A, db, 1, n);
+    Meta mn = load_meta(A, db, 2, n), mnn = load_meta(A, db, 3, n);
     float eX[CPT], eM[CPT], eY[CPT];          // emissions of the current anti-diagonal's cells
     int32_t kid1[CPT];                        // k-mer ids / events of the next anti-diagonal's cells
     Event32 ev1[CPT];
@@ -292,66 +340,49 @@ __device__ void forward_region(const Ctx &c, Shared *sh, float *fring) {
     int32_t kid2[CPT];                        // ... and of the one after
     Event32 ev2[CPT];
     bool hev2[CPT];
-    auto cell_xy = [&](int32_t d, int32_t L, int i, int32_t &x, int32_t &y) {
-        const int32_t xmy = L + 2 * i;
-        x = (d + xmy) >> 1;
-        y = (d - xmy) >> 1;
-    };
-    {
-        const int32_t W0 = width_of(L0, R0), Wn = width_of(Ln, Rn);
 #pragma unroll
-        for (int j = 0; j < CPT; ++j) {
-            const int i = tid + j * kGroup;
-            int32_t x = 0, y = 0;
-            eX[j] = eM[j] = eY[j] = kNegInf;
-            if (i < W0) {
-                cell_xy(1, L0, i, x, y);
-                const int32_t kid = load_kid(c, x);
-                const KmerConst32 kc = load_kc(c, kid);
-                emit_event_pair(c, kid, kc, load_event(c, y - 1), y >= 1, eM[j], eY[j]);
-                eX[j] = c.hdp ? (kid >= 0 ? (float) kLogPointOne : kNegInf) : kc.gapx;
-            }
-            kid1[j] = -1; hev1[j] = false; ev1[j] = Event32{0, 1, 0, 1};
-            if (i < Wn) {
-                cell_xy(2, Ln, i, x, y);
-                kid1[j] = load_kid(c, x);
-                ev1[j] = load_event(c, y - 1);
-                hev1[j] = y >= 1;
-            }
+    for (int j = 0; j < CPT; ++j) {
+        const int i = tid + j * kGroup;
+        eX[j] = eM[j] = eY[j] = kNegInf;
+        if (i < m0.W) {
+            const int32_t xmy = m0.L + 2 * i, x = (1 + xmy) >> 1, y = (1 - xmy) >> 1;
+            const int32_t kid = load_kid(c, x);
+            const KmerConst32 kc = load_kc(c, kid);
+            emit_event_pair(c, kid, kc, load_event(c, y - 1), y >= 1, eM[j], eY[j]);
+            eX[j] = c.hdp ? (kid >= 0 ? (float) kLogPointOne : kNegInf) : kc.gapx;
+        }
+        kid1[j] = -1; hev1[j] = false; ev1[j] = Event32{0, 1, 0, 1};
+        if (i < mn.W) {
+            const int32_t xmy = mn.L + 2 * i, x = (2 + xmy) >> 1, y = (2 - xmy) >> 1;
+            kid1[j] = load_kid(c, x);
+            ev1[j] = load_event(c, y - 1);
+            hev1[j] = y >= 1;
         }
     }
     float lm_prev = tid == 0 ? fmaxf(s0, s1) : kNegInf;   // local max of the previous anti-diagonal
     float delta1 = 0.0f;      // base(d-1) - base(d-2)
-    double fbase = 0.0;       // base of d-1, then of d
+    double fbase = 0.0;       // base of d
     int32_t wi = 0;
-    int32_t wD = wins[0].D;
+    group_bar(kBarForward);
     for (int32_t d = 1; d <= n; ++d) {
         // shift of this anti-diagonal: base(d) = base(d-2) + max(d-2)
         float delta0 = 0.0f;
         if (d > 2) {
-            float m = sh->fpart[(d - 2) % 3][0];
-#pragma unroll
-            for (int w = 1; w < kGroupWarps; ++w) m = fmaxf(m, sh->fpart[(d - 2) % 3][w]);
-            delta0 = (m > kNegInf ? m : 0.0f) - delta1;
+            const float *fp = sh->fpart[(d - 2) % 3];
+            const float mx = fmaxf(fmaxf(fp[0], fp[1]), fmaxf(fp[2], fp[3]));
+            delta0 = (mx > kNegInf ? mx : 0.0f) - delta1;
         }
         fbase += (double) delta0;
-        ref_cur = ref_next;
-        ref_next = rt.is_refresh(d + 1);
-        const bool store_gaps = ref_cur || ref_next;
-        const int32_t L3 = band_l(d + 3), R3 = band_r(d + 3);
+        const Meta m3 = load_meta(A, db, d + 3, n);
         // stage 1: ids and events two anti-diagonals ahead
-        const int32_t Wnn = width_of(Lnn, Rnn);
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             const int i = tid + j * kGroup;
-            kid2[j] = -1; hev2[j] = false; ev2[j] = Event32{0, 1, 0, 1};
-            if (i < Wnn) {
-                int32_t x, y;
-                cell_xy(d + 2, Lnn, i, x, y);
-                kid2[j] = load_kid(c, x);
-                ev2[j] = load_event(c, y - 1);
-                hev2[j] = y >= 1;
-            }
+            const int32_t xmy = mnn.L + 2 * i, x = (d + 2 + xmy) >> 1, y = (d + 2 - xmy) >> 1;
+            const bool in = i < mnn.W;
+            kid2[j] = in ? load_kid(c, x) : -1;
+            ev2[j] = load_event(c, in ? y - 1 : -1);
+            hev2[j] = in && y >= 1;
         }
         // stage 2: k-mer constants one anti-diagonal ahead
         KmerConst32 kc1[CPT];
@@ -359,46 +390,39 @@ __device__ void forward_region(const Ctx &c, Shared *sh, float *fring) {
         for (int j = 0; j < CPT; ++j) kc1[j] = load_kc(c, kid1[j]);
         // the recursion on anti-diagonal d (stateMachine3_cellCalculate order: lower -> gap-X,
         // middle -> match, upper -> gap-Y, each state accumulated from LOG_ZERO)
-        const int32_t W0 = width_of(L0, R0);
-        const int sl = d % 3, s1l = (d + 2) % 3, s2l = (d + 1) % 3;
+        const int32_t W0 = m0.W;
         const float shL = -delta0, shM = -delta1 - delta0;
-        float *Fd = Freg + kStoreStride * off0;
+        const bool store_gaps = (m0.flags & kFlagStoreGaps) != 0;
         float lm = kNegInf;
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             const int i = tid + j * kGroup;
-            if (i >= W0) break;
-            const int32_t xmy = L0 + 2 * i;
-            float vM = kNegInf, vX = kNegInf, vY = kNegInf;
-            if (xmy - 1 >= L1 && xmy - 1 <= R1) {
-                const int il = (xmy - 1 - L1) >> 1;
-                const float e = eX[j] + shL;
-                vX = slot_ptr(fring, wmax, s1l, 0)[il] + (e + t[T_OX]);
-                vX = lae(tab, vX, slot_ptr(fring, wmax, s1l, 1)[il] + (e + t[T_EX]));
-                vX = lae(tab, vX, slot_ptr(fring, wmax, s1l, 2)[il] + (e + t[T_SX]));
-            }
-            if (xmy >= L2 && xmy <= R2) {
-                const int im = (xmy - L2) >> 1;
-                const float e = eM[j] + shM;
-                vM = slot_ptr(fring, wmax, s2l, 0)[im] + (e + t[T_MC]);
-                vM = lae(tab, vM, slot_ptr(fring, wmax, s2l, 1)[im] + (e + t[T_MFGX]));
-                vM = lae(tab, vM, slot_ptr(fring, wmax, s2l, 2)[im] + (e + t[T_MFGY]));
-            }
-            if (xmy + 1 >= L1 && xmy + 1 <= R1) {
-                const int iu = (xmy + 1 - L1) >> 1;
-                const float e = eY[j] + shL;
-                vY = slot_ptr(fring, wmax, s1l, 0)[iu] + (e + t[T_OY]);
-                vY = lae(tab, vY, slot_ptr(fring, wmax, s1l, 2)[iu] + (e + t[T_EY]));
-            }
-            slot_ptr(fring, wmax, sl, 0)[i] = vM;
-            slot_ptr(fring, wmax, sl, 1)[i] = vX;
-            slot_ptr(fring, wmax, sl, 2)[i] = vY;
-            Fd[ST_M * W0 + i] = vM;
-            Fd[ST_EM * W0 + i] = eM[j];
-            Fd[ST_EY * W0 + i] = eY[j];
-            if (store_gaps) {
-                Fd[ST_X * W0 + i] = vX;
-                Fd[ST_Y * W0 + i] = vY;
+            const int32_t xmy = m0.L + 2 * i;
+            const int il = clampi((xmy - 1 - m1.L) >> 1, -1, wmax);
+            const int iu = clampi((xmy + 1 - m1.L) >> 1, -1, wmax);
+            const int im = clampi((xmy - m2.L) >> 1, -1, wmax);
+            const float ex = eX[j] + shL, em = eM[j] + shM, ey = eY[j] + shL;
+            float vX = rg.st(1, 0)[il] + (ex + t[T_OX]);
+            vX = lae(tab, vX, rg.st(1, 1)[il] + (ex + t[T_EX]));
+            vX = lae(tab, vX, rg.st(1, 2)[il] + (ex + t[T_SX]));
+            float vM = rg.st(2, 0)[im] + (em + t[T_MC]);
+            vM = lae(tab, vM, rg.st(2, 1)[im] + (em + t[T_MFGX]));
+            vM = lae(tab, vM, rg.st(2, 2)[im] + (em + t[T_MFGY]));
+            float vY = rg.st(1, 0)[iu] + (ey + t[T_OY]);
+            vY = lae(tab, vY, rg.st(1, 2)[iu] + (ey + t[T_EY]));
+            const bool in = i < W0;
+            if (!in) vM = vX = vY = kNegInf;
+            rg.st(0, 0)[i] = vM;
+            rg.st(0, 1)[i] = vX;
+            rg.st(0, 2)[i] = vY;
+            if (in) {
+                Fd[ST_M * W0 + i] = vM;
+                Fd[ST_EM * W0 + i] = eM[j];
+                Fd[ST_EY * W0 + i] = eY[j];
+                if (store_gaps) {
+                    Fd[ST_X * W0 + i] = vX;
+                    Fd[ST_Y * W0 + i] = vY;
+                }
             }
             lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
         }
@@ -408,34 +432,25 @@ __device__ void forward_region(const Ctx &c, Shared *sh, float *fring) {
             if (lane == 0) sh->fpart[(d - 1) % 3][warp] = wm;
         }
         // emissions of the next anti-diagonal's cells
-        const int32_t Wn = width_of(Ln, Rn);
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
-            const int i = tid + j * kGroup;
-            if (i < Wn) {
-                emit_event_pair(c, kid1[j], kc1[j], ev1[j], hev1[j], eM[j], eY[j]);
-                eX[j] = c.hdp ? (kid1[j] >= 0 ? (float) kLogPointOne : kNegInf) : kc1[j].gapx;
-            } else {
-                eM[j] = eY[j] = eX[j] = kNegInf;
-            }
+            emit_event_pair(c, kid1[j], kc1[j], ev1[j], hev1[j], eM[j], eY[j]);
+            eX[j] = c.hdp ? (kid1[j] >= 0 ? (float) kLogPointOne : kNegInf) : kc1[j].gapx;
             kid1[j] = kid2[j]; ev1[j] = ev2[j]; hev1[j] = hev2[j];
         }
         if (tid == 0) {
             A.base[db + d] = fbase;
             A.fshift[db + d] = delta0;
         }
-        const bool window_end = d == wD;
+        const bool window_end = (m0.flags & kFlagWindowEnd) != 0;
         if (window_end) __threadfence_block();
         group_bar(kBarForward);
-        if (window_end) {
-            if (tid == 0) atomicExch(&sh->fwd_done, wi + 1);
-            ++wi;
-            if (wi < R.n_windows) wD = wins[wi].D;
-        }
+        if (window_end && tid == 0) atomicExch(&sh->fwd_done, ++wi);
         lm_prev = lm;
         delta1 = delta0;
-        off0 += W0;
-        L2 = L1; R2 = R1; L1 = L0; R1 = R0; L0 = Ln; R0 = Rn; Ln = Lnn; Rn = Rnn; Lnn = L3; Rnn = R3;
+        Fd += kStoreStride * W0;
+        rg.rotate();
+        m2 = m1; m1 = m0; m0 = mn; mn = mnn; mnn = m3;
     }
 }
 
@@ -487,10 +502,9 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
     const int64_t db = R.diag_base;
     const int32_t n = R.n;
     const float *Freg = A.F + kStoreStride * R.cell_base;
-    auto band_l = [&](int32_t d) -> int32_t { return (d >= 0 && d <= n) ? __ldg(A.xl + db + d) : 0; };
-    auto band_r = [&](int32_t d) -> int32_t { return (d >= 0 && d <= n) ? __ldg(A.xr + db + d) : -2; };
     int64_t n_out = 0;
     double ll = 0.0;
+    ring_init(bring, wmax, tid);
     for (int32_t wi = 0; wi < R.n_windows; ++wi) {
         const Window W = A.windows[R.win_base + wi];
         // wait (bounded) for the forward group to pass this window's traceback anti-diagonal
@@ -518,18 +532,24 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
         const float e2 = ragged_end ? t[T_EY] : t[T_MFGY];
         float mxD = fmaxf(e0, fmaxf(e1, e2));
         if (!(mxD > kNegInf)) mxD = 0.0f;
-        // bands of d+2, d+1, d, d-1, d-2 and forward-store offsets of d+2, d+1, d (d = D to start)
-        int32_t Lpp = 0, Rpp = -2, Lp = 0, Rp = -2;
-        int32_t L0 = band_l(D), R0 = band_r(D), Lm = band_l(D - 1), Rm = band_r(D - 1), Lmm = band_l(D - 2),
-                Rmm = band_r(D - 2);
-        int32_t off0 = (int32_t) __ldcg(A.coff + db + D), offp = 0, offpp = 0;
-        {
-            const int32_t W0 = width_of(L0, R0);
-            for (int i = tid; i < W0; i += kGroup) {
-                slot_ptr(bring, wmax, D % 3, 0)[i] = e0;
-                slot_ptr(bring, wmax, D % 3, 1)[i] = e1;
-                slot_ptr(bring, wmax, D % 3, 2)[i] = e2;
-            }
+        Ring rg;
+        rg.stride = wmax + 2;
+        rg.s[0] = bring + 1;                      // d = D
+        rg.s[1] = bring + 3 * rg.stride + 1;      // d + 1 (none yet: -inf)
+        rg.s[2] = bring + 6 * rg.stride + 1;      // d + 2
+        // metas of d+2, d+1, d, d-1, d-2 (d = D to start) and store offsets of d+2, d+1, d
+        Meta mpp{0, 0, 0}, mp{0, 0, 0};
+        Meta m0 = load_meta(A, db, D, n), mm = load_meta(A, db, D - 1, n), mmm = load_meta(A, db, D - 2, n);
+        int32_t off0 = __ldg(A.window_off + R.win_base + wi), offp = off0, offpp = off0;
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+            const int i = tid + j * kGroup;
+            const bool in = i < m0.W;
+            rg.st(0, 0)[i] = in ? e0 : kNegInf;
+            rg.st(0, 1)[i] = in ? e1 : kNegInf;
+            rg.st(0, 2)[i] = in ? e2 : kNegInf;
+            rg.st(1, 0)[i] = kNegInf; rg.st(1, 1)[i] = kNegInf; rg.st(1, 2)[i] = kNegInf;
+            rg.st(2, 0)[i] = kNegInf; rg.st(2, 1)[i] = kNegInf; rg.st(2, 2)[i] = kNegInf;
         }
         // operands of the current anti-diagonal's cells, loaded one anti-diagonal ahead
         float eMm[CPT], eYu[CPT], eXl[CPT], fM[CPT];
@@ -537,18 +557,17 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
         float fX[CPT], fY[CPT], tM[CPT], tX[CPT], tY[CPT], tE[CPT];
         double fb = __ldcg(A.base + db + D);
         float fsh = __ldcg(A.fshift + db + D);
-        const int32_t W0D = width_of(L0, R0);
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             const int i = tid + j * kGroup;
+            const int ic = min(i, max(m0.W - 1, 0));
+            const float *Fd = Freg + kStoreStride * off0;
+            const bool post = D <= from && i < m0.W;
             eMm[j] = eYu[j] = eXl[j] = kNegInf;
-            fM[j] = fX[j] = fY[j] = tM[j] = tX[j] = tY[j] = tE[j] = kNegInf;
-            if (i < W0D && D <= from) {
-                const float *Fd = Freg + kStoreStride * off0;
-                fM[j] = __ldcg(Fd + ST_M * W0D + i);
-                fX[j] = __ldcg(Fd + ST_X * W0D + i);
-                fY[j] = __ldcg(Fd + ST_Y * W0D + i);
-            }
+            fM[j] = post ? __ldcg(Fd + ST_M * m0.W + ic) : kNegInf;
+            fX[j] = post ? __ldcg(Fd + ST_X * m0.W + ic) : kNegInf;
+            fY[j] = post ? __ldcg(Fd + ST_Y * m0.W + ic) : kNegInf;
+            tM[j] = tX[j] = tY[j] = tE[j] = kNegInf;
         }
         float lm_prev = kNegInf;           // local max of B stored on d+1 (lagged reduction)
         float gamma1 = 0.0f;               // base(d+1) - base(d+2)
@@ -560,65 +579,59 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
         int32_t pend_d = -1;
         group_bar(kBarBackward);
         for (int32_t d = D; d > T; --d) {
-            const int sl = d % 3, sp = (d + 1) % 3, spp = (d + 2) % 3;
-            const int32_t W0 = width_of(L0, R0);
+            const int32_t W0 = m0.W, Wp = mp.W;
             const bool post = d <= from;
-            const bool refresh = post && (from - d) % 10 == 0;
+            const bool refresh = post && (m0.flags & kFlagRefresh);
             float gamma0 = 0.0f;           // base(d) - base(d+1)
             if (d <= D - 2) {
                 float m;
                 if (d == D - 2) {
                     m = mxD;
                 } else {
-                    m = sh->bpart[(d + 2) % 3][0];
-#pragma unroll
-                    for (int w = 1; w < kGroupWarps; ++w) m = fmaxf(m, sh->bpart[(d + 2) % 3][w]);
+                    const float *bp = sh->bpart[(d + 2) % 3];
+                    m = fmaxf(fmaxf(bp[0], bp[1]), fmaxf(bp[2], bp[3]));
                     if (!(m > kNegInf)) m = 0.0f;
                 }
                 gamma0 = m - gamma1;
             }
             bbase += (double) gamma0;
-            // prefetch the operands of the d-1 cells
-            const int32_t L3 = band_l(d - 3), R3 = band_r(d - 3);
-            const int32_t Wm = width_of(Lm, Rm), Wp = width_of(Lp, Rp);
-            const int32_t offm = off0 - Wm;
-            const bool post_m = d - 1 <= from && d - 1 > T;
-            const bool refresh_m = post_m && (from - (d - 1)) % 10 == 0;
+            // prefetch the operands of the d-1 cells (indices clamped into the owning anti-diagonal:
+            // a value fetched for an absent neighbour is only ever added to a -inf ring value)
+            const Meta m3 = load_meta(A, db, d - 3, n);
+            const int32_t Wm = mm.W, Wmm = mmm.W;
+            const int32_t offm = off0 - Wm, offmm = offm - Wmm;
+            const bool live_m = d - 1 > T;
+            const bool post_m = live_m && d - 1 <= from;
+            const bool refresh_m = post_m && (mm.flags & kFlagRefresh);
             float eMm_n[CPT], eYu_n[CPT], eXl_n[CPT], fM_n[CPT], fX_n[CPT], fY_n[CPT];
             float tM_n[CPT], tX_n[CPT], tY_n[CPT], tE_n[CPT];
             {
-                const float *Fd = Freg + kStoreStride * off0;      // d (the d-1 cells' "d+1")
-                const float *Fp = Freg + kStoreStride * offp;      // d+1 (the d-1 cells' "d+2")
+                const float *Fd = Freg + kStoreStride * off0;      // d
+                const float *Fp = Freg + kStoreStride * offp;      // d+1
                 const float *Fm = Freg + kStoreStride * offm;      // d-1
-                const float *Fmm = Freg + kStoreStride * (offm - width_of(Lmm, Rmm));   // d-2
+                const float *Fmm = Freg + kStoreStride * offmm;    // d-2
 #pragma unroll
                 for (int j = 0; j < CPT; ++j) {
                     const int i = tid + j * kGroup;
-                    eMm_n[j] = eYu_n[j] = eXl_n[j] = fM_n[j] = fX_n[j] = fY_n[j] = kNegInf;
-                    tM_n[j] = tX_n[j] = tY_n[j] = tE_n[j] = kNegInf;
-                    if (i < Wm && d - 1 > T) {
-                        const int32_t xmy = Lm + 2 * i, x = (d - 1 + xmy) >> 1;
-                        if (d + 1 <= D && xmy >= Lp && xmy <= Rp) eMm_n[j] = __ldcg(Fp + ST_EM * Wp + ((xmy - Lp) >> 1));
-                        if (xmy - 1 >= L0 && xmy - 1 <= R0) eYu_n[j] = __ldcg(Fd + ST_EY * W0 + ((xmy - 1 - L0) >> 1));
-                        if (xmy + 1 >= L0 && xmy + 1 <= R0) eXl_n[j] = load_gapx(c, x + 1);
-                        if (post_m) fM_n[j] = __ldcg(Fm + ST_M * Wm + i);
-                        if (refresh_m) {
-                            fX_n[j] = __ldcg(Fm + ST_X * Wm + i);
-                            fY_n[j] = __ldcg(Fm + ST_Y * Wm + i);
-                        }
-                    }
-                    // match-through inputs for a refresh at d-1: the cells of d, F of d-2, emissions of d
-                    if (refresh_m && i < W0) {
-                        const int32_t xmy = L0 + 2 * i;
-                        const int32_t Wmm = width_of(Lmm, Rmm);
-                        tE_n[j] = __ldcg(Fd + ST_EM * W0 + i);
-                        if (xmy >= Lmm && xmy <= Rmm && d - 2 >= 0) {
-                            const int im = (xmy - Lmm) >> 1;
-                            tM_n[j] = __ldcg(Fmm + ST_M * Wmm + im);
-                            tX_n[j] = __ldcg(Fmm + ST_X * Wmm + im);
-                            tY_n[j] = __ldcg(Fmm + ST_Y * Wmm + im);
-                        }
-                    }
+                    const int32_t xmy = mm.L + 2 * i, x = (d - 1 + xmy) >> 1;
+                    const bool in = live_m && i < Wm;
+                    const bool has_p = d + 1 <= D && Wp > 0;
+                    eMm_n[j] = in && has_p ? __ldcg(Fp + ST_EM * Wp + clampi((xmy - mp.L) >> 1, 0, Wp - 1)) : kNegInf;
+                    eYu_n[j] = in && W0 > 0 ? __ldcg(Fd + ST_EY * W0 + clampi((xmy - 1 - m0.L) >> 1, 0, W0 - 1)) : kNegInf;
+                    eXl_n[j] = in ? load_gapx(c, x + 1) : kNegInf;
+                    const int ic = min(i, max(Wm - 1, 0));
+                    fM_n[j] = post_m && i < Wm ? __ldcg(Fm + ST_M * Wm + ic) : kNegInf;
+                    fX_n[j] = refresh_m && i < Wm ? __ldcg(Fm + ST_X * Wm + ic) : kNegInf;
+                    fY_n[j] = refresh_m && i < Wm ? __ldcg(Fm + ST_Y * Wm + ic) : kNegInf;
+                    // match-through inputs for a refresh at d-1: cells of d, F of d-2, emissions of d
+                    const bool thr = refresh_m && i < W0;
+                    const int32_t xmy0 = m0.L + 2 * i;
+                    const bool has_mm = thr && Wmm > 0 && xmy0 >= mmm.L && ((xmy0 - mmm.L) >> 1) < Wmm && d - 2 >= 0;
+                    const int imm = clampi((xmy0 - mmm.L) >> 1, 0, max(Wmm - 1, 0));
+                    tE_n[j] = thr ? __ldcg(Fd + ST_EM * W0 + min(i, W0 - 1)) : kNegInf;
+                    tM_n[j] = has_mm ? __ldcg(Fmm + ST_M * Wmm + imm) : kNegInf;
+                    tX_n[j] = has_mm ? __ldcg(Fmm + ST_X * Wmm + imm) : kNegInf;
+                    tY_n[j] = has_mm ? __ldcg(Fmm + ST_Y * Wmm + imm) : kNegInf;
                 }
             }
             const double fb_n = d - 1 >= 0 ? __ldcg(A.base + db + d - 1) : 0.0;
@@ -630,32 +643,28 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
 #pragma unroll
                 for (int j = 0; j < CPT; ++j) {
                     const int i = tid + j * kGroup;
-                    if (i >= W0) break;
-                    const int32_t xmy = L0 + 2 * i;
-                    float vM = kNegInf, vX = kNegInf, vY = kNegInf;
-                    if (d + 2 <= D && xmy >= Lpp && xmy <= Rpp) {
-                        const float bm = slot_ptr(bring, wmax, spp, 0)[(xmy - Lpp) >> 1];
-                        const float e = eMm[j] + shM;
-                        vM = bm + (e + t[T_MC]);
-                        vX = bm + (e + t[T_MFGX]);
-                        vY = bm + (e + t[T_MFGY]);
-                    }
-                    if (xmy - 1 >= Lp && xmy - 1 <= Rp) {
-                        const float bu = slot_ptr(bring, wmax, sp, 2)[(xmy - 1 - Lp) >> 1];
-                        const float e = eYu[j] + shU;
-                        vM = lae(tab, vM, bu + (e + t[T_OY]));
-                        vY = lae(tab, vY, bu + (e + t[T_EY]));
-                    }
-                    if (xmy + 1 >= Lp && xmy + 1 <= Rp) {
-                        const float bl = slot_ptr(bring, wmax, sp, 1)[(xmy + 1 - Lp) >> 1];
-                        const float e = eXl[j] + shU;
-                        vM = lae(tab, vM, bl + (e + t[T_OX]));
-                        vX = lae(tab, vX, bl + (e + t[T_EX]));
-                        vY = lae(tab, vY, bl + (e + t[T_SX]));
-                    }
-                    slot_ptr(bring, wmax, sl, 0)[i] = vM;
-                    slot_ptr(bring, wmax, sl, 1)[i] = vX;
-                    slot_ptr(bring, wmax, sl, 2)[i] = vY;
+                    const int32_t xmy = m0.L + 2 * i;
+                    const int ipp = clampi((xmy - mpp.L) >> 1, -1, wmax);
+                    const int iu = clampi((xmy - 1 - mp.L) >> 1, -1, wmax);
+                    const int il = clampi((xmy + 1 - mp.L) >> 1, -1, wmax);
+                    const float bm = rg.st(2, 0)[ipp];
+                    const float em = eMm[j] + shM;
+                    float vM = bm + (em + t[T_MC]);
+                    float vX = bm + (em + t[T_MFGX]);
+                    float vY = bm + (em + t[T_MFGY]);
+                    const float bu = rg.st(1, 2)[iu];
+                    const float ey = eYu[j] + shU;
+                    vM = lae(tab, vM, bu + (ey + t[T_OY]));
+                    vY = lae(tab, vY, bu + (ey + t[T_EY]));
+                    const float bl = rg.st(1, 1)[il];
+                    const float ex = eXl[j] + shU;
+                    vM = lae(tab, vM, bl + (ex + t[T_OX]));
+                    vX = lae(tab, vX, bl + (ex + t[T_EX]));
+                    vY = lae(tab, vY, bl + (ex + t[T_SX]));
+                    if (i >= W0) vM = vX = vY = kNegInf;
+                    rg.st(0, 0)[i] = vM;
+                    rg.st(0, 1)[i] = vX;
+                    rg.st(0, 2)[i] = vY;
                     lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
                 }
             }
@@ -678,9 +687,9 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
                     for (int j = 0; j < CPT; ++j) {
                         const int i = tid + j * kGroup;
                         if (i < W0) {
-                            float s = fM[j] + slot_ptr(bring, wmax, sl, 0)[i];
-                            s = lae(tab, s, fX[j] + slot_ptr(bring, wmax, sl, 1)[i]);
-                            s = lae(tab, s, fY[j] + slot_ptr(bring, wmax, sl, 2)[i]);
+                            float s = fM[j] + rg.st(0, 0)[i];
+                            s = lae(tab, s, fX[j] + rg.st(0, 1)[i]);
+                            s = lae(tab, s, fY[j] + rg.st(0, 2)[i]);
                             chain[i] = s;
                         }
                     }
@@ -690,10 +699,10 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
                         for (int j = 0; j < CPT; ++j) {
                             const int i = tid + j * kGroup;
                             if (i < Wp) {
-                                float m = tM[j] + (tE[j] + t[T_MC]);
-                                m = lae(tab, m, tX[j] + (tE[j] + t[T_MFGX]));
-                                m = lae(tab, m, tY[j] + (tE[j] + t[T_MFGY]));
-                                chain[wmax + i] = m + slot_ptr(bring, wmax, sp, 0)[i];
+                                float mth = tM[j] + (tE[j] + t[T_MC]);
+                                mth = lae(tab, mth, tX[j] + (tE[j] + t[T_MFGX]));
+                                mth = lae(tab, mth, tY[j] + (tE[j] + t[T_MFGY]));
+                                chain[wmax + i] = mth + rg.st(1, 0)[i];
                             }
                         }
                     }
@@ -715,19 +724,12 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
 #pragma unroll
                 for (int j = 0; j < CPT; ++j) {
                     const int i = tid + j * kGroup;
-                    bool hit = false;
-                    if (i < W0) {
-                        const int32_t xmy = L0 + 2 * i, x = (d + xmy) >> 1, y = (d - xmy) >> 1;
-                        if (x > 0 && y > 0) {
-                            const float p = __expf(fM[j] + slot_ptr(bring, wmax, sl, 0)[i] + kd);
-                            if (p >= A.threshold) {
-                                hit = true;
-                                pv[j] = p;
-                                px[j] = x;
-                                py[j] = y;
-                            }
-                        }
-                    }
+                    const int32_t xmy = m0.L + 2 * i, x = (d + xmy) >> 1, y = (d - xmy) >> 1;
+                    const float p = __expf(fM[j] + rg.st(0, 0)[i] + kd);
+                    const bool hit = i < W0 && x > 0 && y > 0 && p >= A.threshold;
+                    pv[j] = p;
+                    px[j] = x;
+                    py[j] = y;
                     const unsigned bal = __ballot_sync(0xffffffffu, hit);
                     if (hit) pend |= 1u << j;
                     if (lane == 0) sh->wcnt[d & 1][j][warp] = __popc(bal);
@@ -745,7 +747,9 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
             lm_prev = d == D ? kNegInf : lm;   // D's maximum is known exactly (mxD)
             gamma1 = gamma0;
             offpp = offp; offp = off0; off0 = offm;
-            Lpp = Lp; Rpp = Rp; Lp = L0; Rp = R0; L0 = Lm; R0 = Rm; Lm = Lmm; Rm = Rmm; Lmm = L3; Rmm = R3;
+            rg.rotate();
+            // after rotate: s[0] takes the old d+2 slot, which becomes d-1
+            mpp = mp; mp = m0; m0 = mm; mm = mmm; mmm = m3;
         }
         // flush the last anti-diagonal's pairs
         group_bar(kBarBackward);
@@ -764,8 +768,8 @@ __global__ void __launch_bounds__(kThreads) batch_kernel(const __grid_constant__
     extern __shared__ float4 smem_raw[];
     Shared *sh = reinterpret_cast<Shared *>(smem_raw);
     float *fring = reinterpret_cast<float *>(sh + 1);
-    float *bring = fring + 9 * A.wmax;
-    float *chain = bring + 9 * A.wmax;
+    float *bring = fring + 9 * (A.wmax + 2);
+    float *chain = bring + 9 * (A.wmax + 2);
     if (threadIdx.x < 16) log_add_piece(threadIdx.x, sh->la[threadIdx.x]);
     for (;;) {
         if (threadIdx.x == 0) {
