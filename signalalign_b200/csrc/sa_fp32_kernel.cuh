@@ -254,6 +254,8 @@ __device__ __forceinline__ KmerConst32 load_kc(const Ctx &c, int32_t kid) {
     return KmerConst32{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 }
 
+__device__ __forceinline__ Event32 as_event(float4 v) { return Event32{v.x, v.y, v.z, v.w}; }
+
 // match / extra-event emissions of k-mer kid (constants k) against event ev
 __device__ __forceinline__ void emit_event_pair(const Ctx &c, int32_t kid, const KmerConst32 &k, const Event32 &ev,
                                                 bool have_event, float &em, float &ey) {
@@ -268,9 +270,41 @@ __device__ __forceinline__ void emit_event_pair(const Ctx &c, int32_t kid, const
 
 __device__ __forceinline__ int32_t clampi(int32_t v, int32_t lo, int32_t hi) { return min(max(v, lo), hi); }
 
+// Raw loads: always from a valid address (indices clamped into the region's arrays), never
+// followed by a select on the loaded value.  Validity is computed from indices alone and applied
+// where the value is consumed, one anti-diagonal later, so the load latency overlaps a whole step.
+__device__ __forceinline__ int32_t raw_kid(const Ctx &c, int32_t x) {
+    const int64_t at = c.R.lX > 0 ? c.R.kmer_base + clampi(x - 1, 0, c.R.lX - 1) : 0;
+    return __ldg(c.A->kmer + at);
+}
+
+__device__ __forceinline__ float raw_gapx(const Ctx &c, int32_t x) {
+    const int64_t at = c.R.lX > 0 ? c.R.kmer_base + clampi(x - 1, 0, c.R.lX - 1) : 0;
+    return __ldg(c.A->gapx + at);
+}
+
+__device__ __forceinline__ float4 raw_event(const Ctx &c, int32_t yi) {
+    const int64_t at = c.R.lY > 0 ? c.R.event_base + clampi(yi, 0, c.R.lY - 1) : 0;
+    return __ldg(reinterpret_cast<const float4 *>(c.A->events + at));
+}
+
+__device__ __forceinline__ KmerConst32 raw_kc(const Ctx &c, int32_t kid) {
+    const float4 *p = reinterpret_cast<const float4 *>(c.M->kc + max(kid, 0));
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    return KmerConst32{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+}
+
+__device__ __forceinline__ int2 raw_meta(const Args &A, int64_t db, int32_t d, int32_t n) {
+    return __ldg(A.meta + db + clampi(d, 0, n));
+}
+
 struct Meta {
     int32_t L, W, flags;
 };
+
+__device__ __forceinline__ Meta decode_meta(int2 m, bool exists) {
+    return exists ? Meta{m.x, m.y & kWidthMask, m.y & ~kWidthMask} : Meta{0, 0, 0};
+}
 
 __device__ __forceinline__ Meta load_meta(const Args &A, int64_t db, int32_t d, int32_t n) {
     if (d < 0 || d > n) return Meta{0, 0, 0};
@@ -331,32 +365,33 @@ __device__ void forward_region(const Ctx &c, Shared *sh, float *fring) {
         A.fshift[db] = 0.0f;
     }
     Fd += kStoreStride;   // anti-diagonal 0 has one cell
-    Meta m2{0, 0, 0}, m1 = load_meta(A, db, 0, n), m0 = load_meta(A, db, 1, n);
-    Meta mn = load_meta(A, db, 2, n), mnn = load_meta(A, db, 3, n);
+    Meta m2{0, 0, 0};
+    Meta m1 = decode_meta(raw_meta(A, db, 0, n), true), m0 = decode_meta(raw_meta(A, db, 1, n), 1 <= n);
+    Meta mn = decode_meta(raw_meta(A, db, 2, n), 2 <= n);
+    int2 raw_nn = raw_meta(A, db, 3, n);      // meta of d+2, decoded at the top of each step
     float eX[CPT], eM[CPT], eY[CPT];          // emissions of the current anti-diagonal's cells
-    int32_t kid1[CPT];                        // k-mer ids / events of the next anti-diagonal's cells
-    Event32 ev1[CPT];
-    bool hev1[CPT];
-    int32_t kid2[CPT];                        // ... and of the one after
-    Event32 ev2[CPT];
-    bool hev2[CPT];
+    // raw id / event of the next anti-diagonal's cells, with their validity
+    int32_t rk1[CPT];
+    float4 re1[CPT];
+    bool vx1[CPT], vy1[CPT];
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
         const int i = tid + j * kGroup;
-        eX[j] = eM[j] = eY[j] = kNegInf;
-        if (i < m0.W) {
+        {
             const int32_t xmy = m0.L + 2 * i, x = (1 + xmy) >> 1, y = (1 - xmy) >> 1;
-            const int32_t kid = load_kid(c, x);
-            const KmerConst32 kc = load_kc(c, kid);
-            emit_event_pair(c, kid, kc, load_event(c, y - 1), y >= 1, eM[j], eY[j]);
-            eX[j] = c.hdp ? (kid >= 0 ? (float) kLogPointOne : kNegInf) : kc.gapx;
+            const bool in = i < m0.W;
+            const int32_t kid = in && x >= 1 && x <= R.lX ? raw_kid(c, x) : -1;
+            const KmerConst32 kc = raw_kc(c, kid);
+            emit_event_pair(c, kid, kc, as_event(raw_event(c, y - 1)), in && y >= 1, eM[j], eY[j]);
+            eX[j] = kid < 0 ? kNegInf : (c.hdp ? (float) kLogPointOne : kc.gapx);
         }
-        kid1[j] = -1; hev1[j] = false; ev1[j] = Event32{0, 1, 0, 1};
-        if (i < mn.W) {
+        {
             const int32_t xmy = mn.L + 2 * i, x = (2 + xmy) >> 1, y = (2 - xmy) >> 1;
-            kid1[j] = load_kid(c, x);
-            ev1[j] = load_event(c, y - 1);
-            hev1[j] = y >= 1;
+            const bool in = i < mn.W;
+            rk1[j] = raw_kid(c, x);
+            re1[j] = raw_event(c, y - 1);
+            vx1[j] = in && x >= 1 && x <= R.lX;
+            vy1[j] = in && y >= 1;
         }
     }
     float lm_prev = tid == 0 ? fmaxf(s0, s1) : kNegInf;   // local max of the previous anti-diagonal
@@ -373,21 +408,30 @@ __device__ void forward_region(const Ctx &c, Shared *sh, float *fring) {
             delta0 = (mx > kNegInf ? mx : 0.0f) - delta1;
         }
         fbase += (double) delta0;
-        const Meta m3 = load_meta(A, db, d + 3, n);
-        // stage 1: ids and events two anti-diagonals ahead
+        const Meta mnn = decode_meta(raw_nn, d + 2 <= n);
+        raw_nn = raw_meta(A, db, d + 3, n);
+        // stage 1: raw ids and events two anti-diagonals ahead (consumed next step)
+        int32_t rk2[CPT];
+        float4 re2[CPT];
+        bool vx2[CPT], vy2[CPT];
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             const int i = tid + j * kGroup;
             const int32_t xmy = mnn.L + 2 * i, x = (d + 2 + xmy) >> 1, y = (d + 2 - xmy) >> 1;
             const bool in = i < mnn.W;
-            kid2[j] = in ? load_kid(c, x) : -1;
-            ev2[j] = load_event(c, in ? y - 1 : -1);
-            hev2[j] = in && y >= 1;
+            rk2[j] = raw_kid(c, x);
+            re2[j] = raw_event(c, y - 1);
+            vx2[j] = in && x >= 1 && x <= R.lX;
+            vy2[j] = in && y >= 1;
         }
-        // stage 2: k-mer constants one anti-diagonal ahead
+        // stage 2: k-mer constants one anti-diagonal ahead (ids loaded last step)
+        int32_t kid1[CPT];
         KmerConst32 kc1[CPT];
 #pragma unroll
-        for (int j = 0; j < CPT; ++j) kc1[j] = load_kc(c, kid1[j]);
+        for (int j = 0; j < CPT; ++j) {
+            kid1[j] = vx1[j] ? rk1[j] : -1;
+            kc1[j] = raw_kc(c, kid1[j]);
+        }
         // the recursion on anti-diagonal d (stateMachine3_cellCalculate order: lower -> gap-X,
         // middle -> match, upper -> gap-Y, each state accumulated from LOG_ZERO)
         const int32_t W0 = m0.W;
@@ -434,9 +478,9 @@ __device__ void forward_region(const Ctx &c, Shared *sh, float *fring) {
         // emissions of the next anti-diagonal's cells
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
-            emit_event_pair(c, kid1[j], kc1[j], ev1[j], hev1[j], eM[j], eY[j]);
-            eX[j] = c.hdp ? (kid1[j] >= 0 ? (float) kLogPointOne : kNegInf) : kc1[j].gapx;
-            kid1[j] = kid2[j]; ev1[j] = ev2[j]; hev1[j] = hev2[j];
+            emit_event_pair(c, kid1[j], kc1[j], as_event(re1[j]), vy1[j], eM[j], eY[j]);
+            eX[j] = kid1[j] < 0 ? kNegInf : (c.hdp ? (float) kLogPointOne : kc1[j].gapx);
+            rk1[j] = rk2[j]; re1[j] = re2[j]; vx1[j] = vx2[j]; vy1[j] = vy2[j];
         }
         if (tid == 0) {
             A.base[db + d] = fbase;
@@ -450,7 +494,7 @@ __device__ void forward_region(const Ctx &c, Shared *sh, float *fring) {
         delta1 = delta0;
         Fd += kStoreStride * W0;
         rg.rotate();
-        m2 = m1; m1 = m0; m0 = mn; mn = mnn; mnn = m3;
+        m2 = m1; m1 = m0; m0 = mn; mn = mnn;
     }
 }
 
@@ -459,7 +503,7 @@ __device__ void forward_region(const Ctx &c, Shared *sh, float *fring) {
 // ------------------------------------------------------------------------------------------------
 template <int CPT>
 __device__ __forceinline__ void write_pairs(const Ctx &c, Shared *sh, int32_t pend_d, unsigned pend, const float *pv,
-                                            const int32_t *px, const int32_t *py, int64_t &n_out) {
+                                            const int32_t *px, const int32_t *py, const int32_t *pk, int64_t &n_out) {
     const Args &A = *c.A;
     const RegionDesc &R = c.R;
     const int tid = threadIdx.x - kGroup, lane = tid & 31, warp = tid >> 5;
@@ -481,7 +525,7 @@ __device__ __forceinline__ void write_pairs(const Ctx &c, Shared *sh, int32_t pe
                 o.score = (int64_t) floor((double) fminf(pv[j], 1.0f) * 10000000.0);
                 o.x = R.x1 + px[j] - 1;
                 o.y = R.y1 + py[j] - 1;
-                o.kmer = load_kid(c, px[j]);
+                o.kmer = pk[j];
                 A.out[R.out_base + slot] = o;
             } else {
                 atomicMax(A.status + R.read, (int32_t) SA_E_OUTPUT);
@@ -537,10 +581,12 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
         rg.s[0] = bring + 1;                      // d = D
         rg.s[1] = bring + 3 * rg.stride + 1;      // d + 1 (none yet: -inf)
         rg.s[2] = bring + 6 * rg.stride + 1;      // d + 2
-        // metas of d+2, d+1, d, d-1, d-2 (d = D to start) and store offsets of d+2, d+1, d
+        // metas of d+2, d+1, d, d-1, d-2 (d = D to start) and store offsets of d+1, d
         Meta mpp{0, 0, 0}, mp{0, 0, 0};
-        Meta m0 = load_meta(A, db, D, n), mm = load_meta(A, db, D - 1, n), mmm = load_meta(A, db, D - 2, n);
-        int32_t off0 = __ldg(A.window_off + R.win_base + wi), offp = off0, offpp = off0;
+        Meta m0 = decode_meta(raw_meta(A, db, D, n), true);
+        Meta mm = decode_meta(raw_meta(A, db, D - 1, n), D - 1 >= 0);
+        int2 raw_mmm = raw_meta(A, db, D - 2, n);
+        int32_t off0 = __ldg(A.window_off + R.win_base + wi), offp = off0;
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             const int i = tid + j * kGroup;
@@ -555,19 +601,20 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
         float eMm[CPT], eYu[CPT], eXl[CPT], fM[CPT];
         // refresh operands: gap states of d, and the match-through inputs of the d+1 cells
         float fX[CPT], fY[CPT], tM[CPT], tX[CPT], tY[CPT], tE[CPT];
+        bool tv[CPT];
         double fb = __ldcg(A.base + db + D);
         float fsh = __ldcg(A.fshift + db + D);
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             const int i = tid + j * kGroup;
-            const int ic = min(i, max(m0.W - 1, 0));
+            const int ic = clampi(i, 0, max(m0.W - 1, 0));
             const float *Fd = Freg + kStoreStride * off0;
-            const bool post = D <= from && i < m0.W;
             eMm[j] = eYu[j] = eXl[j] = kNegInf;
-            fM[j] = post ? __ldcg(Fd + ST_M * m0.W + ic) : kNegInf;
-            fX[j] = post ? __ldcg(Fd + ST_X * m0.W + ic) : kNegInf;
-            fY[j] = post ? __ldcg(Fd + ST_Y * m0.W + ic) : kNegInf;
+            fM[j] = __ldcg(Fd + ST_M * m0.W + ic);
+            fX[j] = __ldcg(Fd + ST_X * m0.W + ic);
+            fY[j] = __ldcg(Fd + ST_Y * m0.W + ic);
             tM[j] = tX[j] = tY[j] = tE[j] = kNegInf;
+            tv[j] = false;
         }
         float lm_prev = kNegInf;           // local max of B stored on d+1 (lagged reduction)
         float gamma1 = 0.0f;               // base(d+1) - base(d+2)
@@ -575,7 +622,7 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
         double pref = 0.0;                 // latest refresh total probability (absolute)
         unsigned pend = 0;
         float pv[CPT];
-        int32_t px[CPT], py[CPT];
+        int32_t px[CPT], py[CPT], pk[CPT];
         int32_t pend_d = -1;
         group_bar(kBarBackward);
         for (int32_t d = D; d > T; --d) {
@@ -595,47 +642,48 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
                 gamma0 = m - gamma1;
             }
             bbase += (double) gamma0;
-            // prefetch the operands of the d-1 cells (indices clamped into the owning anti-diagonal:
-            // a value fetched for an absent neighbour is only ever added to a -inf ring value)
-            const Meta m3 = load_meta(A, db, d - 3, n);
+            // prefetch the operands of the d-1 cells: raw loads from clamped indices; a value
+            // fetched for an absent neighbour is only ever added to a -inf ring value
+            const Meta mmm = decode_meta(raw_mmm, d - 2 >= 0);
+            raw_mmm = raw_meta(A, db, d - 3, n);
             const int32_t Wm = mm.W, Wmm = mmm.W;
             const int32_t offm = off0 - Wm, offmm = offm - Wmm;
             const bool live_m = d - 1 > T;
-            const bool post_m = live_m && d - 1 <= from;
-            const bool refresh_m = post_m && (mm.flags & kFlagRefresh);
+            const bool refresh_m = live_m && d - 1 <= from && (mm.flags & kFlagRefresh);
             float eMm_n[CPT], eYu_n[CPT], eXl_n[CPT], fM_n[CPT], fX_n[CPT], fY_n[CPT];
             float tM_n[CPT], tX_n[CPT], tY_n[CPT], tE_n[CPT];
+            bool tv_n[CPT];
             {
                 const float *Fd = Freg + kStoreStride * off0;      // d
-                const float *Fp = Freg + kStoreStride * offp;      // d+1
+                const float *Fp = Freg + kStoreStride * offp;      // d+1 (or d at the window top)
                 const float *Fm = Freg + kStoreStride * offm;      // d-1
-                const float *Fmm = Freg + kStoreStride * offmm;    // d-2
+                const float *Fmm = Freg + kStoreStride * (Wmm > 0 ? offmm : offm);   // d-2
+                const int32_t Wpl = Wp > 0 ? Wp : W0;              // width of the block Fp points at
 #pragma unroll
                 for (int j = 0; j < CPT; ++j) {
                     const int i = tid + j * kGroup;
                     const int32_t xmy = mm.L + 2 * i, x = (d - 1 + xmy) >> 1;
-                    const bool in = live_m && i < Wm;
-                    const bool has_p = d + 1 <= D && Wp > 0;
-                    eMm_n[j] = in && has_p ? __ldcg(Fp + ST_EM * Wp + clampi((xmy - mp.L) >> 1, 0, Wp - 1)) : kNegInf;
-                    eYu_n[j] = in && W0 > 0 ? __ldcg(Fd + ST_EY * W0 + clampi((xmy - 1 - m0.L) >> 1, 0, W0 - 1)) : kNegInf;
-                    eXl_n[j] = in ? load_gapx(c, x + 1) : kNegInf;
-                    const int ic = min(i, max(Wm - 1, 0));
-                    fM_n[j] = post_m && i < Wm ? __ldcg(Fm + ST_M * Wm + ic) : kNegInf;
-                    fX_n[j] = refresh_m && i < Wm ? __ldcg(Fm + ST_X * Wm + ic) : kNegInf;
-                    fY_n[j] = refresh_m && i < Wm ? __ldcg(Fm + ST_Y * Wm + ic) : kNegInf;
+                    eMm_n[j] = __ldcg(Fp + ST_EM * Wpl + clampi((xmy - mp.L) >> 1, 0, max(Wpl - 1, 0)));
+                    eYu_n[j] = __ldcg(Fd + ST_EY * W0 + clampi((xmy - 1 - m0.L) >> 1, 0, max(W0 - 1, 0)));
+                    eXl_n[j] = raw_gapx(c, x + 1);
+                    const int ic = clampi(i, 0, max(Wm - 1, 0));
+                    fM_n[j] = __ldcg(Fm + ST_M * Wm + ic);
+                    fX_n[j] = __ldcg(Fm + ST_X * Wm + ic);
+                    fY_n[j] = __ldcg(Fm + ST_Y * Wm + ic);
                     // match-through inputs for a refresh at d-1: cells of d, F of d-2, emissions of d
-                    const bool thr = refresh_m && i < W0;
                     const int32_t xmy0 = m0.L + 2 * i;
-                    const bool has_mm = thr && Wmm > 0 && xmy0 >= mmm.L && ((xmy0 - mmm.L) >> 1) < Wmm && d - 2 >= 0;
-                    const int imm = clampi((xmy0 - mmm.L) >> 1, 0, max(Wmm - 1, 0));
-                    tE_n[j] = thr ? __ldcg(Fd + ST_EM * W0 + min(i, W0 - 1)) : kNegInf;
-                    tM_n[j] = has_mm ? __ldcg(Fmm + ST_M * Wmm + imm) : kNegInf;
-                    tX_n[j] = has_mm ? __ldcg(Fmm + ST_X * Wmm + imm) : kNegInf;
-                    tY_n[j] = has_mm ? __ldcg(Fmm + ST_Y * Wmm + imm) : kNegInf;
+                    const int32_t r = (xmy0 - mmm.L) >> 1;
+                    tv_n[j] = refresh_m && i < W0 && Wmm > 0 && xmy0 >= mmm.L && r < Wmm;
+                    const int imm = clampi(r, 0, max(Wmm - 1, 0));
+                    const int32_t Wml = Wmm > 0 ? Wmm : Wm;
+                    tE_n[j] = __ldcg(Fd + ST_EM * W0 + clampi(i, 0, max(W0 - 1, 0)));
+                    tM_n[j] = __ldcg(Fmm + ST_M * Wml + imm);
+                    tX_n[j] = __ldcg(Fmm + ST_X * Wml + imm);
+                    tY_n[j] = __ldcg(Fmm + ST_Y * Wml + imm);
                 }
             }
-            const double fb_n = d - 1 >= 0 ? __ldcg(A.base + db + d - 1) : 0.0;
-            const float fsh_n = d - 1 >= 0 ? __ldcg(A.fshift + db + d - 1) : 0.0f;
+            const double fb_n = __ldcg(A.base + db + max(d - 1, 0));
+            const float fsh_n = __ldcg(A.fshift + db + max(d - 1, 0));
             // the recursion on d (D itself holds the end-state values)
             float lm = kNegInf;
             if (d < D) {
@@ -675,7 +723,7 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
             group_bar(kBarBackward);
             // pairs of the previous anti-diagonal, in the reference's order (ascending xmy)
             if (pend_d >= 0) {
-                write_pairs<CPT>(c, sh, pend_d, pend, pv, px, py, n_out);
+                write_pairs<CPT>(c, sh, pend_d, pend, pv, px, py, pk, n_out);
                 pend = 0;
                 pend_d = -1;
             }
@@ -699,9 +747,12 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
                         for (int j = 0; j < CPT; ++j) {
                             const int i = tid + j * kGroup;
                             if (i < Wp) {
-                                float mth = tM[j] + (tE[j] + t[T_MC]);
-                                mth = lae(tab, mth, tX[j] + (tE[j] + t[T_MFGX]));
-                                mth = lae(tab, mth, tY[j] + (tE[j] + t[T_MFGY]));
+                                float mth = kNegInf;
+                                if (tv[j]) {
+                                    mth = tM[j] + (tE[j] + t[T_MC]);
+                                    mth = lae(tab, mth, tX[j] + (tE[j] + t[T_MFGX]));
+                                    mth = lae(tab, mth, tY[j] + (tE[j] + t[T_MFGY]));
+                                }
                                 chain[wmax + i] = mth + rg.st(1, 0)[i];
                             }
                         }
@@ -730,6 +781,7 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
                     pv[j] = p;
                     px[j] = x;
                     py[j] = y;
+                    pk[j] = raw_kid(c, x);    // consumed by write_pairs after the next barrier
                     const unsigned bal = __ballot_sync(0xffffffffu, hit);
                     if (hit) pend |= 1u << j;
                     if (lane == 0) sh->wcnt[d & 1][j][warp] = __popc(bal);
@@ -740,21 +792,19 @@ __device__ void backward_region(const Ctx &c, Shared *sh, float *bring, float *c
             for (int j = 0; j < CPT; ++j) {
                 eMm[j] = eMm_n[j]; eYu[j] = eYu_n[j]; eXl[j] = eXl_n[j];
                 fM[j] = fM_n[j]; fX[j] = fX_n[j]; fY[j] = fY_n[j];
-                tM[j] = tM_n[j]; tX[j] = tX_n[j]; tY[j] = tY_n[j]; tE[j] = tE_n[j];
+                tM[j] = tM_n[j]; tX[j] = tX_n[j]; tY[j] = tY_n[j]; tE[j] = tE_n[j]; tv[j] = tv_n[j];
             }
             fb = fb_n;
             fsh = fsh_n;
             lm_prev = d == D ? kNegInf : lm;   // D's maximum is known exactly (mxD)
             gamma1 = gamma0;
-            offpp = offp; offp = off0; off0 = offm;
+            offp = off0; off0 = offm;
             rg.rotate();
-            // after rotate: s[0] takes the old d+2 slot, which becomes d-1
-            mpp = mp; mp = m0; m0 = mm; mm = mmm; mmm = m3;
+            mpp = mp; mp = m0; m0 = mm; mm = mmm;
         }
         // flush the last anti-diagonal's pairs
         group_bar(kBarBackward);
-        if (pend_d >= 0) write_pairs<CPT>(c, sh, pend_d, pend, pv, px, py, n_out);
-        (void) offpp;
+        if (pend_d >= 0) write_pairs<CPT>(c, sh, pend_d, pend, pv, px, py, pk, n_out);
         group_bar(kBarBackward);
     }
     if (tid == 0) {
