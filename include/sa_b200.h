@@ -222,6 +222,45 @@ sa_status sa_batch_transfer_bytes(const sa_batch *b, int64_t *h2d, int64_t *d2h)
 int64_t sa_batch_regions(const sa_batch *b);
 void sa_batch_destroy(sa_batch *b);
 
+/* ---- batched FP32 form without device allocation (no counterpart in signalAlign) ---- */
+
+/* Size of the one static device array behind sa_align_batch_noalloc, per device: 64 MiB, room for
+ * about 3 million band cells with their inputs and pair output (e.g. ten reads of 1 kb reference
+ * and 1.5k events at diagonal expansion 50). */
+#define SA_NOALLOC_SCRATCH_BYTES (64ll << 20)
+
+/* sa_align_batch for callers that must not allocate device memory.  Such callers exist: a process
+ * whose framework already holds almost all of the GPU's memory in its own pool (a caching allocator,
+ * a serving engine that reserved its arena at start-up), where cudaMalloc fails or makes the
+ * framework give memory back; and latency-bound loops, where cudaMalloc / cudaFree can synchronise
+ * the whole device and stall every other stream.  This call runs the same batched FP32 kernel as
+ * sa_align_batch, with every device buffer (packed inputs, forward store, counters, pair output)
+ * carved from one file-scope device array of SA_NOALLOC_SCRATCH_BYTES; it calls no cudaMalloc,
+ * cudaFree or other allocating routine.
+ *   - Each read's state machine must already hold current device tables (they are written by the
+ *     first allocating call that uses the machine after it was loaded or changed: sa_align_batch,
+ *     sa_batch_create, sa_getAlignedPairsUsingAnchors); otherwise SA_E_ARG.
+ *   - A batch that needs more than SA_NOALLOC_SCRATCH_BYTES is rejected with SA_E_CAPACITY before
+ *     any device work; *scratch_bytes (optional) receives the bytes the batch needs in every case.
+ *   - What must be zero when the kernel starts (the region queue counter, per-read status words and
+ *     per-region pair counts) is cleared by the call itself on `stream` before every launch; every
+ *     other byte the kernel reads is written earlier in the same call.
+ *   - The first call on a device looks the array's address up (cudaGetSymbolAddress, which can load
+ *     the library's device code on that device): make one call on each device during set-up, before
+ *     any stream capture begins.
+ *   - All calls on a device share the array, so two calls whose device work overlapped would
+ *     overwrite each other's data.  The call is synchronous (it returns after `stream` drained) and
+ *     holds a per-device lock for its whole duration, so calls from several host threads run one
+ *     after another.
+ * Results: read r's pairs are pairs[pair_offsets[r] .. pair_offsets[r + 1]) (reference emission
+ * order); pair_offsets has n_reads + 1 entries; read_status n_reads entries (as
+ * sa_batch_read_status); log_likelihood n_reads entries or NULL.  If the pairs exceed pair_capacity
+ * the call returns SA_E_OUTPUT with pair_offsets filled (pair_offsets[n_reads] is the capacity
+ * needed) and writes no pair. */
+sa_status sa_align_batch_noalloc(const sa_read *reads, int64_t n_reads, const sa_params *p, void *stream,
+                                 sa_aligned_pair *pairs, int64_t pair_capacity, int64_t *pair_offsets,
+                                 int32_t *read_status, double *log_likelihood, int64_t *scratch_bytes);
+
 /* ---- diagnostics ---- */
 const char *sa_status_string(sa_status s);
 /* number of kernel launches this process has made through the library (all entry points) */

@@ -98,6 +98,9 @@ def _bind(L):
         "sa_batch_regions": (C.c_int64, [vp]),
         "sa_batch_transfer_bytes": (C.c_int, [vp, _i64p, _i64p]),
         "sa_batch_destroy": (None, [vp]),
+        "sa_align_batch_noalloc": (C.c_int, [C.POINTER(Read), C.c_int64, C.POINTER(Params), vp,
+                                             C.POINTER(AlignedPair), C.c_int64, _i64p, C.POINTER(C.c_int32), _f64p,
+                                             _i64p]),
         "sa_status_string": (C.c_char_p, [C.c_int]),
         "sa_kernel_launch_count": (C.c_int64, []),
         "sa_measure_fp32_peak": (C.c_int, [C.c_int32, _f64p]),
@@ -312,27 +315,33 @@ class ReadInput:
     degenerate: int = CYTOSINE_METHYLATION3
 
 
+def _read_array(reads, keep):
+    """sa_read array of ReadInputs; the numpy / bytes buffers it points into are appended to keep."""
+    arr = (Read * len(reads))()
+    for i, r in enumerate(reads):
+        ev = _f64(r.events, 4)
+        a = _anchors(r.anchors)
+        ref = r.reference.encode()
+        keep += [ev, a, ref]
+        arr[i].sm = r.sm.handle.value
+        arr[i].reference = ref
+        arr[i].reference_length = len(ref)
+        arr[i].events = ev.ctypes.data_as(_f64p)
+        arr[i].n_events = len(ev)
+        arr[i].anchors = a.ctypes.data_as(_i64p)
+        arr[i].n_anchors = len(a)
+        arr[i].scale, arr[i].shift, arr[i].var = r.scale, r.shift, r.var
+        arr[i].ragged_left, arr[i].ragged_right = int(r.ragged_left), int(r.ragged_right)
+        arr[i].degenerate = r.degenerate
+    return arr
+
+
 class Batch:
     """A planned batch on the device: upload / run / download, or all at once with align()."""
 
     def __init__(self, reads, p):
         self._keep = []
-        arr = (Read * len(reads))()
-        for i, r in enumerate(reads):
-            ev = _f64(r.events, 4)
-            a = _anchors(r.anchors)
-            ref = r.reference.encode()
-            self._keep += [ev, a, ref]
-            arr[i].sm = r.sm.handle.value
-            arr[i].reference = ref
-            arr[i].reference_length = len(ref)
-            arr[i].events = ev.ctypes.data_as(_f64p)
-            arr[i].n_events = len(ev)
-            arr[i].anchors = a.ctypes.data_as(_i64p)
-            arr[i].n_anchors = len(a)
-            arr[i].scale, arr[i].shift, arr[i].var = r.scale, r.shift, r.var
-            arr[i].ragged_left, arr[i].ragged_right = int(r.ragged_left), int(r.ragged_right)
-            arr[i].degenerate = r.degenerate
+        arr = _read_array(reads, self._keep)
         self._reads = arr
         self.n = len(reads)
         self._sms = [r.sm for r in reads]
@@ -390,6 +399,54 @@ def align_batch(reads, p, stream=None):
     b.run(stream)
     b.download(stream)
     return b
+
+
+# size of the static device array behind sa_align_batch_noalloc (SA_NOALLOC_SCRATCH_BYTES)
+NOALLOC_SCRATCH_BYTES = 64 << 20
+
+
+class NoallocResult:
+    """Host results of one sa_align_batch_noalloc call."""
+
+    def __init__(self, pairs, offsets, status, loglik, scratch_bytes):
+        self._pairs, self._off = pairs, offsets
+        self._status, self._ll = status, loglik
+        self.scratch_bytes = scratch_bytes
+
+    def status(self, i):
+        return int(self._status[i])
+
+    def log_likelihood(self, i):
+        return float(self._ll[i])
+
+    def pairs(self, i):
+        return self._pairs[self._off[i]:self._off[i + 1]].copy()
+
+
+def align_batch_noalloc(reads, p, stream=None, pair_capacity=None):
+    """Batched FP32 form without device allocation (sa_align_batch_noalloc).  The reads' state
+    machines must already hold device tables (any earlier allocating alignment with them)."""
+    keep = []
+    arr = _read_array(reads, keep)
+    n = len(reads)
+    if pair_capacity is None:
+        pair_capacity = sum(4 * (len(r.reference) + len(r.events)) + 256 for r in reads)
+    for _ in range(2):
+        pairs = np.zeros(max(pair_capacity, 1), PAIR_DTYPE)
+        off = np.zeros(n + 1, np.int64)
+        status = np.zeros(max(n, 1), np.int32)
+        ll = np.zeros(max(n, 1), np.float64)
+        need = C.c_int64(0)
+        st = lib().sa_align_batch_noalloc(arr, n, C.byref(p), stream, pairs.ctypes.data_as(C.POINTER(AlignedPair)),
+                                          pair_capacity, off.ctypes.data_as(_i64p),
+                                          status.ctypes.data_as(C.POINTER(C.c_int32)), ll.ctypes.data_as(_f64p),
+                                          C.byref(need))
+        if st == 6 and off[n] > pair_capacity:   # SA_E_OUTPUT: size the pair array from pair_offsets
+            pair_capacity = int(off[n])
+            continue
+        _check(st, "align_batch_noalloc")
+        return NoallocResult(pairs, off, status, ll, need.value)
+    raise SAError(6, "align_batch_noalloc")
 
 
 def kernel_launch_count():

@@ -129,17 +129,11 @@ void free_batch_device(sa_batch *b) {
     cudaFree(b->d_queue);
 }
 
-}  // namespace
-
-extern "C" {
-
-sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch **out) {
-    if (!reads || n_reads < 0 || !p || !out) return SA_E_ARG;
-    *out = nullptr;
-    sa_status st = check_params(*p);
-    if (st) return st;
-    auto *b = new (std::nothrow) sa_batch();
-    if (!b) return SA_E_NOMEM;
+// Host planning of a batch (no device work): per read k-mer ids, events and regions, per region its
+// windows and per-anti-diagonal meta, the LPT order.  Returns SA_E_CAPACITY for a band wider than
+// the kernel's widest ring.
+sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch *b) {
+    sa_status st = SA_OK;
     b->n_reads = n_reads;
     b->threshold = (float) p->threshold;
     b->read_status.assign(n_reads, SA_OK);
@@ -235,10 +229,7 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
         }
         b->read_n_regions[r] = (int64_t) b->regions.size() - b->read_first_region[r];
     }
-    if (b->max_width > kMaxCpt * kGroup) {
-        delete b;
-        return SA_E_CAPACITY;
-    }
+    if (b->max_width > kMaxCpt * kGroup) return SA_E_CAPACITY;
     b->device = device < 0 ? 0 : device;
     // largest band area first (LPT order for the persistent CTAs)
     b->order.resize(b->regions.size());
@@ -249,6 +240,25 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
         area[i] = (i + 1 < b->regions.size() ? b->regions[i + 1].cell_base : b->cells) - d.cell_base;
     }
     std::stable_sort(b->order.begin(), b->order.end(), [&](int32_t a, int32_t c) { return area[a] > area[c]; });
+    return SA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch **out) {
+    if (!reads || n_reads < 0 || !p || !out) return SA_E_ARG;
+    *out = nullptr;
+    sa_status st = check_params(*p);
+    if (st) return st;
+    auto *b = new (std::nothrow) sa_batch();
+    if (!b) return SA_E_NOMEM;
+    st = plan_batch(reads, n_reads, p, b);
+    if (st) {
+        delete b;
+        return st;
+    }
     // device buffers
     int prev = 0;
     cudaGetDevice(&prev);
@@ -537,3 +547,67 @@ void sa_batch_destroy(sa_batch *b) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// batches whose device buffers live in caller-provided device memory (sa_noalloc.cu)
+// ------------------------------------------------------------------------------------------------
+namespace sa {
+
+sa_status batch_plan_host(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch **out) {
+    if (!reads || n_reads < 0 || !p || !out) return SA_E_ARG;
+    *out = nullptr;
+    sa_status st = check_params(*p);
+    if (st) return st;
+    auto *b = new (std::nothrow) sa_batch();
+    if (!b) return SA_E_NOMEM;
+    st = plan_batch(reads, n_reads, p, b);
+    if (st) {
+        delete b;
+        return st;
+    }
+    *out = b;
+    return SA_OK;
+}
+
+int batch_device(const sa_batch *b) { return b->device; }
+
+bool batch_models_resident(const sa_batch *b) {
+    for (const sa_state_machine *sm : b->models)
+        if (sm->dev_dirty) return false;
+    return true;
+}
+
+size_t batch_bind_scratch(sa_batch *b, unsigned char *base) {
+    size_t at = 0;
+    auto carve = [&](auto **ptr, size_t n) {
+        using T = std::remove_reference_t<decltype(**ptr)>;
+        at = (at + 255) & ~(size_t) 255;
+        if (base) *ptr = reinterpret_cast<T *>(base + at);
+        at += std::max<size_t>(n, 1) * sizeof(T);
+    };
+    const size_t nd = b->meta.size(), nr = b->regions.size();
+    carve(&b->d_regions, nr);
+    carve(&b->d_order, b->order.size());
+    carve(&b->d_models, b->models.size());
+    carve(&b->d_read_scale, b->read_scale.size());
+    carve(&b->d_meta, nd);
+    carve(&b->d_window_off, b->window_off.size());
+    carve(&b->d_windows, b->windows.size());
+    carve(&b->d_kmer, b->kmer.size());
+    carve(&b->d_gapx, b->gapx.size());
+    carve(&b->d_events_raw, b->events.size());
+    carve(&b->d_events, b->events.size());
+    carve(&b->d_F, (size_t) kStoreStride * (size_t) b->cells);
+    carve(&b->d_base, nd);
+    carve(&b->d_fshift, nd);
+    carve(&b->d_out, (size_t) b->out_total);
+    carve(&b->d_out_count, nr);
+    carve(&b->d_loglik, nr);
+    carve(&b->d_status, (size_t) b->n_reads);
+    carve(&b->d_queue, 1);
+    return (at + 255) & ~(size_t) 255;
+}
+
+void batch_release_host(sa_batch *b) { delete b; }
+
+}  // namespace sa

@@ -127,6 +127,16 @@ void free_device_model(sa_state_machine *sm);
 
 void count_launch(int64_t n = 1);
 
+// batches bound to one caller-provided device area instead of their own allocations (sa_fp32.cu)
+sa_status batch_plan_host(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch **out);
+int batch_device(const sa_batch *b);
+bool batch_models_resident(const sa_batch *b);
+// bytes of the area that holds every device buffer of `b`; with base != nullptr the batch's device
+// pointers are set into [base, base + bytes), each buffer 256-byte aligned
+size_t batch_bind_scratch(sa_batch *b, unsigned char *base);
+// frees the host side only (the device area belongs to the caller)
+void batch_release_host(sa_batch *b);
+
 #define SA_CUDA_TRY(expr)                                   \
     do {                                                    \
         cudaError_t _e = (expr);                            \
