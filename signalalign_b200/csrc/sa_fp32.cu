@@ -1,24 +1,17 @@
-// Batched FP32 form: all regions of all reads in one persistent launch.
+// Batched FP32 form: host side.  Plans a batch (band geometry, traceback windows, k-mer ids,
+// emission chunks, output segments), owns its device buffers, and runs the three kernels of
+// sa_fp32_kernel.cuh: emissions of every band cell, the persistent worker (forward sweeps and
+// traceback-window backward sweeps pulled from a device queue), and the per-read gather of pairs.
 //
-// Work distribution: regions are sorted by band area (largest first) on the host; persistent CTAs
-// of 128 threads pull the next region from a device counter.  A CTA sweeps its region's band one
-// anti-diagonal at a time (cells of an anti-diagonal spread over the threads, neighbours exchanged
-// through a 3-slot shared-memory ring, one barrier per anti-diagonal).  Forward values go to HBM
-// (3 floats per cell, SoA per anti-diagonal) together with each anti-diagonal's FP64 base.  At each
-// traceback point of getPosteriorProbsWithBanding (pairwiseAligner.c:1319-1333) the CTA runs the
-// window's backward sweep in shared memory with the posterior test fused into it, so backward
-// values never leave the SM.  Total probabilities are refreshed on the reference's schedule
-// (every 10th posterior anti-diagonal, :1370-1380) and accumulated in the reference's sequential
-// cell order, which the 7.5 cut-off of logAdd makes order dependent.
-//
-// Values are log probabilities relative to a per-anti-diagonal base: the base of anti-diagonal d is
-// the base of d-1 plus the largest value stored on d-1 (FP64, carried by every thread), so stored
-// FP32 values stay near zero.
+// Every device buffer of a batch is listed once (for_each_buffer), so the allocating path
+// (sa_batch_create) and the path that carves them from caller-provided memory
+// (batch_bind_scratch) lay out the same set.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "sa_dp32.cuh"
@@ -53,6 +46,10 @@ __global__ void __launch_bounds__(256) fma_probe(float *sink, int iters, float s
     if (s == 12345.678f) sink[0] = s;
 }
 
+// Slack after the emission and forward stores: the kernels' clamped look-ahead loads past a
+// region's last anti-diagonal stay inside the allocation.
+constexpr size_t kStoreSlack = 1024;
+
 }  // namespace fp32
 }  // namespace sa
 
@@ -70,10 +67,12 @@ struct sa_batch {
     std::vector<int32_t> order;
     std::vector<int32_t> read_status;       // host planning status per read
     std::vector<int64_t> read_first_region, read_n_regions;
+    std::vector<int64_t> read_win;          // per read: first window, window count
     std::vector<ReadScale32> read_scale;
     std::vector<int2> meta;
-    std::vector<int32_t> window_off;
     std::vector<Window> windows;
+    std::vector<WindowTask> wtask;
+    std::vector<Chunk> chunks;
     std::vector<int32_t> kmer;
     std::vector<float> gapx;
     std::vector<double2> events;
@@ -86,21 +85,24 @@ struct sa_batch {
     ModelDesc *d_models = nullptr;
     ReadScale32 *d_read_scale = nullptr;
     int2 *d_meta = nullptr;
-    int32_t *d_window_off = nullptr, *d_kmer = nullptr, *d_status = nullptr;
-    float *d_gapx = nullptr;
-    int64_t *d_out_count = nullptr;
     Window *d_windows = nullptr;
+    WindowTask *d_wtask = nullptr;
+    Chunk *d_chunks = nullptr;
+    int32_t *d_kmer = nullptr;
+    float *d_gapx = nullptr;
     double2 *d_events_raw = nullptr;
     Event32 *d_events = nullptr;
-    float *d_F = nullptr, *d_fshift = nullptr;
+    float *d_E = nullptr, *d_F = nullptr, *d_fshift = nullptr;
     double *d_base = nullptr, *d_loglik = nullptr;
-    sa_aligned_pair *d_out = nullptr;
-    unsigned int *d_queue = nullptr;
+    int32_t *d_ready = nullptr, *d_status = nullptr;
+    sa_aligned_pair *d_out = nullptr, *d_packed = nullptr;
+    int64_t *d_wcount = nullptr, *d_read_win = nullptr, *d_read_base = nullptr, *d_read_count = nullptr;
+    Control *d_ctl = nullptr;
     // results
-    std::vector<int64_t> out_count;
+    std::vector<int64_t> read_base, read_count;
     std::vector<double> loglik;
     std::vector<int32_t> dev_status;
-    std::vector<sa_aligned_pair> out;
+    Control ctl{};
     std::vector<std::vector<sa_aligned_pair>> read_pairs;
     std::vector<double> read_ll;
     bool downloaded = false;
@@ -108,10 +110,37 @@ struct sa_batch {
 
 namespace {
 
-template <typename T>
-sa_status dalloc(T **p, size_t n) {
-    if (n == 0) n = 1;
-    return cudaMalloc((void **) p, n * sizeof(T)) == cudaSuccess ? SA_OK : SA_E_NOMEM;
+// Calls fn(pointer, element count) for every device buffer of the batch.
+template <typename Fn>
+void for_each_buffer(sa_batch *b, Fn &&fn) {
+    const size_t nr = b->regions.size(), nd = b->meta.size(), nw = b->windows.size(), nreads = (size_t) b->n_reads;
+    const size_t cells = (size_t) b->cells;
+    fn(b->d_regions, nr);
+    fn(b->d_order, b->order.size());
+    fn(b->d_models, b->models.size());
+    fn(b->d_read_scale, b->read_scale.size());
+    fn(b->d_meta, nd);
+    fn(b->d_windows, nw);
+    fn(b->d_wtask, nw);
+    fn(b->d_chunks, b->chunks.size());
+    fn(b->d_kmer, b->kmer.size());
+    fn(b->d_gapx, b->gapx.size());
+    fn(b->d_events_raw, b->events.size());
+    fn(b->d_events, b->events.size());
+    fn(b->d_E, 2 * cells + kStoreSlack);
+    fn(b->d_F, 3 * cells + kStoreSlack);
+    fn(b->d_base, nd);
+    fn(b->d_fshift, nd);
+    fn(b->d_ready, nw);
+    fn(b->d_out, (size_t) b->out_total);
+    fn(b->d_wcount, nw);
+    fn(b->d_loglik, nr);
+    fn(b->d_status, nreads);
+    fn(b->d_ctl, (size_t) 1);
+    fn(b->d_read_win, 2 * nreads);
+    fn(b->d_packed, (size_t) b->out_total);
+    fn(b->d_read_base, nreads);
+    fn(b->d_read_count, nreads);
 }
 
 template <typename T>
@@ -121,17 +150,24 @@ sa_status h2d(T *dst, const std::vector<T> &src, cudaStream_t s) {
                ? SA_OK : SA_E_CUDA;
 }
 
+template <typename T>
+sa_status d2h(std::vector<T> &dst, const T *src, size_t n, cudaStream_t s) {
+    dst.resize(n);
+    if (n == 0) return SA_OK;
+    return cudaMemcpyAsync(dst.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, s) == cudaSuccess ? SA_OK
+                                                                                                     : SA_E_CUDA;
+}
+
 void free_batch_device(sa_batch *b) {
-    cudaFree(b->d_regions); cudaFree(b->d_order); cudaFree(b->d_models); cudaFree(b->d_read_scale);
-    cudaFree(b->d_meta); cudaFree(b->d_window_off); cudaFree(b->d_kmer); cudaFree(b->d_gapx); cudaFree(b->d_status);
-    cudaFree(b->d_out_count); cudaFree(b->d_windows); cudaFree(b->d_events_raw); cudaFree(b->d_events);
-    cudaFree(b->d_F); cudaFree(b->d_fshift); cudaFree(b->d_base); cudaFree(b->d_loglik); cudaFree(b->d_out);
-    cudaFree(b->d_queue);
+    for_each_buffer(b, [](auto *&p, size_t) {
+        cudaFree(p);
+        p = nullptr;
+    });
 }
 
 // Host planning of a batch (no device work): per read k-mer ids, events and regions, per region its
-// windows and per-anti-diagonal meta, the LPT order.  Returns SA_E_CAPACITY for a band wider than
-// the kernel's widest ring.
+// windows, per-anti-diagonal meta and emission chunks, per window its task and output segment, the
+// LPT order.  Returns SA_E_CAPACITY for a band wider than the kernel's widest ring.
 sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch *b) {
     sa_status st = SA_OK;
     b->n_reads = n_reads;
@@ -139,6 +175,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     b->read_status.assign(n_reads, SA_OK);
     b->read_first_region.assign(n_reads, 0);
     b->read_n_regions.assign(n_reads, 0);
+    b->read_win.assign(2 * n_reads, 0);
     b->read_scale.resize(n_reads);
     std::vector<Region> regs;
     PathTable pt;
@@ -147,6 +184,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         const sa_read &rd = reads[r];
         auto *sm = const_cast<sa_state_machine *>(rd.sm);
         b->read_first_region[r] = (int64_t) b->regions.size();
+        b->read_win[2 * r] = (int64_t) b->windows.size();
         if (!sm || rd.reference_length < 0 || rd.n_events < 0 || rd.n_anchors < 0 ||
             (rd.reference_length > 0 && !rd.reference) || (rd.n_events > 0 && !rd.events) ||
             (rd.n_anchors > 0 && !rd.anchors) || !(rd.var != 0.0)) {
@@ -185,6 +223,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         for (int64_t y = 0; y < rd.n_events; ++y)
             b->events.push_back(make_double2(rd.events[y * kEventParams], rd.events[y * kEventParams + 1]));
         for (const Region &rg : regs) {
+            const int32_t region = (int32_t) b->regions.size();
             RegionDesc d;
             std::memset(&d, 0, sizeof(d));
             d.n = (int32_t) (rg.lX + rg.lY);
@@ -202,14 +241,11 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
             d.event_base = event_base + rg.y1;
             d.x1 = rg.x1;
             d.y1 = rg.y1;
-            d.out_cap = 4 * (int64_t) d.n + 256;
-            d.out_base = b->out_total;
-            b->out_total += d.out_cap;
             // per anti-diagonal meta: band start, width, window end / refresh / stored gap states
             std::vector<int32_t> flags(d.n + 2, 0);
             for (const Window &w : rg.windows) {
                 flags[w.D] |= kFlagWindowEnd;
-                for (int32_t r = w.from; r > w.T; r -= 10) flags[r] |= kFlagRefresh;
+                for (int32_t q = w.from; q > w.T; q -= 10) flags[q] |= kFlagRefresh;
             }
             std::vector<int64_t> off(d.n + 1, 0);
             int64_t acc = 0;
@@ -221,17 +257,36 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
                 off[dd] = acc;
                 acc += w;
             }
-            for (const Window &w : rg.windows) b->window_off.push_back((int32_t) off[w.D]);
+            for (int32_t d0 = 0; d0 <= d.n; d0 += kChunkDiags) {
+                Chunk ch;
+                ch.region = region;
+                ch.d0 = d0;
+                ch.nd = std::min(kChunkDiags, d.n + 1 - d0);
+                ch.pad = 0;
+                ch.cell = d.cell_base + off[d0];
+                b->chunks.push_back(ch);
+            }
+            for (const Window &w : rg.windows) {
+                WindowTask t;
+                t.region = region;
+                t.first_cell = (int32_t) off[w.D];
+                t.out_cap = 4 * (w.from - w.T) + 64;
+                t.pad = 0;
+                t.out_base = b->out_total;
+                b->out_total += t.out_cap;
+                b->wtask.push_back(t);
+            }
             b->cells += acc;
             b->max_width = std::max(b->max_width, rg.max_width);
             b->windows.insert(b->windows.end(), rg.windows.begin(), rg.windows.end());
             b->regions.push_back(d);
         }
         b->read_n_regions[r] = (int64_t) b->regions.size() - b->read_first_region[r];
+        b->read_win[2 * r + 1] = (int64_t) b->windows.size() - b->read_win[2 * r];
     }
-    if (b->max_width > kMaxCpt * kGroup) return SA_E_CAPACITY;
+    if (b->max_width > kMaxCpt * kThreads) return SA_E_CAPACITY;
     b->device = device < 0 ? 0 : device;
-    // largest band area first (LPT order for the persistent CTAs)
+    // largest band area first (LPT order of the forward claims)
     b->order.resize(b->regions.size());
     std::iota(b->order.begin(), b->order.end(), 0);
     std::vector<int64_t> area(b->regions.size());
@@ -267,27 +322,10 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
         st = ensure_device_model(sm);
         if (st) { cudaSetDevice(prev); delete b; return st; }
     }
-    const size_t nd = b->meta.size();
-    st = SA_OK;
-    if (!st) st = dalloc(&b->d_regions, b->regions.size());
-    if (!st) st = dalloc(&b->d_order, b->order.size());
-    if (!st) st = dalloc(&b->d_models, b->models.size());
-    if (!st) st = dalloc(&b->d_read_scale, b->read_scale.size());
-    if (!st) st = dalloc(&b->d_meta, nd);
-    if (!st) st = dalloc(&b->d_window_off, b->window_off.size());
-    if (!st) st = dalloc(&b->d_windows, b->windows.size());
-    if (!st) st = dalloc(&b->d_kmer, b->kmer.size());
-    if (!st) st = dalloc(&b->d_gapx, b->gapx.size());
-    if (!st) st = dalloc(&b->d_events_raw, b->events.size());
-    if (!st) st = dalloc(&b->d_events, b->events.size());
-    if (!st) st = dalloc(&b->d_F, (size_t) kStoreStride * (size_t) b->cells);
-    if (!st) st = dalloc(&b->d_base, nd);
-    if (!st) st = dalloc(&b->d_fshift, nd);
-    if (!st) st = dalloc(&b->d_out, (size_t) b->out_total);
-    if (!st) st = dalloc(&b->d_out_count, b->regions.size());
-    if (!st) st = dalloc(&b->d_loglik, b->regions.size());
-    if (!st) st = dalloc(&b->d_status, (size_t) n_reads);
-    if (!st) st = dalloc(&b->d_queue, 1);
+    for_each_buffer(b, [&](auto *&ptr, size_t n) {
+        using T = std::remove_reference_t<decltype(*ptr)>;
+        if (!st && cudaMalloc((void **) &ptr, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) st = SA_E_NOMEM;
+    });
     cudaSetDevice(prev);
     if (st) {
         free_batch_device(b);
@@ -329,11 +367,13 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
     if (!st) st = h2d(b->d_models, md, s);
     if (!st) st = h2d(b->d_read_scale, b->read_scale, s);
     if (!st) st = h2d(b->d_meta, b->meta, s);
-    if (!st) st = h2d(b->d_window_off, b->window_off, s);
     if (!st) st = h2d(b->d_windows, b->windows, s);
+    if (!st) st = h2d(b->d_wtask, b->wtask, s);
+    if (!st) st = h2d(b->d_chunks, b->chunks, s);
     if (!st) st = h2d(b->d_kmer, b->kmer, s);
     if (!st) st = h2d(b->d_gapx, b->gapx, s);
     if (!st) st = h2d(b->d_events_raw, b->events, s);
+    if (!st) st = h2d(b->d_read_win, b->read_win, s);
     if (!st && !b->events.empty()) {
         const int64_t n = (int64_t) b->events.size();
         prep_events<<<(unsigned) std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(b->d_events_raw, b->d_events, n);
@@ -351,52 +391,70 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
     int prev = 0;
     cudaGetDevice(&prev);
     if (cudaSetDevice(b->device) != cudaSuccess) return SA_E_CUDA;
+    const size_t nr = b->regions.size(), nw = b->windows.size();
     sa_status st = SA_OK;
-    if (cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), s) != cudaSuccess ||
+    // what the kernels expect cleared: counters, per-read status, window counts, log-likelihoods,
+    // and the ready queue (-1 = empty)
+    if (cudaMemsetAsync(b->d_ctl, 0, sizeof(Control), s) != cudaSuccess ||
         cudaMemsetAsync(b->d_status, 0, sizeof(int32_t) * std::max<int64_t>(1, b->n_reads), s) != cudaSuccess ||
-        cudaMemsetAsync(b->d_out_count, 0, sizeof(int64_t) * std::max<size_t>(1, b->regions.size()), s) != cudaSuccess)
+        cudaMemsetAsync(b->d_wcount, 0, sizeof(int64_t) * std::max<size_t>(1, nw), s) != cudaSuccess ||
+        cudaMemsetAsync(b->d_loglik, 0, sizeof(double) * std::max<size_t>(1, nr), s) != cudaSuccess ||
+        cudaMemsetAsync(b->d_ready, 0xff, sizeof(int32_t) * std::max<size_t>(1, nw), s) != cudaSuccess)
         st = SA_E_CUDA;
-    if (!st && !b->regions.empty()) {
+    if (!st && nr > 0) {
         Args a;
         std::memset(&a, 0, sizeof(a));
         a.regions = b->d_regions;
         a.order = b->d_order;
-        a.n_regions = (int64_t) b->regions.size();
+        a.n_regions = (int64_t) nr;
         a.models = b->d_models;
         a.read_scale = b->d_read_scale;
         a.meta = b->d_meta;
-        a.window_off = b->d_window_off;
         a.windows = b->d_windows;
+        a.wtask = b->d_wtask;
+        a.n_windows = (int64_t) nw;
+        a.chunks = b->d_chunks;
+        a.n_chunks = (int64_t) b->chunks.size();
         a.kmer = b->d_kmer;
         a.gapx = b->d_gapx;
         a.events = b->d_events;
+        a.E = b->d_E;
         a.F = b->d_F;
         a.base = b->d_base;
         a.fshift = b->d_fshift;
+        a.ready = b->d_ready;
         a.out = b->d_out;
-        a.out_count = b->d_out_count;
+        a.wcount = b->d_wcount;
         a.loglik = b->d_loglik;
         a.status = b->d_status;
-        a.queue = b->d_queue;
+        a.ctl = b->d_ctl;
         a.threshold = b->threshold;
-        const int cpt = std::max(1, (b->max_width + kGroup - 1) / kGroup);
+        a.n_reads = b->n_reads;
+        a.read_win = b->d_read_win;
+        a.packed = b->d_packed;
+        a.read_base = b->d_read_base;
+        a.read_count = b->d_read_count;
+        const int cpt = std::max(1, (b->max_width + kThreads - 1) / kThreads);
         const int cpt_pow2 = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
-        a.wmax = cpt_pow2 * kGroup;
-        a.spin_limit = 20000000000LL;   // ~10 s at 2 GHz: far beyond any window's forward time
-        const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) (18 * (a.wmax + 2) + 2 * a.wmax);
+        a.wmax = cpt_pow2 * kThreads;
+        a.spin_limit = 20000000000LL;   // ~10 s at 2 GHz: far beyond any forward sweep
+        const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) (9 * (a.wmax + 2) + 2 * a.wmax);
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+        sms = std::max(1, sms);
+        emission_kernel<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(sms * 8, (a.n_chunks + 7) / 8)), 256, 0,
+                          s>>>(a);
         auto launch = [&](auto kern) {
             if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
-            int64_t grid = (int64_t) std::max(1, sms) * std::max(1, per_sm);
-            grid = std::min<int64_t>(grid, (int64_t) b->regions.size());
+            const int64_t grid = (int64_t) sms * std::max(1, per_sm);
             kern<<<(unsigned) grid, kThreads, smem, s>>>(a);
         };
-        if (cpt_pow2 == 1) launch(batch_kernel<1>);
-        else if (cpt_pow2 == 2) launch(batch_kernel<2>);
-        else launch(batch_kernel<4>);
-        count_launch();
+        if (cpt_pow2 == 1) launch(worker_kernel<1>);
+        else if (cpt_pow2 == 2) launch(worker_kernel<2>);
+        else launch(worker_kernel<4>);
+        gather_pairs<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(b->n_reads, sms * 4)), 256, 0, s>>>(a);
+        count_launch(3);
         if (cudaGetLastError() != cudaSuccess) st = SA_E_CUDA;
     }
     cudaSetDevice(prev);
@@ -410,46 +468,32 @@ sa_status sa_batch_download(sa_batch *b, void *stream) {
     int prev = 0;
     cudaGetDevice(&prev);
     if (cudaSetDevice(b->device) != cudaSuccess) return SA_E_CUDA;
-    const size_t nr = b->regions.size();
-    b->out_count.assign(nr, 0);
-    b->loglik.assign(nr, 0.0);
-    b->dev_status.assign(b->n_reads, 0);
+    const size_t nr = b->regions.size(), nreads = (size_t) b->n_reads;
     sa_status st = SA_OK;
-    if (nr) {
-        if (cudaMemcpyAsync(b->out_count.data(), b->d_out_count, nr * sizeof(int64_t), cudaMemcpyDeviceToHost, s) !=
-                cudaSuccess ||
-            cudaMemcpyAsync(b->loglik.data(), b->d_loglik, nr * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
-            st = SA_E_CUDA;
-    }
-    if (!st && b->n_reads &&
-        cudaMemcpyAsync(b->dev_status.data(), b->d_status, b->n_reads * sizeof(int32_t), cudaMemcpyDeviceToHost, s) !=
-            cudaSuccess)
+    b->ctl = Control{};
+    if (!st) st = d2h(b->read_base, b->d_read_base, nr ? nreads : 0, s);
+    if (!st) st = d2h(b->read_count, b->d_read_count, nr ? nreads : 0, s);
+    if (!st) st = d2h(b->loglik, b->d_loglik, nr, s);
+    if (!st) st = d2h(b->dev_status, b->d_status, nreads, s);
+    if (!st && nr && cudaMemcpyAsync(&b->ctl, b->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, s) != cudaSuccess)
         st = SA_E_CUDA;
     if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = SA_E_CUDA;
-    // pairs: one copy per region segment in use
-    b->read_pairs.assign(b->n_reads, {});
-    b->read_ll.assign(b->n_reads, 0.0);
-    for (int64_t r = 0; r < b->n_reads && !st; ++r) {
-        int64_t total = 0;
-        for (int64_t i = 0; i < b->read_n_regions[r]; ++i) {
-            const int64_t ri = b->read_first_region[r] + i;
-            total += std::min(b->out_count[ri], b->regions[ri].out_cap);
-        }
-        b->read_pairs[r].resize(total);
-        int64_t at = 0;
-        for (int64_t i = 0; i < b->read_n_regions[r]; ++i) {
-            const int64_t ri = b->read_first_region[r] + i;
-            const int64_t cnt = std::min(b->out_count[ri], b->regions[ri].out_cap);
-            if (cnt > 0 && cudaMemcpyAsync(b->read_pairs[r].data() + at, b->d_out + b->regions[ri].out_base,
-                                           cnt * sizeof(sa_aligned_pair), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
-                st = SA_E_CUDA;
-                break;
-            }
-            at += cnt;
-            b->read_ll[r] += b->loglik[ri];
-        }
+    if (!nr) {
+        b->read_base.assign(nreads, 0);
+        b->read_count.assign(nreads, 0);
     }
+    // the packed pairs in one copy, then split per read on the host
+    std::vector<sa_aligned_pair> packed;
+    if (!st) st = d2h(packed, b->d_packed, (size_t) b->ctl.packed, s);
     if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = SA_E_CUDA;
+    b->read_pairs.assign(nreads, {});
+    b->read_ll.assign(nreads, 0.0);
+    for (size_t r = 0; r < nreads && !st; ++r) {
+        const int64_t base = b->read_base[r], cnt = b->read_count[r];
+        if (cnt > 0 && base >= 0 && base + cnt <= (int64_t) packed.size())
+            b->read_pairs[r].assign(packed.begin() + base, packed.begin() + base + cnt);
+        for (int64_t i = 0; i < b->read_n_regions[r]; ++i) b->read_ll[r] += b->loglik[b->read_first_region[r] + i];
+    }
     cudaSetDevice(prev);
     b->downloaded = st == SA_OK;
     return st;
@@ -468,6 +512,7 @@ sa_status sa_batch_read_status(const sa_batch *b, int64_t read) {
     if (!b || read < 0 || read >= b->n_reads) return SA_E_ARG;
     if (b->read_status[read]) return (sa_status) b->read_status[read];
     if (!b->downloaded) return SA_E_ARG;
+    if (b->ctl.error) return SA_E_TIMEOUT;
     return (sa_status) b->dev_status[read];
 }
 
@@ -488,16 +533,16 @@ double sa_batch_log_likelihood(const sa_batch *b, int64_t read) {
 
 int64_t sa_batch_cells(const sa_batch *b) { return b ? b->cells : 0; }
 
-sa_status sa_batch_transfer_bytes(const sa_batch *b, int64_t *h2d, int64_t *d2h) {
-    if (!b || !h2d || !d2h) return SA_E_ARG;
+sa_status sa_batch_transfer_bytes(const sa_batch *b, int64_t *h2d_bytes, int64_t *d2h_bytes) {
+    if (!b || !h2d_bytes || !d2h_bytes) return SA_E_ARG;
     auto bytes = [](const auto &v) { return (int64_t) (v.size() * sizeof(v[0])); };
-    *h2d = bytes(b->regions) + bytes(b->order) + (int64_t) (b->models.size() * sizeof(ModelDesc)) +
-           bytes(b->read_scale) + bytes(b->meta) + bytes(b->window_off) + bytes(b->windows) + bytes(b->kmer) + bytes(b->gapx) +
-           bytes(b->events);
+    *h2d_bytes = bytes(b->regions) + bytes(b->order) + (int64_t) (b->models.size() * sizeof(ModelDesc)) +
+                 bytes(b->read_scale) + bytes(b->meta) + bytes(b->windows) + bytes(b->wtask) + bytes(b->chunks) +
+                 bytes(b->kmer) + bytes(b->gapx) + bytes(b->events) + bytes(b->read_win);
     int64_t pairs = 0;
     for (const auto &rp : b->read_pairs) pairs += (int64_t) rp.size();
-    *d2h = (int64_t) (b->regions.size() * (sizeof(int64_t) + sizeof(double))) + b->n_reads * (int64_t) sizeof(int32_t) +
-           pairs * (int64_t) sizeof(sa_aligned_pair);
+    *d2h_bytes = bytes(b->read_base) + bytes(b->read_count) + bytes(b->loglik) + bytes(b->dev_status) +
+                 (int64_t) sizeof(Control) + pairs * (int64_t) sizeof(sa_aligned_pair);
     return SA_OK;
 }
 
@@ -579,32 +624,12 @@ bool batch_models_resident(const sa_batch *b) {
 
 size_t batch_bind_scratch(sa_batch *b, unsigned char *base) {
     size_t at = 0;
-    auto carve = [&](auto **ptr, size_t n) {
-        using T = std::remove_reference_t<decltype(**ptr)>;
+    for_each_buffer(b, [&](auto *&ptr, size_t n) {
+        using T = std::remove_reference_t<decltype(*ptr)>;
         at = (at + 255) & ~(size_t) 255;
-        if (base) *ptr = reinterpret_cast<T *>(base + at);
+        if (base) ptr = reinterpret_cast<T *>(base + at);
         at += std::max<size_t>(n, 1) * sizeof(T);
-    };
-    const size_t nd = b->meta.size(), nr = b->regions.size();
-    carve(&b->d_regions, nr);
-    carve(&b->d_order, b->order.size());
-    carve(&b->d_models, b->models.size());
-    carve(&b->d_read_scale, b->read_scale.size());
-    carve(&b->d_meta, nd);
-    carve(&b->d_window_off, b->window_off.size());
-    carve(&b->d_windows, b->windows.size());
-    carve(&b->d_kmer, b->kmer.size());
-    carve(&b->d_gapx, b->gapx.size());
-    carve(&b->d_events_raw, b->events.size());
-    carve(&b->d_events, b->events.size());
-    carve(&b->d_F, (size_t) kStoreStride * (size_t) b->cells);
-    carve(&b->d_base, nd);
-    carve(&b->d_fshift, nd);
-    carve(&b->d_out, (size_t) b->out_total);
-    carve(&b->d_out_count, nr);
-    carve(&b->d_loglik, nr);
-    carve(&b->d_status, (size_t) b->n_reads);
-    carve(&b->d_queue, 1);
+    });
     return (at + 255) & ~(size_t) 255;
 }
 
