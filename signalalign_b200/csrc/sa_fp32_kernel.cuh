@@ -30,10 +30,11 @@
 // depend on the recursion are issued two anti-diagonals ahead from clamped (always valid) addresses
 // and masked where they are consumed.
 //
-// Values are log probabilities relative to a per-anti-diagonal FP64 base.  The base of d is the
-// base of d-2 plus the largest value computed on d-2 (a lagged renormalisation, so the max reduction
-// is off the critical path); the recorded bases are built from the same float shifts the kernel
-// applies, so they describe the stored values exactly.
+// Values are log probabilities relative to a per-anti-diagonal FP64 base.  The forward base of d is
+// the base of d-3 plus the largest value computed on d-3, the backward base of d the base of d+2
+// plus the largest value on d+2 (lagged renormalisations, so the max reductions are off the
+// critical path); the recorded bases are built from the same float shifts the kernel applies, so
+// they describe the stored values exactly.
 //
 // Stores, per anti-diagonal d with first cell c (region relative) and width W:
 //   emission store at 2c: [ match emission | extra-event emission ], W floats each;
@@ -168,13 +169,23 @@ __host__ __device__ inline void log_add_piece(int k, float4 &c) {
 }
 
 // logAdd in FP32: max(x, y) + h(|x - y|) below the 7.5 cut-off, max(x, y) at or above it (also
-// when the smaller argument is -inf: the difference is inf, or NaN if both are -inf)
+// when the smaller argument is -inf: the difference is inf, or NaN if both are -inf).
+// The table index ceil(2 d) comes from one add rounded toward +inf: 2 d + 2^23 lands on the
+// integer 2^23 + ceil(2 d) for 0 <= 2 d <= 15, whose low four bits are the index; beyond the
+// cut-off (or for inf / NaN) the low bits are some index in 0..15 whose value is discarded.
 __device__ __forceinline__ float lae(const float4 *tab, float x, float y) {
     const float mx = fmaxf(x, y), d = fabsf(x - y);
-    const int k = min(max(__float2int_ru(2.0f * d), 0), 15);
+    const int k = __float_as_int(__fmaf_ru(d, 2.0f, 8388608.0f)) & 15;
     const float4 c = tab[k];
     const float h = fmaf(fmaf(fmaf(c.x, d, c.y), d, c.z), d, c.w);
     return d < 7.5f ? mx + h : mx;
+}
+
+// warp-wide maximum in one instruction
+__device__ __forceinline__ float warp_max1(float v) {
+    float r;
+    asm volatile("redux.sync.max.f32 %0, %1, 0xffffffff;" : "=f"(r) : "f"(v));
+    return r;
 }
 
 __device__ __forceinline__ float warp_max(float v) {
@@ -443,19 +454,28 @@ __device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
     }
     int32_t eoffnn = eoffn + mn.W;            // first cell of d + 2
     float lm_prev = tid == 0 ? fmaxf(s0, s1) : kNegInf;   // local max of the previous anti-diagonal
-    float delta1 = 0.0f;      // base(d-1) - base(d-2)
-    double fbase = 0.0;       // base of d
+    // Renormalisation: base(d + 1) = base(d - 2) + max(d - 2), known one step ahead, so neither the
+    // reduction nor the shared-memory read of the warps' maxima sits on the recursion's path.
+    // delta(d) = base(d) - base(d-1) is a float and base(d) = base(d-1) + delta(d) exactly.
+    float delta0 = 0.0f, delta1 = 0.0f;   // delta(d), delta(d-1)
+    double base0 = 0.0, base1 = 0.0, base2 = 0.0;   // base(d), base(d-1), base(d-2)
     int32_t wi = 0;
     __syncthreads();
     for (int32_t d = 1; d <= n; ++d) {
-        // shift of this anti-diagonal: base(d) = base(d-2) + max(d-2)
-        float delta0 = 0.0f;
-        if (d > 2) {
+        // maximum of d-1 (one instruction per warp), published for the shift of d+2
+        {
+            const float wm = warp_max1(lm_prev);
+            if (lane == 0) sh->part[(d - 1) % 3][warp] = wm;
+        }
+        // shift of d+1 from the maximum of d-2 (complete since the last barrier)
+        float delta_next = 0.0f;
+        if (d >= 2) {
             const float *fp = sh->part[(d - 2) % 3];
             const float mx = fmaxf(fmaxf(fp[0], fp[1]), fmaxf(fp[2], fp[3]));
-            delta0 = (mx > kNegInf ? mx : 0.0f) - delta1;
+            delta_next = (float) (base2 + (double) (mx > kNegInf ? mx : 0.0f) - base0);
+        } else {
+            delta_next = (float) (0.0 - base0);
         }
-        fbase += (double) delta0;
         const Meta mnn = decode_meta(raw_nn, d + 2 <= n);
         raw_nn = raw_meta(A, db, d + 3, n);
         // loads two anti-diagonals ahead (consumed next step, masked there)
@@ -507,11 +527,6 @@ __device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
             }
             lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
         }
-        // lagged reduction of the previous anti-diagonal's maximum
-        {
-            const float wm = warp_max(lm_prev);
-            if (lane == 0) sh->part[(d - 1) % 3][warp] = wm;
-        }
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             eM[j] = rM1[j];
@@ -520,7 +535,7 @@ __device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
             rM1[j] = rM2[j]; rY1[j] = rY2[j]; rX1[j] = rX2[j]; vx1[j] = vx2[j];
         }
         if (tid == 0) {
-            A.base[db + d] = fbase;
+            A.base[db + d] = base0;
             A.fshift[db + d] = delta0;
         }
         const bool window_end = (m0.flags & kFlagWindowEnd) != 0;
@@ -533,6 +548,10 @@ __device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
         }
         lm_prev = lm;
         delta1 = delta0;
+        delta0 = delta_next;
+        base2 = base1;
+        base1 = base0;
+        base0 = base0 + (double) delta_next;
         Fd += 3 * W0;
         eoffnn += mnn.W;
         rg.rotate();
