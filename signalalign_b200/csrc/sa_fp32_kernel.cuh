@@ -389,135 +389,115 @@ __global__ void __launch_bounds__(256) emission_kernel(const __grid_constant__ A
 // ------------------------------------------------------------------------------------------------
 // forward sweep of one region
 // ------------------------------------------------------------------------------------------------
+// The sweep is unrolled by three anti-diagonals: ring slots, shared maxima and the look-ahead
+// registers are indexed by d mod 3 at compile time, so nothing rotates and every look-ahead load
+// has three anti-diagonals to land.
 template <int CPT>
-__device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
-    const Args &A = *c.A;
-    const RegionDesc &R = c.R;
-    const float *t = c.t;
-    const float4 *tab = sh->la;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wmax = A.wmax;
-    const int64_t db = R.diag_base;
-    const int32_t n = R.n;
-    float *Fd = A.F + 3 * R.cell_base;               // forward store of the anti-diagonal being computed
-    const float *Ereg = A.E + 2 * R.cell_base;
+struct ForwardSweep {
+    const Ctx &c;
+    const Args &A;
+    const RegionDesc &R;
+    Shared *sh;
+    float *ring;                  // 3 slots x 3 states x (wmax + 2); slot of d is (d - 1) mod 3
+    const float4 *tab;
+    int tid, lane, warp, wmax, stride;
+    int64_t db;
+    int32_t n;
+    float *Fd;                    // forward store of the anti-diagonal being computed
+    const float *Ereg;
+    // band facts: metas of d-2, d-1, d (m2, m1, m0); by phase, decoded metas of d+1 .. d+3 and
+    // raw metas of d+3 .. d+5 (loaded three steps before they are decoded)
+    Meta m2, m1, m0;
+    Meta near[3];
+    int2 raw[3];
+    int32_t eoff3;                // first cell of d+3
+    // look-ahead emissions by phase: match, extra event, skip (and whether the column exists)
+    float pM[3][CPT], pY[3][CPT], pX[3][CPT];
+    bool pV[3][CPT];
+    float lm_prev;
+    float delta0, delta1;
+    double base0, base1, base2;
+    int32_t wi;
 
-    ring_init(ring, wmax);
-    __syncthreads();
-    Ring rg;
-    rg.stride = wmax + 2;
-    // slot of d = 1 is s[0]; s[1] holds d = 0, s[2] holds d = -1 (all -inf)
-    rg.s[1] = ring + 1;
-    rg.s[2] = ring + 3 * rg.stride + 1;
-    rg.s[0] = ring + 6 * rg.stride + 1;
+    __device__ __forceinline__ ForwardSweep(const Ctx &cc, Shared *s, float *r)
+        : c(cc), A(*cc.A), R(cc.R), sh(s), ring(r) {}
 
-    // anti-diagonal 0: startStateProb / raggedStartStateProb (stateMachine.c:1022-1032)
-    const float s0 = R.ragged_left ? kNegInf : 0.0f, s1 = R.ragged_left ? 0.0f : kNegInf;
-    if (tid == 0) {
-        Fd[ST_M] = s0; Fd[ST_X] = s1; Fd[ST_Y] = s1;
-        rg.st(1, 0)[0] = s0;
-        rg.st(1, 1)[0] = s1;
-        rg.st(1, 2)[0] = s1;
-        A.base[db] = 0.0;
-        A.fshift[db] = 0.0f;
-    }
-    Fd += 3;   // anti-diagonal 0 has one cell
-    Meta m2{0, 0, 0};
-    Meta m1 = decode_meta(raw_meta(A, db, 0, n), true), m0 = decode_meta(raw_meta(A, db, 1, n), 1 <= n);
-    Meta mn = decode_meta(raw_meta(A, db, 2, n), 2 <= n);
-    int2 raw_nn = raw_meta(A, db, 3, n);      // meta of d+2, decoded at the top of each step
-    // emissions of the current anti-diagonal's cells (masked), and raw ones of the next
-    float eX[CPT], eM[CPT], eY[CPT];
-    float rX1[CPT], rM1[CPT], rY1[CPT];
-    bool vx1[CPT];
-    const int32_t eoff1 = 1;                  // region-relative first cell of d = 1
-    const int32_t eoffn = eoff1 + m0.W;       // of d = 2
+    __device__ __forceinline__ float *slot(int k, int state) const { return ring + (k * 3 + state) * stride + 1; }
+
+    // issue the look-ahead loads of anti-diagonal dd (meta m, first cell off) into phase P
+    template <int P>
+    __device__ __forceinline__ void prefetch(int32_t dd, const Meta &m, int32_t off) {
 #pragma unroll
-    for (int j = 0; j < CPT; ++j) {
-        const int i = tid + j * kThreads;
-        {
-            const int32_t xmy = m0.L + 2 * i, x = (1 + xmy) >> 1;
-            const int ic = clampi(i, 0, max(m0.W - 1, 0));
-            eM[j] = __ldg(Ereg + 2 * eoff1 + SE_M * m0.W + ic);
-            eY[j] = __ldg(Ereg + 2 * eoff1 + SE_Y * m0.W + ic);
-            const float gx = raw_gapx(c, x);
-            eX[j] = x >= 1 ? gx : kNegInf;
-        }
-        {
-            const int32_t xmy = mn.L + 2 * i, x = (2 + xmy) >> 1;
-            const int ic = clampi(i, 0, max(mn.W - 1, 0));
-            rM1[j] = __ldg(Ereg + 2 * eoffn + SE_M * mn.W + ic);
-            rY1[j] = __ldg(Ereg + 2 * eoffn + SE_Y * mn.W + ic);
-            rX1[j] = raw_gapx(c, x);
-            vx1[j] = x >= 1;
+        for (int j = 0; j < CPT; ++j) {
+            const int i = tid + j * kThreads;
+            const int32_t xmy = m.L + 2 * i, x = (dd + xmy) >> 1;
+            const int ic = clampi(i, 0, max(m.W - 1, 0));
+            pM[P][j] = __ldg(Ereg + 2 * off + SE_M * m.W + ic);
+            pY[P][j] = __ldg(Ereg + 2 * off + SE_Y * m.W + ic);
+            pX[P][j] = raw_gapx(c, x);
+            pV[P][j] = x >= 1;
         }
     }
-    int32_t eoffnn = eoffn + mn.W;            // first cell of d + 2
-    float lm_prev = tid == 0 ? fmaxf(s0, s1) : kNegInf;   // local max of the previous anti-diagonal
-    // Renormalisation: base(d + 1) = base(d - 2) + max(d - 2), known one step ahead, so neither the
-    // reduction nor the shared-memory read of the warps' maxima sits on the recursion's path.
-    // delta(d) = base(d) - base(d-1) is a float and base(d) = base(d-1) + delta(d) exactly.
-    float delta0 = 0.0f, delta1 = 0.0f;   // delta(d), delta(d-1)
-    double base0 = 0.0, base1 = 0.0, base2 = 0.0;   // base(d), base(d-1), base(d-2)
-    int32_t wi = 0;
-    __syncthreads();
-    for (int32_t d = 1; d <= n; ++d) {
+
+    template <int P>
+    __device__ __forceinline__ void step(int32_t d) {
+        constexpr int S0 = P, S1 = (P + 2) % 3, S2 = (P + 1) % 3;   // slots of d, d-1, d-2
+        const float *t = c.t;
         // maximum of d-1 (one instruction per warp), published for the shift of d+2
         {
             const float wm = warp_max1(lm_prev);
-            if (lane == 0) sh->part[(d - 1) % 3][warp] = wm;
+            if (lane == 0) sh->part[S1][warp] = wm;
         }
         // shift of d+1 from the maximum of d-2 (complete since the last barrier)
-        float delta_next = 0.0f;
+        float delta_next;
         if (d >= 2) {
-            const float *fp = sh->part[(d - 2) % 3];
+            const float *fp = sh->part[S2];
             const float mx = fmaxf(fmaxf(fp[0], fp[1]), fmaxf(fp[2], fp[3]));
             delta_next = (float) (base2 + (double) (mx > kNegInf ? mx : 0.0f) - base0);
         } else {
             delta_next = (float) (0.0 - base0);
         }
-        const Meta mnn = decode_meta(raw_nn, d + 2 <= n);
-        raw_nn = raw_meta(A, db, d + 3, n);
-        // loads two anti-diagonals ahead (consumed next step, masked there)
-        float rX2[CPT], rM2[CPT], rY2[CPT];
-        bool vx2[CPT];
+        // band facts: d+3 decoded (loaded three steps ago), d+6 requested
+        const Meta m3 = decode_meta(raw[P], d + 3 <= n);
+        near[P] = m3;
+        raw[P] = raw_meta(A, db, d + 6, n);
+        // emissions of d (landed), then the loads of d+3 into the same phase
+        float eM[CPT], eY[CPT], eX[CPT];
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
-            const int i = tid + j * kThreads;
-            const int32_t xmy = mnn.L + 2 * i, x = (d + 2 + xmy) >> 1;
-            const int ic = clampi(i, 0, max(mnn.W - 1, 0));
-            rM2[j] = __ldg(Ereg + 2 * eoffnn + SE_M * mnn.W + ic);
-            rY2[j] = __ldg(Ereg + 2 * eoffnn + SE_Y * mnn.W + ic);
-            rX2[j] = raw_gapx(c, x);
-            vx2[j] = x >= 1;
+            eM[j] = pM[P][j];
+            eY[j] = pY[P][j];
+            eX[j] = pV[P][j] ? pX[P][j] : kNegInf;
         }
-        // the recursion on anti-diagonal d (stateMachine3_cellCalculate order: lower -> gap-X,
-        // middle -> match, upper -> gap-Y, each state accumulated from LOG_ZERO)
+        prefetch<P>(d + 3, m3, eoff3);
+        eoff3 += m3.W;
+        // the recursion on d (stateMachine3_cellCalculate order: lower -> gap-X, middle -> match,
+        // upper -> gap-Y, each state accumulated from LOG_ZERO)
         const int32_t W0 = m0.W;
         const float shL = -delta0, shM = -delta1 - delta0;
         const bool store_gaps = (m0.flags & kFlagStoreGaps) != 0;
+        const int32_t dl = (m0.L - 1 - m1.L) >> 1, du = (m0.L + 1 - m1.L) >> 1, dm = (m0.L - m2.L) >> 1;
         float lm = kNegInf;
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             const int i = tid + j * kThreads;
-            const int32_t xmy = m0.L + 2 * i;
-            const int il = clampi((xmy - 1 - m1.L) >> 1, -1, wmax);
-            const int iu = clampi((xmy + 1 - m1.L) >> 1, -1, wmax);
-            const int im = clampi((xmy - m2.L) >> 1, -1, wmax);
+            const int il = clampi(i + dl, -1, wmax);
+            const int iu = clampi(i + du, -1, wmax);
+            const int im = clampi(i + dm, -1, wmax);
             const float ex = eX[j] + shL, em = eM[j] + shM, ey = eY[j] + shL;
-            float vX = rg.st(1, 0)[il] + (ex + t[T_OX]);
-            vX = lae(tab, vX, rg.st(1, 1)[il] + (ex + t[T_EX]));
-            vX = lae(tab, vX, rg.st(1, 2)[il] + (ex + t[T_SX]));
-            float vM = rg.st(2, 0)[im] + (em + t[T_MC]);
-            vM = lae(tab, vM, rg.st(2, 1)[im] + (em + t[T_MFGX]));
-            vM = lae(tab, vM, rg.st(2, 2)[im] + (em + t[T_MFGY]));
-            float vY = rg.st(1, 0)[iu] + (ey + t[T_OY]);
-            vY = lae(tab, vY, rg.st(1, 2)[iu] + (ey + t[T_EY]));
+            float vX = slot(S1, 0)[il] + (ex + t[T_OX]);
+            vX = lae(tab, vX, slot(S1, 1)[il] + (ex + t[T_EX]));
+            vX = lae(tab, vX, slot(S1, 2)[il] + (ex + t[T_SX]));
+            float vM = slot(S2, 0)[im] + (em + t[T_MC]);
+            vM = lae(tab, vM, slot(S2, 1)[im] + (em + t[T_MFGX]));
+            vM = lae(tab, vM, slot(S2, 2)[im] + (em + t[T_MFGY]));
+            float vY = slot(S1, 0)[iu] + (ey + t[T_OY]);
+            vY = lae(tab, vY, slot(S1, 2)[iu] + (ey + t[T_EY]));
             const bool in = i < W0;
             if (!in) vM = vX = vY = kNegInf;
-            rg.st(0, 0)[i] = vM;
-            rg.st(0, 1)[i] = vX;
-            rg.st(0, 2)[i] = vY;
+            slot(S0, 0)[i] = vM;
+            slot(S0, 1)[i] = vX;
+            slot(S0, 2)[i] = vY;
             if (in) {
                 Fd[ST_M * W0 + i] = vM;
                 if (store_gaps) {
@@ -527,13 +507,6 @@ __device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
             }
             lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
         }
-#pragma unroll
-        for (int j = 0; j < CPT; ++j) {
-            eM[j] = rM1[j];
-            eY[j] = rY1[j];
-            eX[j] = vx1[j] ? rX1[j] : kNegInf;
-            rM1[j] = rM2[j]; rY1[j] = rY2[j]; rX1[j] = rX2[j]; vx1[j] = vx2[j];
-        }
         if (tid == 0) {
             A.base[db + d] = base0;
             A.fshift[db + d] = delta0;
@@ -542,8 +515,8 @@ __device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
         if (window_end) __threadfence();   // this anti-diagonal and all before it, device-wide
         __syncthreads();
         if (window_end && tid == 0) {
-            const unsigned slot = atomicAdd(&A.ctl->pub, 1u);
-            atomicExch(A.ready + slot, (int32_t) (R.win_base + wi));
+            const unsigned q = atomicAdd(&A.ctl->pub, 1u);
+            atomicExch(A.ready + q, (int32_t) (R.win_base + wi));
             ++wi;
         }
         lm_prev = lm;
@@ -553,10 +526,77 @@ __device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
         base1 = base0;
         base0 = base0 + (double) delta_next;
         Fd += 3 * W0;
-        eoffnn += mnn.W;
-        rg.rotate();
-        m2 = m1; m1 = m0; m0 = mn; mn = mnn;
+        m2 = m1;
+        m1 = m0;
+        m0 = near[(P + 1) % 3];   // meta of d+1, decoded two steps ago
     }
+
+    __device__ void run() {
+        tab = sh->la;
+        tid = threadIdx.x;
+        lane = tid & 31;
+        warp = tid >> 5;
+        wmax = A.wmax;
+        stride = wmax + 2;
+        db = R.diag_base;
+        n = R.n;
+        Fd = A.F + 3 * R.cell_base;
+        Ereg = A.E + 2 * R.cell_base;
+        ring_init(ring, wmax);
+        __syncthreads();
+        // anti-diagonal 0 (slot 2): startStateProb / raggedStartStateProb (stateMachine.c:1022-1032)
+        const float s0 = R.ragged_left ? kNegInf : 0.0f, s1 = R.ragged_left ? 0.0f : kNegInf;
+        if (tid == 0) {
+            Fd[ST_M] = s0; Fd[ST_X] = s1; Fd[ST_Y] = s1;
+            slot(2, 0)[0] = s0;
+            slot(2, 1)[0] = s1;
+            slot(2, 2)[0] = s1;
+            A.base[db] = 0.0;
+            A.fshift[db] = 0.0f;
+        }
+        Fd += 3;   // anti-diagonal 0 has one cell
+        m2 = Meta{0, 0, 0};
+        m1 = decode_meta(raw_meta(A, db, 0, n), true);
+        m0 = decode_meta(raw_meta(A, db, 1, n), 1 <= n);
+        const Meta ma = decode_meta(raw_meta(A, db, 2, n), 2 <= n);
+        const Meta mb = decode_meta(raw_meta(A, db, 3, n), 3 <= n);
+        // look-ahead of d = 1, 2, 3 (phases 0, 1, 2); metas of d = 2, 3 decoded, 4, 5, 6 raw
+        int32_t off = 1;
+        prefetch<0>(1, m0, off);
+        off += m0.W;
+        prefetch<1>(2, ma, off);
+        off += ma.W;
+        prefetch<2>(3, mb, off);
+        off += mb.W;
+        eoff3 = off;   // first cell of d = 4
+        near[0] = Meta{0, 0, 0};
+        near[1] = ma;
+        near[2] = mb;
+        raw[0] = raw_meta(A, db, 4, n);
+        raw[1] = raw_meta(A, db, 5, n);
+        raw[2] = raw_meta(A, db, 6, n);
+        lm_prev = tid == 0 ? fmaxf(s0, s1) : kNegInf;
+        // Renormalisation: base(d + 1) = base(d - 2) + max(d - 2), known one step ahead, so neither
+        // the reduction nor the shared-memory read of the warps' maxima sits on the recursion's
+        // path.  delta(d) = base(d) - base(d-1) is a float and base(d) = base(d-1) + delta(d).
+        delta0 = delta1 = 0.0f;
+        base0 = base1 = base2 = 0.0;
+        wi = 0;
+        __syncthreads();
+        for (int32_t d = 1; d <= n; d += 3) {
+            step<0>(d);
+            if (d + 1 > n) break;
+            step<1>(d + 1);
+            if (d + 2 > n) break;
+            step<2>(d + 2);
+        }
+    }
+};
+
+template <int CPT>
+__device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
+    ForwardSweep<CPT> f(c, sh, ring);
+    f.run();
 }
 
 // ------------------------------------------------------------------------------------------------
