@@ -415,8 +415,8 @@ struct ForwardSweep {
     float pM[3][CPT], pY[3][CPT], pX[3][CPT];
     bool pV[3][CPT];
     float lm_prev;
-    float delta0, delta1;
-    double base0, base1, base2;
+    float delta0, delta1;         // delta(d) = base(d) - base(d-1), delta(d-1)
+    double base0;                 // base(d)
     int32_t wi;
 
     __device__ __forceinline__ ForwardSweep(const Ctx &cc, Shared *s, float *r)
@@ -448,14 +448,13 @@ struct ForwardSweep {
             const float wm = warp_max1(lm_prev);
             if (lane == 0) sh->part[S1][warp] = wm;
         }
-        // shift of d+1 from the maximum of d-2 (complete since the last barrier)
-        float delta_next;
+        // shift of d+1 from the maximum of d-2 (complete since the last barrier):
+        // base(d+1) - base(d) = max(d-2) - delta(d) - delta(d-1)
+        float delta_next = 0.0f;
         if (d >= 2) {
             const float *fp = sh->part[S2];
             const float mx = fmaxf(fmaxf(fp[0], fp[1]), fmaxf(fp[2], fp[3]));
-            delta_next = (float) (base2 + (double) (mx > kNegInf ? mx : 0.0f) - base0);
-        } else {
-            delta_next = (float) (0.0 - base0);
+            delta_next = ((mx > kNegInf ? mx : 0.0f) - delta0) - delta1;
         }
         // band facts: d+3 decoded (loaded three steps ago), d+6 requested
         const Meta m3 = decode_meta(raw[P], d + 3 <= n);
@@ -484,28 +483,27 @@ struct ForwardSweep {
             const int il = clampi(i + dl, -1, wmax);
             const int iu = clampi(i + du, -1, wmax);
             const int im = clampi(i + dm, -1, wmax);
-            const float ex = eX[j] + shL, em = eM[j] + shM, ey = eY[j] + shL;
-            float vX = slot(S1, 0)[il] + (ex + t[T_OX]);
-            vX = lae(tab, vX, slot(S1, 1)[il] + (ex + t[T_EX]));
-            vX = lae(tab, vX, slot(S1, 2)[il] + (ex + t[T_SX]));
-            float vM = slot(S2, 0)[im] + (em + t[T_MC]);
-            vM = lae(tab, vM, slot(S2, 1)[im] + (em + t[T_MFGX]));
-            vM = lae(tab, vM, slot(S2, 2)[im] + (em + t[T_MFGY]));
-            float vY = slot(S1, 0)[iu] + (ey + t[T_OY]);
-            vY = lae(tab, vY, slot(S1, 2)[iu] + (ey + t[T_EY]));
+            // logAdd depends only on the difference of its arguments, so the cell's emission (and
+            // the shift to this anti-diagonal's base) is added once after each state's fold
+            float vX = lae(tab, slot(S1, 0)[il] + t[T_OX], slot(S1, 1)[il] + t[T_EX]);
+            vX = lae(tab, vX, slot(S1, 2)[il] + t[T_SX]) + (eX[j] + shL);
+            float vM = lae(tab, slot(S2, 0)[im] + t[T_MC], slot(S2, 1)[im] + t[T_MFGX]);
+            vM = lae(tab, vM, slot(S2, 2)[im] + t[T_MFGY]) + (eM[j] + shM);
+            const float vY = lae(tab, slot(S1, 0)[iu] + t[T_OY], slot(S1, 2)[iu] + t[T_EY]) + (eY[j] + shL);
             const bool in = i < W0;
-            if (!in) vM = vX = vY = kNegInf;
+            if (!in) vM = vX = kNegInf;
+            const float vYs = in ? vY : kNegInf;
             slot(S0, 0)[i] = vM;
             slot(S0, 1)[i] = vX;
-            slot(S0, 2)[i] = vY;
+            slot(S0, 2)[i] = vYs;
             if (in) {
                 Fd[ST_M * W0 + i] = vM;
                 if (store_gaps) {
                     Fd[ST_X * W0 + i] = vX;
-                    Fd[ST_Y * W0 + i] = vY;
+                    Fd[ST_Y * W0 + i] = vYs;
                 }
             }
-            lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
+            lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vYs)));
         }
         if (tid == 0) {
             A.base[db + d] = base0;
@@ -522,9 +520,7 @@ struct ForwardSweep {
         lm_prev = lm;
         delta1 = delta0;
         delta0 = delta_next;
-        base2 = base1;
-        base1 = base0;
-        base0 = base0 + (double) delta_next;
+        base0 += (double) delta_next;   // only thread 0 stores it
         Fd += 3 * W0;
         m2 = m1;
         m1 = m0;
@@ -580,7 +576,7 @@ struct ForwardSweep {
         // the reduction nor the shared-memory read of the warps' maxima sits on the recursion's
         // path.  delta(d) = base(d) - base(d-1) is a float and base(d) = base(d-1) + delta(d).
         delta0 = delta1 = 0.0f;
-        base0 = base1 = base2 = 0.0;
+        base0 = 0.0;
         wi = 0;
         __syncthreads();
         for (int32_t d = 1; d <= n; d += 3) {
@@ -792,20 +788,18 @@ __device__ void window_task(const Ctx &c, Shared *sh, float *ring, float *chain,
                 const int ipp = clampi((xmy - mpp.L) >> 1, -1, wmax);
                 const int iu = clampi((xmy - 1 - mp.L) >> 1, -1, wmax);
                 const int il = clampi((xmy + 1 - mp.L) >> 1, -1, wmax);
-                const float bm = rg.st(2, 0)[ipp];
-                const float em = eMm[j] + shM;
-                float vM = bm + (em + t[T_MC]);
-                float vX = bm + (em + t[T_MFGX]);
-                float vY = bm + (em + t[T_MFGY]);
-                const float bu = rg.st(1, 2)[iu];
-                const float ey = eYu[j] + shU;
-                vM = lae(tab, vM, bu + (ey + t[T_OY]));
-                vY = lae(tab, vY, bu + (ey + t[T_EY]));
-                const float bl = rg.st(1, 1)[il];
-                const float ex = eXl[j] + shU;
-                vM = lae(tab, vM, bl + (ex + t[T_OX]));
-                vX = lae(tab, vX, bl + (ex + t[T_EX]));
-                vY = lae(tab, vY, bl + (ex + t[T_SX]));
+                // each successor's backward value plus its emission, shared by the transitions into it
+                const float bme = rg.st(2, 0)[ipp] + (eMm[j] + shM);
+                float vM = bme + t[T_MC];
+                float vX = bme + t[T_MFGX];
+                float vY = bme + t[T_MFGY];
+                const float bue = rg.st(1, 2)[iu] + (eYu[j] + shU);
+                vM = lae(tab, vM, bue + t[T_OY]);
+                vY = lae(tab, vY, bue + t[T_EY]);
+                const float ble = rg.st(1, 1)[il] + (eXl[j] + shU);
+                vM = lae(tab, vM, ble + t[T_OX]);
+                vX = lae(tab, vX, ble + t[T_EX]);
+                vY = lae(tab, vY, ble + t[T_SX]);
                 if (i >= W0) vM = vX = vY = kNegInf;
                 rg.st(0, 0)[i] = vM;
                 rg.st(0, 1)[i] = vX;
