@@ -3,14 +3,18 @@
 // sa_fp32_kernel.cuh: emissions of every band cell, the persistent worker (forward sweeps and
 // traceback-window backward sweeps pulled from a device queue), and the per-read gather of pairs.
 //
-// Every device buffer of a batch is listed once (for_each_buffer), so the allocating path
-// (sa_batch_create) and the path that carves them from caller-provided memory
-// (batch_bind_scratch) lay out the same set.
+// Every buffer of a batch is placed by one function (layout): the inputs first, staged on the host
+// in exactly the device layout so that one copy uploads them; then the small results block, which
+// one copy downloads; then the device-only stores.  The device block and the pinned host blocks
+// come from reusable pools (sa_memory.cpp); the no-allocation entry lays the same set out in its
+// static array and stages on the heap.  Host planning runs on all host threads.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -59,27 +63,48 @@ constexpr size_t kStoreSlack = 1024;
 using namespace sa;
 using namespace sa::fp32;
 
+// a typed view into a host block
+template <typename T>
+struct Span {
+    T *p = nullptr;
+    size_t n = 0;
+    T *data() const { return p; }
+    size_t size() const { return n; }
+    T &operator[](size_t i) const { return p[i]; }
+};
+
 struct sa_batch {
     int device = 0;
     int64_t n_reads = 0;
+    bool host_pinned = true;      // staging and results in pinned pool blocks (else heap)
+    bool owns_device = true;      // device block from the pool (else memory of the caller)
     std::vector<sa_state_machine *> models;
-    std::vector<RegionDesc> regions;
-    std::vector<int32_t> order;
     std::vector<int32_t> read_status;       // host planning status per read
     std::vector<int64_t> read_first_region, read_n_regions;
-    std::vector<int64_t> read_win;          // per read: first window, window count
-    std::vector<ReadScale32> read_scale;
-    std::vector<int2> meta;
-    std::vector<Window> windows;
-    std::vector<WindowTask> wtask;
-    std::vector<Chunk> chunks;
-    std::vector<int32_t> kmer;
-    std::vector<float> gapx;
-    std::vector<double2> events;
+    int64_t n_regions = 0, n_diags = 0, n_windows = 0, n_chunks = 0, n_kmers = 0, n_events = 0;
     int64_t cells = 0, out_total = 0;
     int32_t max_width = 0;
     float threshold = 0.01f;
-    // device
+    // inputs, staged on the host with the device layout (one copy uploads them all)
+    Span<RegionDesc> regions;
+    Span<int32_t> order;
+    Span<ModelDesc> mdesc;
+    Span<ReadScale32> read_scale;
+    Span<int2> meta;
+    Span<Window> windows;
+    Span<WindowTask> wtask;
+    Span<Chunk> chunks;
+    Span<int32_t> kmer;
+    Span<float> gapx;
+    Span<double2> events;
+    Span<int64_t> read_win;                 // per read: first window, window count
+    // results, mirrored from one contiguous device range (one copy downloads them all)
+    Span<int64_t> read_base, read_count;
+    Span<double> loglik;
+    Span<int32_t> dev_status;
+    Span<Control> ctl;
+    size_t in_bytes = 0, res_off = 0, res_bytes = 0, dev_bytes = 0;
+    // device pointers
     RegionDesc *d_regions = nullptr;
     int32_t *d_order = nullptr;
     ModelDesc *d_models = nullptr;
@@ -91,139 +116,250 @@ struct sa_batch {
     int32_t *d_kmer = nullptr;
     float *d_gapx = nullptr;
     double2 *d_events_raw = nullptr;
+    int64_t *d_read_win = nullptr;
+    int64_t *d_read_base = nullptr, *d_read_count = nullptr;
+    double *d_loglik = nullptr;
+    int32_t *d_status = nullptr;
+    Control *d_ctl = nullptr;
     Event32 *d_events = nullptr;
     float *d_E = nullptr, *d_F = nullptr, *d_fshift = nullptr;
-    double *d_base = nullptr, *d_loglik = nullptr;
-    int32_t *d_ready = nullptr, *d_status = nullptr;
+    double *d_base = nullptr;
+    int32_t *d_ready = nullptr;
     sa_aligned_pair *d_out = nullptr, *d_packed = nullptr;
-    int64_t *d_wcount = nullptr, *d_read_win = nullptr, *d_read_base = nullptr, *d_read_count = nullptr;
-    Control *d_ctl = nullptr;
-    // results
-    std::vector<int64_t> read_base, read_count;
-    std::vector<double> loglik;
-    std::vector<int32_t> dev_status;
-    Control ctl{};
-    std::vector<std::vector<sa_aligned_pair>> read_pairs;
+    int64_t *d_wcount = nullptr;
+    // memory
+    MemBlock host_in, host_res, host_pairs, dev;
+    unsigned char *dev_base = nullptr;
     std::vector<double> read_ll;
     bool downloaded = false;
+
+    ~sa_batch() {
+        mem_put(host_in);
+        mem_put(host_res);
+        mem_put(host_pairs);
+        if (owns_device) mem_put(dev);
+    }
 };
 
 namespace {
 
-// Calls fn(pointer, element count) for every device buffer of the batch.
+// Lays out the batch's buffers, 256-byte aligned, in three groups: inputs (staged on the host in
+// the same layout), results (mirrored to the host), work buffers (device only).  With non-null bases
+// the host spans and device pointers are set.  Returns the device bytes; sets in/res offsets.
+size_t layout(sa_batch *b, unsigned char *host_in, unsigned char *host_res, unsigned char *dev) {
+    size_t at = 0;
+    auto place = [&](auto &span, auto *&dptr, size_t n, unsigned char *host, size_t host_origin) {
+        using T = std::remove_reference_t<decltype(*dptr)>;
+        at = (at + 255) & ~(size_t) 255;
+        if (host) {
+            span.p = reinterpret_cast<T *>(host + (at - host_origin));
+            span.n = n;
+        }
+        if (dev) dptr = reinterpret_cast<T *>(dev + at);
+        at += std::max<size_t>(n, 1) * sizeof(T);
+    };
+    auto work = [&](auto *&dptr, size_t n) {
+        using T = std::remove_reference_t<decltype(*dptr)>;
+        at = (at + 255) & ~(size_t) 255;
+        if (dev) dptr = reinterpret_cast<T *>(dev + at);
+        at += std::max<size_t>(n, 1) * sizeof(T);
+    };
+    const size_t nr = (size_t) b->n_regions, nd = (size_t) b->n_diags, nw = (size_t) b->n_windows;
+    const size_t nreads = (size_t) b->n_reads, cells = (size_t) b->cells;
+    place(b->regions, b->d_regions, nr, host_in, 0);
+    place(b->order, b->d_order, nr, host_in, 0);
+    place(b->mdesc, b->d_models, b->models.size(), host_in, 0);
+    place(b->read_scale, b->d_read_scale, nreads, host_in, 0);
+    place(b->meta, b->d_meta, nd, host_in, 0);
+    place(b->windows, b->d_windows, nw, host_in, 0);
+    place(b->wtask, b->d_wtask, nw, host_in, 0);
+    place(b->chunks, b->d_chunks, (size_t) b->n_chunks, host_in, 0);
+    place(b->kmer, b->d_kmer, (size_t) b->n_kmers, host_in, 0);
+    place(b->gapx, b->d_gapx, (size_t) b->n_kmers, host_in, 0);
+    place(b->events, b->d_events_raw, (size_t) b->n_events, host_in, 0);
+    place(b->read_win, b->d_read_win, 2 * nreads, host_in, 0);
+    b->in_bytes = (at + 255) & ~(size_t) 255;
+    at = b->in_bytes;
+    b->res_off = at;
+    place(b->read_base, b->d_read_base, nreads, host_res, b->res_off);
+    place(b->read_count, b->d_read_count, nreads, host_res, b->res_off);
+    place(b->loglik, b->d_loglik, nr, host_res, b->res_off);
+    place(b->dev_status, b->d_status, nreads, host_res, b->res_off);
+    place(b->ctl, b->d_ctl, 1, host_res, b->res_off);
+    b->res_bytes = ((at + 255) & ~(size_t) 255) - b->res_off;
+    work(b->d_events, (size_t) b->n_events);
+    work(b->d_E, 2 * cells + kStoreSlack);
+    work(b->d_F, 3 * cells + kStoreSlack);
+    work(b->d_base, nd);
+    work(b->d_fshift, nd);
+    work(b->d_ready, nw);
+    work(b->d_out, (size_t) b->out_total);
+    work(b->d_wcount, nw);
+    work(b->d_packed, (size_t) b->out_total);
+    b->dev_bytes = (at + 255) & ~(size_t) 255;
+    return b->dev_bytes;
+}
+
+// Runs fn(i) for i in [0, n) on up to `threads` host threads (the calling thread included).
 template <typename Fn>
-void for_each_buffer(sa_batch *b, Fn &&fn) {
-    const size_t nr = b->regions.size(), nd = b->meta.size(), nw = b->windows.size(), nreads = (size_t) b->n_reads;
-    const size_t cells = (size_t) b->cells;
-    fn(b->d_regions, nr);
-    fn(b->d_order, b->order.size());
-    fn(b->d_models, b->models.size());
-    fn(b->d_read_scale, b->read_scale.size());
-    fn(b->d_meta, nd);
-    fn(b->d_windows, nw);
-    fn(b->d_wtask, nw);
-    fn(b->d_chunks, b->chunks.size());
-    fn(b->d_kmer, b->kmer.size());
-    fn(b->d_gapx, b->gapx.size());
-    fn(b->d_events_raw, b->events.size());
-    fn(b->d_events, b->events.size());
-    fn(b->d_E, 2 * cells + kStoreSlack);
-    fn(b->d_F, 3 * cells + kStoreSlack);
-    fn(b->d_base, nd);
-    fn(b->d_fshift, nd);
-    fn(b->d_ready, nw);
-    fn(b->d_out, (size_t) b->out_total);
-    fn(b->d_wcount, nw);
-    fn(b->d_loglik, nr);
-    fn(b->d_status, nreads);
-    fn(b->d_ctl, (size_t) 1);
-    fn(b->d_read_win, 2 * nreads);
-    fn(b->d_packed, (size_t) b->out_total);
-    fn(b->d_read_base, nreads);
-    fn(b->d_read_count, nreads);
+void parallel_for(int64_t n, int threads, Fn &&fn) {
+    threads = (int) std::max<int64_t>(1, std::min<int64_t>(threads, n));
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        for (int64_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) fn(i);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &th : pool) th.join();
 }
 
-template <typename T>
-sa_status h2d(T *dst, const std::vector<T> &src, cudaStream_t s) {
-    if (src.empty()) return SA_OK;
-    return cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, s) == cudaSuccess
-               ? SA_OK : SA_E_CUDA;
+int planning_threads() {
+    if (const char *e = std::getenv("SA_PLAN_THREADS")) {
+        const int v = std::atoi(e);
+        if (v > 0) return v;
+    }
+    return (int) std::max(1u, std::thread::hardware_concurrency());
 }
 
-template <typename T>
-sa_status d2h(std::vector<T> &dst, const T *src, size_t n, cudaStream_t s) {
-    dst.resize(n);
-    if (n == 0) return SA_OK;
-    return cudaMemcpyAsync(dst.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, s) == cudaSuccess ? SA_OK
-                                                                                                     : SA_E_CUDA;
-}
+// one read's plan before packing
+struct ReadPlan {
+    sa_status status = SA_OK;
+    int32_t model = -1;
+    int64_t lX = 0;
+    std::vector<int32_t> kid;   // k-mer id per column 1..lX
+    std::vector<Region> regs;
+    int64_t diags = 0, cells = 0, windows = 0, chunks = 0, out = 0;
+    int32_t max_width = 0;
+    // packing offsets
+    int64_t region_base = 0, diag_base = 0, cell_base = 0, win_base = 0, chunk_base = 0, kmer_base = 0,
+            event_base = 0, out_base = 0;
+};
 
-void free_batch_device(sa_batch *b) {
-    for_each_buffer(b, [](auto *&p, size_t) {
-        cudaFree(p);
-        p = nullptr;
-    });
-}
-
-// Host planning of a batch (no device work): per read k-mer ids, events and regions, per region its
-// windows, per-anti-diagonal meta and emission chunks, per window its task and output segment, the
-// LPT order.  Returns SA_E_CAPACITY for a band wider than the kernel's widest ring.
-sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch *b) {
-    sa_status st = SA_OK;
+// Host planning of a batch (no device work): per read its regions and their windows (in parallel
+// over reads), then the packed inputs, written straight into a host staging block (pinned when
+// `pinned`): per region its descriptor, per-anti-diagonal meta and emission chunks, per window its
+// task and output segment, per read its k-mer ids, skip emissions and events; and the LPT order.
+// Returns SA_E_CAPACITY for a band wider than the kernel's widest ring.
+sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, bool pinned, sa_batch *b) {
     b->n_reads = n_reads;
+    b->host_pinned = pinned;
     b->threshold = (float) p->threshold;
     b->read_status.assign(n_reads, SA_OK);
     b->read_first_region.assign(n_reads, 0);
     b->read_n_regions.assign(n_reads, 0);
-    b->read_win.assign(2 * n_reads, 0);
-    b->read_scale.resize(n_reads);
-    std::vector<Region> regs;
-    PathTable pt;
+    std::vector<ReadScale32> scale(n_reads);
+    std::vector<ReadPlan> plan(n_reads);
+    // arguments, devices and models (serial: models are shared)
     int device = -1;
     for (int64_t r = 0; r < n_reads; ++r) {
         const sa_read &rd = reads[r];
+        ReadPlan &rp = plan[r];
         auto *sm = const_cast<sa_state_machine *>(rd.sm);
-        b->read_first_region[r] = (int64_t) b->regions.size();
-        b->read_win[2 * r] = (int64_t) b->windows.size();
+        std::memset(&scale[r], 0, sizeof(ReadScale32));
         if (!sm || rd.reference_length < 0 || rd.n_events < 0 || rd.n_anchors < 0 ||
             (rd.reference_length > 0 && !rd.reference) || (rd.n_events > 0 && !rd.events) ||
             (rd.n_anchors > 0 && !rd.anchors) || !(rd.var != 0.0)) {
-            b->read_status[r] = SA_E_ARG;
+            rp.status = SA_E_ARG;
             continue;
         }
         if (device < 0) device = sm->dev.device;
-        if (sm->dev.device != device) { b->read_status[r] = SA_E_ARG; continue; }
-        if (sm->emission == SA_EMIT_HDP && !sm->hdp.present) { b->read_status[r] = SA_E_UNSUPPORTED; continue; }
+        if (sm->dev.device != device) { rp.status = SA_E_ARG; continue; }
+        if (sm->emission == SA_EMIT_HDP && !sm->hdp.present) { rp.status = SA_E_UNSUPPORTED; continue; }
         const int k = sm->kmer_length;
-        const int64_t lX = rd.reference_length == 0 ? 0 : rd.reference_length - (k - 1);
-        if (lX < 0) { b->read_status[r] = SA_E_ARG; continue; }
-        st = build_paths(sm, rd.reference, lX, rd.degenerate, pt);
-        if (st) { b->read_status[r] = st; continue; }
-        if (pt.multi) { b->read_status[r] = SA_E_UNSUPPORTED; continue; }
-        st = plan_regions(rd.anchors, rd.n_anchors, lX, rd.n_events, *p, rd.ragged_left != 0, rd.ragged_right != 0,
-                          regs);
-        if (st) { b->read_status[r] = st; continue; }
-        int32_t model = -1;
+        rp.lX = rd.reference_length == 0 ? 0 : rd.reference_length - (k - 1);
+        if (rp.lX < 0) { rp.status = SA_E_ARG; continue; }
         for (size_t i = 0; i < b->models.size(); ++i)
-            if (b->models[i] == sm) model = (int32_t) i;
-        if (model < 0) { model = (int32_t) b->models.size(); b->models.push_back(sm); }
+            if (b->models[i] == sm) rp.model = (int32_t) i;
+        if (rp.model < 0) { rp.model = (int32_t) b->models.size(); b->models.push_back(sm); }
         const double var = sm->emission == SA_EMIT_PLAIN ? 1.0 : rd.var;
-        ReadScale32 &rs = b->read_scale[r];
+        ReadScale32 &rs = scale[r];
         rs.scale = sm->emission == SA_EMIT_PLAIN ? 1.0f : (float) rd.scale;
         rs.shift = sm->emission == SA_EMIT_PLAIN ? 0.0f : (float) rd.shift;
         rs.inv_var = (float) (1.0 / var);
         rs.log_inv_var = (float) std::log(1.0 / var);
-        const int64_t kmer_base = (int64_t) b->kmer.size();
-        for (int64_t x = 1; x <= lX; ++x) {
-            const int32_t kid = pt.ids[pt.first[x]];
-            b->kmer.push_back(kid);
-            b->gapx.push_back(sm->emission == SA_EMIT_HDP ? (float) kLogPointOne : (float) sm->gapx[kid]);
+    }
+    const int threads = planning_threads();
+    // k-mer ids, regions and windows of each read
+    parallel_for(n_reads, threads, [&](int64_t r) {
+        ReadPlan &rp = plan[r];
+        if (rp.status) return;
+        const sa_read &rd = reads[r];
+        PathTable pt;
+        sa_status st = build_paths(rd.sm, rd.reference, rp.lX, rd.degenerate, pt);
+        if (!st && pt.multi) st = SA_E_UNSUPPORTED;
+        if (!st)
+            st = plan_regions(rd.anchors, rd.n_anchors, rp.lX, rd.n_events, *p, rd.ragged_left != 0,
+                              rd.ragged_right != 0, rp.regs);
+        if (st) {
+            rp.status = st;
+            rp.regs.clear();
+            return;
         }
-        const int64_t event_base = (int64_t) b->events.size();
+        rp.kid.resize(rp.lX);
+        for (int64_t x = 1; x <= rp.lX; ++x) rp.kid[x - 1] = pt.ids[pt.first[x]];
+        for (const Region &rg : rp.regs) {
+            const int64_t n = rg.lX + rg.lY;
+            rp.diags += n + 1;
+            rp.cells += rg.cells;
+            rp.windows += (int64_t) rg.windows.size();
+            rp.chunks += (n + kChunkDiags) / kChunkDiags;
+            for (const Window &w : rg.windows) rp.out += 4 * (int64_t) (w.from - w.T) + 64;
+            rp.max_width = std::max(rp.max_width, rg.max_width);
+        }
+    });
+    // packing offsets
+    int64_t nreg = 0, ndiag = 0, ncell = 0, nwin = 0, nchunk = 0, nkmer = 0, nevent = 0, nout = 0;
+    for (int64_t r = 0; r < n_reads; ++r) {
+        ReadPlan &rp = plan[r];
+        b->read_status[r] = rp.status;
+        rp.region_base = nreg; rp.diag_base = ndiag; rp.cell_base = ncell; rp.win_base = nwin;
+        rp.chunk_base = nchunk; rp.kmer_base = nkmer; rp.event_base = nevent; rp.out_base = nout;
+        b->read_first_region[r] = nreg;
+        b->read_n_regions[r] = (int64_t) rp.regs.size();
+        nreg += (int64_t) rp.regs.size(); ndiag += rp.diags; ncell += rp.cells; nwin += rp.windows;
+        nchunk += rp.chunks; nout += rp.out;
+        if (!rp.status) {
+            nkmer += rp.lX;
+            nevent += reads[r].n_events;
+        }
+        b->max_width = std::max(b->max_width, rp.max_width);
+    }
+    if (b->max_width > kMaxCpt * kThreads) return SA_E_CAPACITY;
+    b->device = device < 0 ? 0 : device;
+    b->n_regions = nreg; b->n_diags = ndiag; b->n_windows = nwin; b->n_chunks = nchunk;
+    b->n_kmers = nkmer; b->n_events = nevent;
+    b->cells = ncell;
+    b->out_total = nout;
+    layout(b, nullptr, nullptr, nullptr);
+    sa_status st = mem_get(pinned ? MemKind::Pinned : MemKind::Heap, b->device, b->in_bytes, b->host_in);
+    if (st) return st;
+    layout(b, static_cast<unsigned char *>(b->host_in.ptr), nullptr, nullptr);
+    for (int64_t r = 0; r < n_reads; ++r) {
+        b->read_scale[r] = scale[r];
+        b->read_win[2 * r] = plan[r].win_base;
+        b->read_win[2 * r + 1] = plan[r].windows;
+    }
+    // the packed inputs, read by read
+    parallel_for(n_reads, threads, [&](int64_t r) {
+        const ReadPlan &rp = plan[r];
+        if (rp.status) return;
+        const sa_read &rd = reads[r];
+        const sa_state_machine *sm = rd.sm;
+        for (int64_t x = 0; x < rp.lX; ++x) {
+            const int32_t kid = rp.kid[x];
+            b->kmer[rp.kmer_base + x] = kid;
+            b->gapx[rp.kmer_base + x] = sm->emission == SA_EMIT_HDP ? (float) kLogPointOne : (float) sm->gapx[kid];
+        }
         for (int64_t y = 0; y < rd.n_events; ++y)
-            b->events.push_back(make_double2(rd.events[y * kEventParams], rd.events[y * kEventParams + 1]));
-        for (const Region &rg : regs) {
-            const int32_t region = (int32_t) b->regions.size();
+            b->events[rp.event_base + y] = make_double2(rd.events[y * kEventParams], rd.events[y * kEventParams + 1]);
+        int64_t dbase = rp.diag_base, cbase = rp.cell_base, wbase = rp.win_base, chbase = rp.chunk_base,
+                obase = rp.out_base;
+        std::vector<int32_t> flags;
+        std::vector<int64_t> off;
+        for (size_t gi = 0; gi < rp.regs.size(); ++gi) {
+            const Region &rg = rp.regs[gi];
+            const int32_t region = (int32_t) (rp.region_base + (int64_t) gi);
             RegionDesc d;
             std::memset(&d, 0, sizeof(d));
             d.n = (int32_t) (rg.lX + rg.lY);
@@ -231,70 +367,65 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
             d.lY = (int32_t) rg.lY;
             d.read = (int32_t) r;
             d.n_windows = (int32_t) rg.windows.size();
-            d.model = model;
+            d.model = rp.model;
             d.ragged_left = rg.ragged_left;
             d.ragged_right = rg.ragged_right;
-            d.diag_base = (int64_t) b->meta.size();
-            d.cell_base = b->cells;
-            d.win_base = (int64_t) b->windows.size();
-            d.kmer_base = kmer_base + rg.x1;
-            d.event_base = event_base + rg.y1;
+            d.diag_base = dbase;
+            d.cell_base = cbase;
+            d.win_base = wbase;
+            d.kmer_base = rp.kmer_base + rg.x1;
+            d.event_base = rp.event_base + rg.y1;
             d.x1 = rg.x1;
             d.y1 = rg.y1;
             // per anti-diagonal meta: band start, width, window end / refresh / stored gap states
-            std::vector<int32_t> flags(d.n + 2, 0);
+            flags.assign(d.n + 2, 0);
             for (const Window &w : rg.windows) {
                 flags[w.D] |= kFlagWindowEnd;
                 for (int32_t q = w.from; q > w.T; q -= 10) flags[q] |= kFlagRefresh;
             }
-            std::vector<int64_t> off(d.n + 1, 0);
+            off.resize(d.n + 1);
             int64_t acc = 0;
             for (int32_t dd = 0; dd <= d.n; ++dd) {
                 const int32_t w = (rg.xmy_r[dd] - rg.xmy_l[dd]) / 2 + 1;
                 int32_t f = flags[dd];
                 if ((flags[dd] | flags[dd + 1]) & kFlagRefresh) f |= kFlagStoreGaps;
-                b->meta.push_back(make_int2(rg.xmy_l[dd], w | f));
+                b->meta[dbase + dd] = make_int2(rg.xmy_l[dd], w | f);
                 off[dd] = acc;
                 acc += w;
             }
             for (int32_t d0 = 0; d0 <= d.n; d0 += kChunkDiags) {
-                Chunk ch;
+                Chunk &ch = b->chunks[chbase++];
                 ch.region = region;
                 ch.d0 = d0;
                 ch.nd = std::min(kChunkDiags, d.n + 1 - d0);
                 ch.pad = 0;
-                ch.cell = d.cell_base + off[d0];
-                b->chunks.push_back(ch);
+                ch.cell = cbase + off[d0];
             }
-            for (const Window &w : rg.windows) {
-                WindowTask t;
+            for (size_t wi = 0; wi < rg.windows.size(); ++wi) {
+                const Window &w = rg.windows[wi];
+                WindowTask &t = b->wtask[wbase + (int64_t) wi];
                 t.region = region;
                 t.first_cell = (int32_t) off[w.D];
                 t.out_cap = 4 * (w.from - w.T) + 64;
                 t.pad = 0;
-                t.out_base = b->out_total;
-                b->out_total += t.out_cap;
-                b->wtask.push_back(t);
+                t.out_base = obase;
+                obase += t.out_cap;
+                b->windows[wbase + (int64_t) wi] = w;
             }
-            b->cells += acc;
-            b->max_width = std::max(b->max_width, rg.max_width);
-            b->windows.insert(b->windows.end(), rg.windows.begin(), rg.windows.end());
-            b->regions.push_back(d);
+            b->regions[region] = d;
+            dbase += d.n + 1;
+            cbase += acc;
+            wbase += (int64_t) rg.windows.size();
         }
-        b->read_n_regions[r] = (int64_t) b->regions.size() - b->read_first_region[r];
-        b->read_win[2 * r + 1] = (int64_t) b->windows.size() - b->read_win[2 * r];
-    }
-    if (b->max_width > kMaxCpt * kThreads) return SA_E_CAPACITY;
-    b->device = device < 0 ? 0 : device;
+    });
     // largest band area first (LPT order of the forward claims)
-    b->order.resize(b->regions.size());
-    std::iota(b->order.begin(), b->order.end(), 0);
-    std::vector<int64_t> area(b->regions.size());
-    for (size_t i = 0; i < b->regions.size(); ++i) {
-        const RegionDesc &d = b->regions[i];
-        area[i] = (i + 1 < b->regions.size() ? b->regions[i + 1].cell_base : b->cells) - d.cell_base;
-    }
-    std::stable_sort(b->order.begin(), b->order.end(), [&](int32_t a, int32_t c) { return area[a] > area[c]; });
+    std::vector<int32_t> order(nreg);
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<int64_t> area(nreg);
+    for (int64_t i = 0; i < nreg; ++i)
+        area[i] = (i + 1 < nreg ? b->regions[i + 1].cell_base : b->cells) - b->regions[i].cell_base;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) { return area[a] > area[c]; });
+    std::copy(order.begin(), order.end(), b->order.data());
     return SA_OK;
 }
 
@@ -309,29 +440,23 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
     if (st) return st;
     auto *b = new (std::nothrow) sa_batch();
     if (!b) return SA_E_NOMEM;
-    st = plan_batch(reads, n_reads, p, b);
+    st = plan_batch(reads, n_reads, p, true, b);
+    if (!st) {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        if (cudaSetDevice(b->device) != cudaSuccess) st = SA_E_CUDA;
+        for (auto *sm : b->models)
+            if (!st) st = ensure_device_model(sm);
+        cudaSetDevice(prev);
+    }
+    if (!st) st = mem_get(MemKind::Device, b->device, b->dev_bytes, b->dev);
+    if (!st) st = mem_get(MemKind::Pinned, b->device, b->res_bytes, b->host_res);
     if (st) {
         delete b;
         return st;
     }
-    // device buffers
-    int prev = 0;
-    cudaGetDevice(&prev);
-    if (cudaSetDevice(b->device) != cudaSuccess) { delete b; return SA_E_CUDA; }
-    for (auto *sm : b->models) {
-        st = ensure_device_model(sm);
-        if (st) { cudaSetDevice(prev); delete b; return st; }
-    }
-    for_each_buffer(b, [&](auto *&ptr, size_t n) {
-        using T = std::remove_reference_t<decltype(*ptr)>;
-        if (!st && cudaMalloc((void **) &ptr, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) st = SA_E_NOMEM;
-    });
-    cudaSetDevice(prev);
-    if (st) {
-        free_batch_device(b);
-        delete b;
-        return st;
-    }
+    b->dev_base = static_cast<unsigned char *>(b->dev.ptr);
+    layout(b, static_cast<unsigned char *>(b->host_in.ptr), static_cast<unsigned char *>(b->host_res.ptr), b->dev_base);
     *out = b;
     return SA_OK;
 }
@@ -342,10 +467,9 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
     int prev = 0;
     cudaGetDevice(&prev);
     if (cudaSetDevice(b->device) != cudaSuccess) return SA_E_CUDA;
-    std::vector<ModelDesc> md(b->models.size());
     for (size_t i = 0; i < b->models.size(); ++i) {
         const sa_state_machine *sm = b->models[i];
-        ModelDesc &m = md[i];
+        ModelDesc &m = b->mdesc[i];
         std::memset(&m, 0, sizeof(m));
         m.kc = sm->dev.kc32;
         m.emission = sm->emission;
@@ -362,20 +486,11 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
         }
     }
     sa_status st = SA_OK;
-    if (!st) st = h2d(b->d_regions, b->regions, s);
-    if (!st) st = h2d(b->d_order, b->order, s);
-    if (!st) st = h2d(b->d_models, md, s);
-    if (!st) st = h2d(b->d_read_scale, b->read_scale, s);
-    if (!st) st = h2d(b->d_meta, b->meta, s);
-    if (!st) st = h2d(b->d_windows, b->windows, s);
-    if (!st) st = h2d(b->d_wtask, b->wtask, s);
-    if (!st) st = h2d(b->d_chunks, b->chunks, s);
-    if (!st) st = h2d(b->d_kmer, b->kmer, s);
-    if (!st) st = h2d(b->d_gapx, b->gapx, s);
-    if (!st) st = h2d(b->d_events_raw, b->events, s);
-    if (!st) st = h2d(b->d_read_win, b->read_win, s);
-    if (!st && !b->events.empty()) {
-        const int64_t n = (int64_t) b->events.size();
+    // every input in one copy: the staging block has the device layout
+    if (cudaMemcpyAsync(b->dev_base, b->host_in.ptr, b->in_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        st = SA_E_CUDA;
+    if (!st && b->n_events > 0) {
+        const int64_t n = b->n_events;
         prep_events<<<(unsigned) std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(b->d_events_raw, b->d_events, n);
         count_launch();
         if (cudaGetLastError() != cudaSuccess) st = SA_E_CUDA;
@@ -391,14 +506,12 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
     int prev = 0;
     cudaGetDevice(&prev);
     if (cudaSetDevice(b->device) != cudaSuccess) return SA_E_CUDA;
-    const size_t nr = b->regions.size(), nw = b->windows.size();
+    const size_t nr = (size_t) b->n_regions, nw = (size_t) b->n_windows;
     sa_status st = SA_OK;
-    // what the kernels expect cleared: counters, per-read status, window counts, log-likelihoods,
-    // and the ready queue (-1 = empty)
-    if (cudaMemsetAsync(b->d_ctl, 0, sizeof(Control), s) != cudaSuccess ||
-        cudaMemsetAsync(b->d_status, 0, sizeof(int32_t) * std::max<int64_t>(1, b->n_reads), s) != cudaSuccess ||
+    // what the kernels expect cleared: the results block (counters, per-read status and pair
+    // ranges, log-likelihoods), the window pair counts, and the ready queue (-1 = empty)
+    if (cudaMemsetAsync(b->dev_base + b->res_off, 0, b->res_bytes, s) != cudaSuccess ||
         cudaMemsetAsync(b->d_wcount, 0, sizeof(int64_t) * std::max<size_t>(1, nw), s) != cudaSuccess ||
-        cudaMemsetAsync(b->d_loglik, 0, sizeof(double) * std::max<size_t>(1, nr), s) != cudaSuccess ||
         cudaMemsetAsync(b->d_ready, 0xff, sizeof(int32_t) * std::max<size_t>(1, nw), s) != cudaSuccess)
         st = SA_E_CUDA;
     if (!st && nr > 0) {
@@ -414,7 +527,7 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         a.wtask = b->d_wtask;
         a.n_windows = (int64_t) nw;
         a.chunks = b->d_chunks;
-        a.n_chunks = (int64_t) b->chunks.size();
+        a.n_chunks = b->n_chunks;
         a.kmer = b->d_kmer;
         a.gapx = b->d_gapx;
         a.events = b->d_events;
@@ -468,32 +581,31 @@ sa_status sa_batch_download(sa_batch *b, void *stream) {
     int prev = 0;
     cudaGetDevice(&prev);
     if (cudaSetDevice(b->device) != cudaSuccess) return SA_E_CUDA;
-    const size_t nr = b->regions.size(), nreads = (size_t) b->n_reads;
+    const MemKind host_kind = b->host_pinned ? MemKind::Pinned : MemKind::Heap;
     sa_status st = SA_OK;
-    b->ctl = Control{};
-    if (!st) st = d2h(b->read_base, b->d_read_base, nr ? nreads : 0, s);
-    if (!st) st = d2h(b->read_count, b->d_read_count, nr ? nreads : 0, s);
-    if (!st) st = d2h(b->loglik, b->d_loglik, nr, s);
-    if (!st) st = d2h(b->dev_status, b->d_status, nreads, s);
-    if (!st && nr && cudaMemcpyAsync(&b->ctl, b->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    if (!b->host_res.ptr) {
+        st = mem_get(host_kind, b->device, b->res_bytes, b->host_res);
+        if (!st) layout(b, nullptr, static_cast<unsigned char *>(b->host_res.ptr), nullptr);
+    }
+    // the results block in one copy, then the packed pairs in one copy
+    if (!st && cudaMemcpyAsync(b->host_res.ptr, b->dev_base + b->res_off, b->res_bytes, cudaMemcpyDeviceToHost, s) !=
+                   cudaSuccess)
         st = SA_E_CUDA;
     if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = SA_E_CUDA;
-    if (!nr) {
-        b->read_base.assign(nreads, 0);
-        b->read_count.assign(nreads, 0);
+    const size_t npairs = st ? 0 : (size_t) b->ctl[0].packed;
+    const size_t pair_bytes = std::max<size_t>(npairs, 1) * sizeof(sa_aligned_pair);
+    if (!st && b->host_pairs.bytes < pair_bytes) {
+        mem_put(b->host_pairs);
+        st = mem_get(host_kind, b->device, pair_bytes, b->host_pairs);
     }
-    // the packed pairs in one copy, then split per read on the host
-    std::vector<sa_aligned_pair> packed;
-    if (!st) st = d2h(packed, b->d_packed, (size_t) b->ctl.packed, s);
+    if (!st && npairs > 0 &&
+        cudaMemcpyAsync(b->host_pairs.ptr, b->d_packed, npairs * sizeof(sa_aligned_pair), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess)
+        st = SA_E_CUDA;
     if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = SA_E_CUDA;
-    b->read_pairs.assign(nreads, {});
-    b->read_ll.assign(nreads, 0.0);
-    for (size_t r = 0; r < nreads && !st; ++r) {
-        const int64_t base = b->read_base[r], cnt = b->read_count[r];
-        if (cnt > 0 && base >= 0 && base + cnt <= (int64_t) packed.size())
-            b->read_pairs[r].assign(packed.begin() + base, packed.begin() + base + cnt);
+    b->read_ll.assign(b->n_reads, 0.0);
+    for (int64_t r = 0; r < b->n_reads && !st; ++r)
         for (int64_t i = 0; i < b->read_n_regions[r]; ++i) b->read_ll[r] += b->loglik[b->read_first_region[r] + i];
-    }
     cudaSetDevice(prev);
     b->downloaded = st == SA_OK;
     return st;
@@ -512,18 +624,18 @@ sa_status sa_batch_read_status(const sa_batch *b, int64_t read) {
     if (!b || read < 0 || read >= b->n_reads) return SA_E_ARG;
     if (b->read_status[read]) return (sa_status) b->read_status[read];
     if (!b->downloaded) return SA_E_ARG;
-    if (b->ctl.error) return SA_E_TIMEOUT;
+    if (b->ctl[0].error) return SA_E_TIMEOUT;
     return (sa_status) b->dev_status[read];
 }
 
 int64_t sa_batch_pair_count(const sa_batch *b, int64_t read) {
     if (!b || read < 0 || read >= b->n_reads || !b->downloaded) return -1;
-    return (int64_t) b->read_pairs[read].size();
+    return b->read_status[read] ? 0 : b->read_count[read];
 }
 
 const sa_aligned_pair *sa_batch_pairs(const sa_batch *b, int64_t read) {
     if (!b || read < 0 || read >= b->n_reads || !b->downloaded) return nullptr;
-    return b->read_pairs[read].data();
+    return static_cast<const sa_aligned_pair *>(b->host_pairs.ptr) + (b->read_status[read] ? 0 : b->read_base[read]);
 }
 
 double sa_batch_log_likelihood(const sa_batch *b, int64_t read) {
@@ -535,14 +647,8 @@ int64_t sa_batch_cells(const sa_batch *b) { return b ? b->cells : 0; }
 
 sa_status sa_batch_transfer_bytes(const sa_batch *b, int64_t *h2d_bytes, int64_t *d2h_bytes) {
     if (!b || !h2d_bytes || !d2h_bytes) return SA_E_ARG;
-    auto bytes = [](const auto &v) { return (int64_t) (v.size() * sizeof(v[0])); };
-    *h2d_bytes = bytes(b->regions) + bytes(b->order) + (int64_t) (b->models.size() * sizeof(ModelDesc)) +
-                 bytes(b->read_scale) + bytes(b->meta) + bytes(b->windows) + bytes(b->wtask) + bytes(b->chunks) +
-                 bytes(b->kmer) + bytes(b->gapx) + bytes(b->events) + bytes(b->read_win);
-    int64_t pairs = 0;
-    for (const auto &rp : b->read_pairs) pairs += (int64_t) rp.size();
-    *d2h_bytes = bytes(b->read_base) + bytes(b->read_count) + bytes(b->loglik) + bytes(b->dev_status) +
-                 (int64_t) sizeof(Control) + pairs * (int64_t) sizeof(sa_aligned_pair);
+    *h2d_bytes = (int64_t) b->in_bytes;
+    *d2h_bytes = (int64_t) b->res_bytes + (b->downloaded ? (int64_t) (b->ctl[0].packed * sizeof(sa_aligned_pair)) : 0);
     return SA_OK;
 }
 
@@ -581,15 +687,7 @@ sa_status sa_measure_fp32_peak(int32_t device, double *tflops) {
 
 int64_t sa_batch_regions(const sa_batch *b) { return b ? (int64_t) b->regions.size() : 0; }
 
-void sa_batch_destroy(sa_batch *b) {
-    if (!b) return;
-    int prev = 0;
-    cudaGetDevice(&prev);
-    cudaSetDevice(b->device);
-    free_batch_device(b);
-    cudaSetDevice(prev);
-    delete b;
-}
+void sa_batch_destroy(sa_batch *b) { delete b; }
 
 }  // extern "C"
 
@@ -605,7 +703,7 @@ sa_status batch_plan_host(const sa_read *reads, int64_t n_reads, const sa_params
     if (st) return st;
     auto *b = new (std::nothrow) sa_batch();
     if (!b) return SA_E_NOMEM;
-    st = plan_batch(reads, n_reads, p, b);
+    st = plan_batch(reads, n_reads, p, false, b);
     if (st) {
         delete b;
         return st;
@@ -623,14 +721,9 @@ bool batch_models_resident(const sa_batch *b) {
 }
 
 size_t batch_bind_scratch(sa_batch *b, unsigned char *base) {
-    size_t at = 0;
-    for_each_buffer(b, [&](auto *&ptr, size_t n) {
-        using T = std::remove_reference_t<decltype(*ptr)>;
-        at = (at + 255) & ~(size_t) 255;
-        if (base) ptr = reinterpret_cast<T *>(base + at);
-        at += std::max<size_t>(n, 1) * sizeof(T);
-    });
-    return (at + 255) & ~(size_t) 255;
+    b->owns_device = false;
+    b->dev_base = base;
+    return layout(b, nullptr, nullptr, base);
 }
 
 void batch_release_host(sa_batch *b) { delete b; }

@@ -127,6 +127,18 @@ void free_device_model(sa_state_machine *sm);
 
 void count_launch(int64_t n = 1);
 
+// memory blocks reused across batches (sa_memory.cpp): device and pinned host blocks go back to a
+// free list; heap blocks (for callers that must not touch the CUDA allocators) are freed
+enum class MemKind { Device, Pinned, Heap };
+struct MemBlock {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int device = -1;
+    MemKind kind = MemKind::Heap;
+};
+sa_status mem_get(MemKind kind, int device, size_t bytes, MemBlock &out);
+void mem_put(MemBlock &b);
+
 // batches bound to one caller-provided device area instead of their own allocations (sa_fp32.cu)
 sa_status batch_plan_host(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch **out);
 int batch_device(const sa_batch *b);
