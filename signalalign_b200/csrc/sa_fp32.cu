@@ -551,7 +551,7 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         const int cpt_pow2 = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
         a.wmax = cpt_pow2 * kThreads;
         a.spin_limit = 20000000000LL;   // ~10 s at 2 GHz: far beyond any forward sweep
-        const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) (9 * (a.wmax + 2) + 2 * a.wmax);
+        const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) worker_area_floats(cpt_pow2);
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
         sms = std::max(1, sms);

@@ -61,7 +61,6 @@ constexpr int32_t kFlagStoreGaps = 1 << 21;   // a refresh reads this anti-diago
 constexpr int32_t kFlagRefresh = 1 << 22;     // total-probability refresh in its posterior window
 
 enum { T_MC = 0, T_MFGX, T_MFGY, T_OX, T_OY, T_EX, T_EY, T_SX, T_SY };
-enum { TASK_DONE = 0, TASK_FORWARD = 1, TASK_WINDOW = 2 };
 
 struct ModelDesc {
     const KmerConst32 *kc;
@@ -104,12 +103,22 @@ struct Chunk {
 
 // device counters, cleared before every launch
 struct Control {
-    unsigned int claim;   // next task claim
+    unsigned int claim;   // next forward-sweep claim
+    unsigned int wclaim;  // next ready-queue slot claim
     unsigned int pub;     // next ready-queue slot to publish into
     int32_t error;        // a bounded wait gave up
-    int32_t pad;
     unsigned long long packed;   // pairs in the packed output
 };
+
+// per-warp window area (floats) when windows run one per warp: ring + refresh chain
+constexpr int kWarpWindowCpt = 4;
+constexpr int kWarpWindowWidth = 32 * kWarpWindowCpt;
+constexpr int kWarpWindowFloats = 9 * (kWarpWindowWidth + 2) + 2 * kWarpWindowWidth;
+
+// dynamic shared memory of the worker after the Shared header, in floats
+__host__ __device__ constexpr int worker_area_floats(int cpt) {
+    return cpt == 1 ? kWarps * kWarpWindowFloats : 9 * (cpt * kThreads + 2) + 2 * cpt * kThreads;
+}
 
 struct Args {
     const RegionDesc *regions;
@@ -152,7 +161,7 @@ struct Shared {
     float part[3][kWarps];          // per-warp maxima of the last anti-diagonals
     int32_t wcnt[2][kMaxCpt][kWarps];
     float fold[2];
-    int32_t task_kind, task_id;
+    int32_t task_id;
 };
 
 // The reference's lookup (pairwiseAligner.c:237-248) picks one of four cubics by d <= 1, <= 2.5,
@@ -903,59 +912,338 @@ __device__ void window_task(const Ctx &c, Shared *sh, float *ring, float *chain,
 }
 
 // ------------------------------------------------------------------------------------------------
+// backward sweep of one traceback window by one warp (bands up to 32 * WCPT cells wide)
+// ------------------------------------------------------------------------------------------------
+// The same recursion, posterior and refreshes as window_task, with the anti-diagonal's cells spread
+// over one warp (cell i on lane i mod 32): warp-synchronous exchange through the ring, maxima by one
+// warp reduction, pairs numbered by ballots, no block barrier.  Look-ahead loads go to registers
+// indexed by the parity of the step, so they land without register moves; the operands of a
+// refresh (one anti-diagonal in ten) are loaded when it happens.
+template <int WCPT>
+struct WarpWindow {
+    const Ctx &c;
+    const Args &A;
+    const RegionDesc &R;
+    const float4 *tab;
+    float *ring;                  // 3 slots x 3 states x (wmax + 2)
+    float *chain;                 // 2 x wmax: refresh terms
+    int lane, wmax, stride;
+    int64_t db;
+    int32_t n, D, T, from;
+    const float *Freg, *Ereg;
+    float *s0, *s1, *s2;          // ring slots of d, d+1, d+2
+    Meta mpp, mp, m0, mm;         // band facts of d+2, d+1, d, d-1
+    int2 raw_mmm;                 // raw band facts of d-2
+    int32_t off0, offp;           // first cells of d and d+1
+    // look-ahead operands of a step's cells, by step parity: match emission of the match
+    // successor, extra-event emission of the upper successor, skip emission of the lower
+    // successor, forward match value, path k-mer id; and the forward base and shift
+    float qM[2][WCPT], qY[2][WCPT], qX[2][WCPT], qF[2][WCPT];
+    int32_t qK[2][WCPT];
+    double qB[2];
+    float qS[2];
+    float mxD, mx_last, lm_prev, gamma1;
+    double bbase, pref, ll;
+    int64_t n_out;
+
+    __device__ __forceinline__ WarpWindow(const Ctx &cc, float *r, float *ch, const float4 *tb)
+        : c(cc), A(*cc.A), R(cc.R), tab(tb), ring(r), chain(ch) {}
+
+    // operands of the cells of anti-diagonal dd (meta m, first cell off) into parity Q; m1 / off1
+    // describe dd+1 (upper successors), m2 / off2 dd+2 (match successors)
+    template <int Q>
+    __device__ __forceinline__ void prefetch(int32_t dd, const Meta &m, int32_t off, const Meta &m1, int32_t off1,
+                                             const Meta &m2, int32_t off2) {
+        const float *E2 = Ereg + 2 * off2, *E1 = Ereg + 2 * off1, *Fm = Freg + 3 * off;
+#pragma unroll
+        for (int j = 0; j < WCPT; ++j) {
+            const int i = lane + 32 * j;
+            const int32_t xmy = m.L + 2 * i, x = (dd + xmy) >> 1;
+            qM[Q][j] = __ldg(E2 + SE_M * m2.W + clampi((xmy - m2.L) >> 1, 0, max(m2.W - 1, 0)));
+            qY[Q][j] = __ldg(E1 + SE_Y * m1.W + clampi((xmy - 1 - m1.L) >> 1, 0, max(m1.W - 1, 0)));
+            qX[Q][j] = raw_gapx(c, x + 1);
+            qF[Q][j] = __ldcg(Fm + ST_M * m.W + clampi(i, 0, max(m.W - 1, 0)));
+            qK[Q][j] = __ldg(A.kmer + R.kmer_base + clampi(x - 1, 0, max(R.lX - 1, 0)));
+        }
+        qB[Q] = __ldcg(A.base + db + max(dd, 0));
+        qS[Q] = __ldcg(A.fshift + db + max(dd, 0));
+    }
+
+    // anti-diagonal d; K = (D - d) & 1 is the parity of its operands
+    template <int K>
+    __device__ __forceinline__ void step(int32_t d, const WindowTask &wt) {
+        const float *t = c.t;
+        const int32_t W0 = m0.W, Wp = mp.W;
+        // maximum of B on d+1 for the shift of d-1 (d+1 = D holds the end states: known exactly)
+        const float mx_new = warp_max1(lm_prev);
+        float gamma0 = 0.0f;           // base(d) - base(d+1) = max(d+2) - gamma1
+        if (d <= D - 2) {
+            float m = d == D - 2 ? mxD : mx_last;
+            if (!(m > kNegInf)) m = 0.0f;
+            gamma0 = m - gamma1;
+        }
+        bbase += (double) gamma0;
+        // operands of the d-1 cells
+        const Meta mmm = decode_meta(raw_mmm, d - 2 >= 0);
+        raw_mmm = raw_meta(A, db, d - 3, n);
+        const int32_t offm = off0 - mm.W;
+        prefetch<1 - K>(d - 1, mm, offm, m0, off0, mp, offp);
+        // the recursion on d (D itself holds the end-state values)
+        float lm = kNegInf;
+        if (d < D) {
+            const float shU = -gamma0, shM = -gamma1 - gamma0;
+#pragma unroll
+            for (int j = 0; j < WCPT; ++j) {
+                const int i = lane + 32 * j;
+                const int32_t xmy = m0.L + 2 * i;
+                const int ipp = clampi((xmy - mpp.L) >> 1, -1, wmax);
+                const int iu = clampi((xmy - 1 - mp.L) >> 1, -1, wmax);
+                const int il = clampi((xmy + 1 - mp.L) >> 1, -1, wmax);
+                // each successor's backward value plus its emission, shared by the transitions into it
+                const float bme = s2[ipp] + (qM[K][j] + shM);
+                float vM = bme + t[T_MC];
+                float vX = bme + t[T_MFGX];
+                float vY = bme + t[T_MFGY];
+                const float bue = s1[2 * stride + iu] + (qY[K][j] + shU);
+                vM = lae(tab, vM, bue + t[T_OY]);
+                vY = lae(tab, vY, bue + t[T_EY]);
+                const float ble = s1[stride + il] + (qX[K][j] + shU);
+                vM = lae(tab, vM, ble + t[T_OX]);
+                vX = lae(tab, vX, ble + t[T_EX]);
+                vY = lae(tab, vY, ble + t[T_SX]);
+                if (i >= W0) vM = vX = vY = kNegInf;
+                s0[i] = vM;
+                s0[stride + i] = vX;
+                s0[2 * stride + i] = vY;
+                lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
+            }
+        }
+        __syncwarp();
+        const double fb = qB[K];
+        const float fsh = qS[K];
+        if (d <= from) {
+            if ((m0.flags & kFlagRefresh) != 0) {
+                // diagonalCalculationTotalProbability (pairwiseAligner.c:1182-1200): F.B on d in
+                // ascending cell order, then the matches from d-1 over d into d+1, dotted with B(d+1)
+                const float *Fd = Freg + 3 * off0;
+#pragma unroll
+                for (int j = 0; j < WCPT; ++j) {
+                    const int i = lane + 32 * j;
+                    if (i < W0) {
+                        float s = qF[K][j] + s0[i];
+                        s = lae(tab, s, __ldcg(Fd + ST_X * W0 + i) + s0[stride + i]);
+                        s = lae(tab, s, __ldcg(Fd + ST_Y * W0 + i) + s0[2 * stride + i]);
+                        chain[i] = s;
+                    }
+                }
+                const bool have_next = d < D;
+                if (have_next) {
+                    const float *Fm = Freg + 3 * (off0 - mm.W), *Ep = Ereg + 2 * offp;
+                    const int32_t Wm = mm.W;
+#pragma unroll
+                    for (int j = 0; j < WCPT; ++j) {
+                        const int i = lane + 32 * j;
+                        if (i < Wp) {
+                            const int32_t xmy1 = mp.L + 2 * i;
+                            const int32_t r = (xmy1 - mm.L) >> 1;
+                            float mth = kNegInf;
+                            if (Wm > 0 && xmy1 >= mm.L && r < Wm) {
+                                const float e = __ldg(Ep + SE_M * Wp + i);
+                                mth = __ldcg(Fm + ST_M * Wm + r) + (e + t[T_MC]);
+                                mth = lae(tab, mth, __ldcg(Fm + ST_X * Wm + r) + (e + t[T_MFGX]));
+                                mth = lae(tab, mth, __ldcg(Fm + ST_Y * Wm + r) + (e + t[T_MFGY]));
+                            }
+                            chain[wmax + i] = mth + s1[i];
+                        }
+                    }
+                }
+                __syncwarp();
+                const float f0 = ordered_fold(tab, chain, W0);
+                const float f1 = have_next ? ordered_fold(tab, chain + wmax, Wp) : kNegInf;
+                // the through-part is relative to base_F(d-1) + base_B(d+1)
+                const float ptil = lae(tab, f0, f1 - fsh - gamma0);
+                pref = (double) ptil + fb + bbase;
+                if (d == n) ll = pref;
+                __syncwarp();
+            }
+            // posteriors of d, emitted in ascending cell order (the reference's order)
+            const float kd = (float) (fb + bbase - pref);
+            int64_t before = n_out;
+#pragma unroll
+            for (int j = 0; j < WCPT; ++j) {
+                const int i = lane + 32 * j;
+                const int32_t xmy = m0.L + 2 * i, x = (d + xmy) >> 1, y = (d - xmy) >> 1;
+                const float p = __expf(qF[K][j] + s0[i] + kd);
+                const bool hit = i < W0 && x > 0 && y > 0 && p >= A.threshold;
+                const unsigned bal = __ballot_sync(0xffffffffu, hit);
+                if (hit) {
+                    const int64_t q = before + __popc(bal & ((1u << lane) - 1u));
+                    if (q < wt.out_cap) {
+                        sa_aligned_pair o;
+                        o.score = (int64_t) floor((double) fminf(p, 1.0f) * 10000000.0);
+                        o.x = R.x1 + x - 1;
+                        o.y = R.y1 + y - 1;
+                        o.kmer = qK[K][j];
+                        A.out[wt.out_base + q] = o;
+                    } else {
+                        atomicMax(A.status + R.read, (int32_t) SA_E_OUTPUT);
+                    }
+                }
+                before += __popc(bal);
+            }
+            n_out = before;
+        }
+        mx_last = mx_new;
+        lm_prev = d == D ? kNegInf : lm;   // D's maximum is known exactly (mxD)
+        gamma1 = gamma0;
+        offp = off0;
+        off0 = offm;
+        float *fr = s2;
+        s2 = s1;
+        s1 = s0;
+        s0 = fr;
+        mpp = mp; mp = m0; m0 = mm; mm = mmm;
+    }
+
+    __device__ void run(int64_t gw) {
+        lane = threadIdx.x & 31;
+        wmax = 32 * WCPT;
+        stride = wmax + 2;
+        db = R.diag_base;
+        n = R.n;
+        Freg = A.F + 3 * R.cell_base;
+        Ereg = A.E + 2 * R.cell_base;
+        const Window Wn = A.windows[gw];
+        const WindowTask wt = A.wtask[gw];
+        D = Wn.D;
+        T = Wn.T;
+        from = Wn.from;
+        for (int i = lane; i < 9 * stride; i += 32) ring[i] = kNegInf;
+        s0 = ring + 1;
+        s1 = ring + 3 * stride + 1;
+        s2 = ring + 6 * stride + 1;
+        // end-state values on D (stateMachine.c:1034-1061)
+        const float *t = c.t;
+        const bool ragged_end = Wn.at_end && R.ragged_right;
+        const float e0 = ragged_end ? (t[T_OX] + t[T_OY]) / 2.0f : t[T_MC];
+        const float e1 = ragged_end ? t[T_EX] : t[T_MFGX];
+        const float e2 = ragged_end ? t[T_EY] : t[T_MFGY];
+        mxD = fmaxf(e0, fmaxf(e1, e2));
+        if (!(mxD > kNegInf)) mxD = 0.0f;
+        mpp = mp = Meta{0, 0, 0};
+        m0 = decode_meta(raw_meta(A, db, D, n), true);
+        mm = decode_meta(raw_meta(A, db, D - 1, n), D - 1 >= 0);
+        raw_mmm = raw_meta(A, db, D - 2, n);
+        off0 = offp = wt.first_cell;
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < WCPT; ++j) {
+            const int i = lane + 32 * j;
+            if (i < m0.W) {
+                s0[i] = e0;
+                s0[stride + i] = e1;
+                s0[2 * stride + i] = e2;
+            }
+        }
+        prefetch<0>(D, m0, off0, mp, offp, mpp, offp);
+        mx_last = kNegInf;
+        lm_prev = kNegInf;
+        gamma1 = 0.0f;
+        bbase = pref = ll = 0.0;
+        n_out = 0;
+        __syncwarp();
+        for (int32_t d = D; d > T; d -= 2) {
+            step<0>(d, wt);
+            if (d - 1 <= T) break;
+            step<1>(d - 1, wt);
+        }
+        if (lane == 0) {
+            A.wcount[gw] = n_out;
+            if (Wn.at_end) A.loglik[c.region_index] = ll;
+        }
+        __syncwarp();
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
 // the persistent worker
 // ------------------------------------------------------------------------------------------------
+// Bounded wait (one thread) until a forward sweep publishes into ready-queue slot `slot`; -1 if
+// the wait gave up (SA_E_TIMEOUT for the batch) or another worker already did.
+__device__ __forceinline__ int32_t wait_ready(const Args &A, int64_t slot) {
+    const long long t0 = clock64();
+    for (;;) {
+        const int32_t v = *((volatile int32_t *) (A.ready + slot));
+        if (v >= 0) {
+            __threadfence();
+            return v;
+        }
+        if (*((volatile int32_t *) &A.ctl->error)) return -1;
+        if (clock64() - t0 > A.spin_limit) {
+            atomicExch(&A.ctl->error, 1);
+            return -1;
+        }
+        __nanosleep(512);
+    }
+}
+
+// CPT: cells per thread of the forward sweep (128 threads per region).  The first claims are
+// forward sweeps, one per CTA; once none is left, windows are claimed: one per warp for bands up to
+// kWarpWindowWidth cells wide, one per CTA for wider bands.
 template <int CPT>
-__global__ void __launch_bounds__(kThreads, CPT == 1 ? 4 : 1) worker_kernel(const __grid_constant__ Args A) {
+__global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(const __grid_constant__ Args A) {
     extern __shared__ float4 smem_raw[];
     Shared *sh = reinterpret_cast<Shared *>(smem_raw);
-    float *ring = reinterpret_cast<float *>(sh + 1);
-    float *chain = ring + 9 * (A.wmax + 2);
+    float *area = reinterpret_cast<float *>(sh + 1);
     const int tid = threadIdx.x;
     if (tid < 16) log_add_piece(tid, sh->la[tid]);
+    // forward sweeps
     for (;;) {
         if (tid == 0) {
             const unsigned claim = atomicAdd(&A.ctl->claim, 1u);
-            int32_t kind = TASK_DONE, id = -1;
-            if (claim < (unsigned) A.n_regions) {
-                kind = TASK_FORWARD;
-                id = A.order[claim];
-            } else if ((int64_t) claim - A.n_regions < A.n_windows) {
-                // ready-queue slot: wait (bounded) until a forward sweep publishes into it
-                const int64_t slot = (int64_t) claim - A.n_regions;
-                const long long t0 = clock64();
-                int32_t v = -1;
-                for (;;) {
-                    v = *((volatile int32_t *) (A.ready + slot));
-                    if (v >= 0) break;
-                    if (*((volatile int32_t *) &A.ctl->error)) break;
-                    if (clock64() - t0 > A.spin_limit) {
-                        atomicExch(&A.ctl->error, 1);
-                        break;
-                    }
-                    __nanosleep(512);
-                }
-                if (v >= 0) {
-                    __threadfence();
-                    kind = TASK_WINDOW;
-                    id = v;
-                }
-            }
-            sh->task_kind = kind;
-            sh->task_id = id;
+            sh->task_id = claim < (unsigned) A.n_regions ? A.order[claim] : -1;
         }
         __syncthreads();
-        const int32_t kind = sh->task_kind, id = sh->task_id;
-        if (kind == TASK_DONE) break;
+        const int32_t id = sh->task_id;
+        if (id < 0) break;
         Ctx c;
-        if (kind == TASK_FORWARD) {
-            ctx_init(c, A, id);
-            forward_task<CPT>(c, sh, ring);
-        } else {
+        ctx_init(c, A, id);
+        forward_task<CPT>(c, sh, area);
+        __syncthreads();
+    }
+    // traceback windows, in publication order
+    if (CPT == 1) {
+        const int lane = tid & 31, warp = tid >> 5;
+        float *wring = area + warp * kWarpWindowFloats;
+        float *wchain = wring + 9 * (kWarpWindowWidth + 2);
+        for (;;) {
+            int32_t id = -1;
+            if (lane == 0) {
+                const unsigned claim = atomicAdd(&A.ctl->wclaim, 1u);
+                if ((int64_t) claim < A.n_windows) id = wait_ready(A, claim);
+            }
+            id = __shfl_sync(0xffffffffu, id, 0);
+            if (id < 0) break;
+            Ctx c;
+            ctx_init(c, A, A.wtask[id].region);
+            WarpWindow<kWarpWindowCpt> w(c, wring, wchain, sh->la);
+            w.run(id);
+        }
+    } else {
+        float *ring = area, *chain = area + 9 * (A.wmax + 2);
+        for (;;) {
+            if (tid == 0) {
+                const unsigned claim = atomicAdd(&A.ctl->wclaim, 1u);
+                sh->task_id = (int64_t) claim < A.n_windows ? wait_ready(A, claim) : -1;
+            }
+            __syncthreads();
+            const int32_t id = sh->task_id;
+            if (id < 0) break;
+            Ctx c;
             ctx_init(c, A, A.wtask[id].region);
             window_task<CPT>(c, sh, ring, chain, id);
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
