@@ -110,10 +110,11 @@ struct Control {
     unsigned long long packed;   // pairs in the packed output
 };
 
-// per-warp window area (floats) when windows run one per warp: ring + refresh chain
+// per-warp window area (floats) when windows run one per warp: ring, refresh chain (2 rows) and
+// the staged operands of the next refresh (6 rows)
 constexpr int kWarpWindowCpt = 4;
 constexpr int kWarpWindowWidth = 32 * kWarpWindowCpt;
-constexpr int kWarpWindowFloats = 9 * (kWarpWindowWidth + 2) + 2 * kWarpWindowWidth;
+constexpr int kWarpWindowFloats = 9 * (kWarpWindowWidth + 2) + 8 * kWarpWindowWidth;
 
 // dynamic shared memory of the worker after the Shared header, in floats
 __host__ __device__ constexpr int worker_area_floats(int cpt) {
@@ -260,6 +261,90 @@ __device__ float ordered_fold(const float4 *tab, const float *vals, int n) {
         carry = __shfl_sync(0xffffffffu, incl, 31);
     }
     return r;
+}
+
+// Two independent ordered folds (ordered_fold on a[0..na) and on b[0..nb)) run by one warp with
+// their sequential logAdd chains interleaved.
+__device__ __forceinline__ float2 ordered_fold2(const float4 *tab, const float *a, int na, const float *b, int nb) {
+    const int lane = threadIdx.x & 31;
+    float ma = kNegInf, mb = kNegInf;
+    for (int q = 0; q < max(na, nb); q += 32) {
+        ma = fmaxf(ma, q + lane < na ? a[q + lane] : kNegInf);
+        mb = fmaxf(mb, q + lane < nb ? b[q + lane] : kNegInf);
+    }
+    ma = warp_max(ma);
+    mb = warp_max(mb);
+    // first index within kSeedGap of each maximum
+    int sa = na, sb = nb;
+    for (int q = 0; q < na; q += 32) {
+        const unsigned m = __ballot_sync(0xffffffffu, q + lane < na && a[q + lane] >= ma - kSeedGap);
+        if (m) { sa = q + __ffs(m) - 1; break; }
+    }
+    for (int q = 0; q < nb; q += 32) {
+        const unsigned m = __ballot_sync(0xffffffffu, q + lane < nb && b[q + lane] >= mb - kSeedGap);
+        if (m) { sb = q + __ffs(m) - 1; break; }
+    }
+    float seed_a = 0.0f, seed_b = 0.0f, carry_a = kNegInf, carry_b = kNegInf;
+    for (int q = 0; q < max(sa, sb); q += 32) {
+        const float va = q + lane < sa ? a[q + lane] : kNegInf;
+        const float vb = q + lane < sb ? b[q + lane] : kNegInf;
+        seed_a += va > kNegInf ? __expf(va - ma) : 0.0f;
+        seed_b += vb > kNegInf ? __expf(vb - mb) : 0.0f;
+        carry_a = fmaxf(carry_a, va);
+        carry_b = fmaxf(carry_b, vb);
+    }
+    seed_a = warp_sum(seed_a);
+    seed_b = warp_sum(seed_b);
+    carry_a = warp_max(carry_a);
+    carry_b = warp_max(carry_b);
+    float ra = ma > kNegInf && seed_a > 0.0f ? ma + __logf(seed_a) : kNegInf;
+    float rb = mb > kNegInf && seed_b > 0.0f ? mb + __logf(seed_b) : kNegInf;
+    const int ea = ma > kNegInf ? na : 0, eb = mb > kNegInf ? nb : 0;
+    // chunk by chunk: candidates compacted, then both sequential chains side by side
+    for (int ca = sa, cb = sb; ca < ea || cb < eb; ca += 32, cb += 32) {
+        float pa = kNegInf, pb = kNegInf;
+        int nca = 0, ncb = 0;
+        if (ca < ea) {
+            const float v = ca + lane < ea ? a[ca + lane] : kNegInf;
+            float incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl = fmaxf(incl, t);
+            }
+            incl = fmaxf(incl, carry_a);
+            float excl = __shfl_up_sync(0xffffffffu, incl, 1);
+            if (lane == 0) excl = carry_a;
+            const unsigned mask = __ballot_sync(0xffffffffu, v > excl - 7.6f);
+            nca = __popc(mask);
+            const unsigned src = lane < nca ? __fns(mask, 0, lane + 1) : 0u;
+            pa = __shfl_sync(0xffffffffu, v, (int) (src & 31u));
+            carry_a = __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (cb < eb) {
+            const float v = cb + lane < eb ? b[cb + lane] : kNegInf;
+            float incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl = fmaxf(incl, t);
+            }
+            incl = fmaxf(incl, carry_b);
+            float excl = __shfl_up_sync(0xffffffffu, incl, 1);
+            if (lane == 0) excl = carry_b;
+            const unsigned mask = __ballot_sync(0xffffffffu, v > excl - 7.6f);
+            ncb = __popc(mask);
+            const unsigned src = lane < ncb ? __fns(mask, 0, lane + 1) : 0u;
+            pb = __shfl_sync(0xffffffffu, v, (int) (src & 31u));
+            carry_b = __shfl_sync(0xffffffffu, incl, 31);
+        }
+        for (int k = 0; k < max(nca, ncb); ++k) {
+            const float xa = __shfl_sync(0xffffffffu, pa, k), xb = __shfl_sync(0xffffffffu, pb, k);
+            if (k < nca) ra = lae(tab, ra, xa);
+            if (k < ncb) rb = lae(tab, rb, xb);
+        }
+    }
+    return make_float2(ra, rb);
 }
 
 __global__ void prep_events(const double2 *raw, Event32 *out, int64_t n) {
@@ -926,7 +1011,7 @@ struct WarpWindow {
     const RegionDesc &R;
     const float4 *tab;
     float *ring;                  // 3 slots x 3 states x (wmax + 2)
-    float *chain;                 // 2 x wmax: refresh terms
+    float *chain;                 // 2 x wmax: refresh terms, then 6 x wmax: staged refresh operands
     int lane, wmax, stride;
     int64_t db;
     int32_t n, D, T, from;
@@ -943,6 +1028,7 @@ struct WarpWindow {
     double qB[2];
     float qS[2];
     float mxD, mx_last, lm_prev, gamma1;
+    float e0, e1, e2;             // end states on D
     double bbase, pref, ll;
     int64_t n_out;
 
@@ -969,6 +1055,46 @@ struct WarpWindow {
         qS[Q] = __ldcg(A.fshift + db + max(dd, 0));
     }
 
+    // Operands of a refresh at anti-diagonal dd (meta m, first cell off): its gap states, and for
+    // the cells of dd+1 (m1, off1) the forward values of dd-1 (m_1, off_1) on their match
+    // predecessors and their match emissions.  load_refresh issues the loads one anti-diagonal
+    // early (forward values through L2: other CTAs wrote them during this launch);
+    // store_refresh puts them in this warp's staging rows at the end of that step.
+    struct RefreshOps {
+        float x[WCPT], y[WCPT], m[WCPT], tx[WCPT], ty[WCPT], e[WCPT];
+    };
+
+    __device__ __forceinline__ void load_refresh(RefreshOps &o, const Meta &m, int32_t off, const Meta &m1, int32_t off1,
+                                                 const Meta &m_1, int32_t off_1) const {
+        const float *Fd = Freg + 3 * off, *Fm = Freg + 3 * off_1, *E1 = Ereg + 2 * off1;
+#pragma unroll
+        for (int j = 0; j < WCPT; ++j) {
+            const int i = lane + 32 * j;
+            const int ic = clampi(i, 0, max(m.W - 1, 0));
+            o.x[j] = __ldcg(Fd + ST_X * m.W + ic);
+            o.y[j] = __ldcg(Fd + ST_Y * m.W + ic);
+            const int32_t r = clampi((m1.L + 2 * i - m_1.L) >> 1, 0, max(m_1.W - 1, 0));
+            o.m[j] = __ldcg(Fm + ST_M * m_1.W + r);
+            o.tx[j] = __ldcg(Fm + ST_X * m_1.W + r);
+            o.ty[j] = __ldcg(Fm + ST_Y * m_1.W + r);
+            o.e[j] = __ldg(E1 + SE_M * m1.W + clampi(i, 0, max(m1.W - 1, 0)));
+        }
+    }
+
+    __device__ __forceinline__ void store_refresh(const RefreshOps &o) const {
+        float *stg = chain + 2 * wmax;
+#pragma unroll
+        for (int j = 0; j < WCPT; ++j) {
+            const int i = lane + 32 * j;
+            stg[i] = o.x[j];
+            stg[wmax + i] = o.y[j];
+            stg[2 * wmax + i] = o.m[j];
+            stg[3 * wmax + i] = o.tx[j];
+            stg[4 * wmax + i] = o.ty[j];
+            stg[5 * wmax + i] = o.e[j];
+        }
+    }
+
     // anti-diagonal d; K = (D - d) & 1 is the parity of its operands
     template <int K>
     __device__ __forceinline__ void step(int32_t d, const WindowTask &wt) {
@@ -988,9 +1114,21 @@ struct WarpWindow {
         raw_mmm = raw_meta(A, db, d - 3, n);
         const int32_t offm = off0 - mm.W;
         prefetch<1 - K>(d - 1, mm, offm, m0, off0, mp, offp);
-        // the recursion on d (D itself holds the end-state values)
+        const bool refresh_next = d - 1 > T && d - 1 <= from && (mm.flags & kFlagRefresh) != 0;
+        RefreshOps rops;
+        if (refresh_next) load_refresh(rops, mm, offm, m0, off0, mmm, offm - mmm.W);
+        // the recursion on d (D itself holds the end-state values); B of the cells kept in registers
         float lm = kNegInf;
-        if (d < D) {
+        float bM[WCPT], bX[WCPT], bY[WCPT];
+        if (d == D) {
+#pragma unroll
+            for (int j = 0; j < WCPT; ++j) {
+                const bool in = lane + 32 * j < W0;
+                bM[j] = in ? e0 : kNegInf;
+                bX[j] = in ? e1 : kNegInf;
+                bY[j] = in ? e2 : kNegInf;
+            }
+        } else {
             const float shU = -gamma0, shM = -gamma1 - gamma0;
 #pragma unroll
             for (int j = 0; j < WCPT; ++j) {
@@ -1015,6 +1153,9 @@ struct WarpWindow {
                 s0[i] = vM;
                 s0[stride + i] = vX;
                 s0[2 * stride + i] = vY;
+                bM[j] = vM;
+                bX[j] = vX;
+                bY[j] = vY;
                 lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
             }
         }
@@ -1025,20 +1166,19 @@ struct WarpWindow {
             if ((m0.flags & kFlagRefresh) != 0) {
                 // diagonalCalculationTotalProbability (pairwiseAligner.c:1182-1200): F.B on d in
                 // ascending cell order, then the matches from d-1 over d into d+1, dotted with B(d+1)
-                const float *Fd = Freg + 3 * off0;
+                const float *stg = chain + 2 * wmax;
 #pragma unroll
                 for (int j = 0; j < WCPT; ++j) {
                     const int i = lane + 32 * j;
                     if (i < W0) {
-                        float s = qF[K][j] + s0[i];
-                        s = lae(tab, s, __ldcg(Fd + ST_X * W0 + i) + s0[stride + i]);
-                        s = lae(tab, s, __ldcg(Fd + ST_Y * W0 + i) + s0[2 * stride + i]);
+                        float s = qF[K][j] + bM[j];
+                        s = lae(tab, s, stg[i] + bX[j]);
+                        s = lae(tab, s, stg[wmax + i] + bY[j]);
                         chain[i] = s;
                     }
                 }
                 const bool have_next = d < D;
                 if (have_next) {
-                    const float *Fm = Freg + 3 * (off0 - mm.W), *Ep = Ereg + 2 * offp;
                     const int32_t Wm = mm.W;
 #pragma unroll
                     for (int j = 0; j < WCPT; ++j) {
@@ -1048,18 +1188,18 @@ struct WarpWindow {
                             const int32_t r = (xmy1 - mm.L) >> 1;
                             float mth = kNegInf;
                             if (Wm > 0 && xmy1 >= mm.L && r < Wm) {
-                                const float e = __ldg(Ep + SE_M * Wp + i);
-                                mth = __ldcg(Fm + ST_M * Wm + r) + (e + t[T_MC]);
-                                mth = lae(tab, mth, __ldcg(Fm + ST_X * Wm + r) + (e + t[T_MFGX]));
-                                mth = lae(tab, mth, __ldcg(Fm + ST_Y * Wm + r) + (e + t[T_MFGY]));
+                                const float e = stg[5 * wmax + i];
+                                mth = stg[2 * wmax + i] + (e + t[T_MC]);
+                                mth = lae(tab, mth, stg[3 * wmax + i] + (e + t[T_MFGX]));
+                                mth = lae(tab, mth, stg[4 * wmax + i] + (e + t[T_MFGY]));
                             }
                             chain[wmax + i] = mth + s1[i];
                         }
                     }
                 }
                 __syncwarp();
-                const float f0 = ordered_fold(tab, chain, W0);
-                const float f1 = have_next ? ordered_fold(tab, chain + wmax, Wp) : kNegInf;
+                const float2 ff = ordered_fold2(tab, chain, W0, chain + wmax, have_next ? Wp : 0);
+                const float f0 = ff.x, f1 = ff.y;
                 // the through-part is relative to base_F(d-1) + base_B(d+1)
                 const float ptil = lae(tab, f0, f1 - fsh - gamma0);
                 pref = (double) ptil + fb + bbase;
@@ -1073,7 +1213,7 @@ struct WarpWindow {
             for (int j = 0; j < WCPT; ++j) {
                 const int i = lane + 32 * j;
                 const int32_t xmy = m0.L + 2 * i, x = (d + xmy) >> 1, y = (d - xmy) >> 1;
-                const float p = __expf(qF[K][j] + s0[i] + kd);
+                const float p = __expf(qF[K][j] + bM[j] + kd);
                 const bool hit = i < W0 && x > 0 && y > 0 && p >= A.threshold;
                 const unsigned bal = __ballot_sync(0xffffffffu, hit);
                 if (hit) {
@@ -1092,6 +1232,10 @@ struct WarpWindow {
                 before += __popc(bal);
             }
             n_out = before;
+        }
+        if (refresh_next) {
+            __syncwarp();   // this step's refresh (if any) has read the staging rows
+            store_refresh(rops);
         }
         mx_last = mx_new;
         lm_prev = d == D ? kNegInf : lm;   // D's maximum is known exactly (mxD)
@@ -1125,9 +1269,9 @@ struct WarpWindow {
         // end-state values on D (stateMachine.c:1034-1061)
         const float *t = c.t;
         const bool ragged_end = Wn.at_end && R.ragged_right;
-        const float e0 = ragged_end ? (t[T_OX] + t[T_OY]) / 2.0f : t[T_MC];
-        const float e1 = ragged_end ? t[T_EX] : t[T_MFGX];
-        const float e2 = ragged_end ? t[T_EY] : t[T_MFGY];
+        e0 = ragged_end ? (t[T_OX] + t[T_OY]) / 2.0f : t[T_MC];
+        e1 = ragged_end ? t[T_EX] : t[T_MFGX];
+        e2 = ragged_end ? t[T_EY] : t[T_MFGY];
         mxD = fmaxf(e0, fmaxf(e1, e2));
         if (!(mxD > kNegInf)) mxD = 0.0f;
         mpp = mp = Meta{0, 0, 0};
@@ -1146,6 +1290,11 @@ struct WarpWindow {
             }
         }
         prefetch<0>(D, m0, off0, mp, offp, mpp, offp);
+        if (D <= from && (m0.flags & kFlagRefresh) != 0) {
+            RefreshOps o;
+            load_refresh(o, m0, off0, mp, offp, mm, off0 - mm.W);
+            store_refresh(o);
+        }
         mx_last = kNegInf;
         lm_prev = kNegInf;
         gamma1 = 0.0f;
