@@ -29,7 +29,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "dp_cells_per_sec"
 UNIT = "cells/s"
-FLOP_PER_CELL = 74.0   # forward + backward + posterior, FP32 form (per band cell)
+FLOP_PER_CELL = 74.0   # forward + backward + posterior incl. emissions, FP32 form (per band cell)
+# the worker kernel's share: transitions of both sweeps (2 x 16) and the posterior (2); the two
+# emissions per cell (~2 x 10 FLOP per pass in the reference) are computed once by emission_kernel
+WORKER_FLOP_PER_CELL = 34.0
+EMISSION_BYTES_PER_CELL = 8.0   # emission_kernel writes match + extra-event emission per cell
 WORKLOAD = "256 reads x U(2kb,20kb) spans, 6-mer ACGT Gaussian table, expansion 50, threshold 0.01"
 
 
@@ -206,6 +210,7 @@ def main():
     sampler.start()
     launches0 = api.kernel_launch_count()
     step_ms = []
+    kern_ms = []
     barrier()
     for _ in range(args.steps):
         flush.fill_(1)                       # L2 flush between timed steps (outside the events)
@@ -215,6 +220,7 @@ def main():
         e1.record(stream)
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
+        kern_ms.append(b.kernel_ms())        # per-kernel CUDA events on the launching stream
     barrier()
     launches = api.kernel_launch_count() - launches0
     clocks = sampler.stop()
@@ -247,14 +253,24 @@ def main():
     line = None
     if rank == 0:
         peak = api.measure_fp32_peak(local)
-        kernel_ms = t_max / args.steps
-        achieved = FLOP_PER_CELL * cells / (kernel_ms / 1e3) / 1e12
+        em_ms = statistics.mean(k[0] for k in kern_ms)
+        wk_ms = statistics.mean(k[1] for k in kern_ms)
+        ga_ms = statistics.mean(k[2] for k in kern_ms)
+        achieved = WORKER_FLOP_PER_CELL * cells / (wk_ms / 1e3) / 1e12
         traffic = None
-        prof = os.path.join(ROOT, "profiles", "batch_kernel_traffic.json")
+        prof = os.path.join(ROOT, "profiles", "worker_kernel_traffic.json")
         if os.path.exists(prof):
             with open(prof) as fh:
                 pj = json.load(fh)
-            traffic = pj.get("bytes_per_cell", 0) * cells
+            traffic = pj.get("dram_bytes_per_cell", 0) * cells
+        hbm_peak, hbm_src = 6650.0, "fallback"
+        mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.exists(mp):
+            with open(mp) as fh:
+                hbm_peak, hbm_src = float(json.load(fh).get("hbm_gbs", hbm_peak)), "measured"
+        em_gbs = EMISSION_BYTES_PER_CELL * cells / (em_ms / 1e3) / 1e9
+        # the sequential chain: the longest region's anti-diagonals bound the worker from below
+        longest = max(len(rd["reference"]) - 5 + len(rd["events"]) for rd in cfg["reads"])
         # plain FP64 form, one read per launch, on a sample of the batch
         order = np.argsort([len(rd["events"]) for rd in cfg["reads"]])
         sample = [int(i) for i in order[::max(1, len(order) // 8)][:8]]
@@ -287,10 +303,20 @@ def main():
                         "includes": "host planning (bands, windows, k-mer ids), H2D, launch, D2H of all pairs"},
                 "plain_fp64": {"value": plain_value, "unit": UNIT, "sample": "%d reads, one launch per read" % len(sample),
                                "batched_over_plain": value / world / plain_value},
-                "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                             "frac": achieved / peak, "traffic": traffic,
-                             "note": "%.0f FP32 FLOP per band cell (fwd+bwd+posterior); peak = FMA probe "
-                                     "measured in this run" % FLOP_PER_CELL},
+                "roofline": {"kernel": "worker_kernel", "bound": "fp32", "achieved": achieved, "peak": peak,
+                             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                             "kernel_ms": wk_ms,
+                             "note": "%.0f FP32 FLOP per band cell (transitions of both sweeps + posterior; "
+                                     "emissions are emission_kernel's) / worker CUDA-event time; peak = FP32 FMA "
+                                     "probe measured in this run; traffic = dram bytes per cell from the ncu capture "
+                                     "in profiles/ x cells" % WORKER_FLOP_PER_CELL},
+                "kernels_ms": {"emission_kernel": em_ms, "worker_kernel": wk_ms, "gather_pairs": ga_ms},
+                "emission_roofline": {"bound": "hbm", "achieved": em_gbs, "peak": hbm_peak, "unit": "GB/s",
+                                      "frac": em_gbs / hbm_peak, "peak_source": hbm_src,
+                                      "note": "%.0f B written per band cell" % EMISSION_BYTES_PER_CELL},
+                "critical_path": {"longest_region_antidiagonals": longest,
+                                  "worker_ns_per_antidiagonal": wk_ms * 1e6 / longest,
+                                  "note": "the forward sweep of one region is sequential over its anti-diagonals"},
                 "gpu_launches": launches, "clocks": clocks}
     if world > 1:
         dist.barrier()

@@ -220,6 +220,10 @@ int64_t sa_batch_cells(const sa_batch *b);
 /* bytes the batch moves host->device on upload and device->host on download (after a download) */
 sa_status sa_batch_transfer_bytes(const sa_batch *b, int64_t *h2d, int64_t *d2h);
 int64_t sa_batch_regions(const sa_batch *b);
+/* device time (CUDA events) of the last sa_batch_run's three kernels: per-cell emissions, the
+ * forward / traceback-window worker, the pair gather.  Waits for them.  SA_E_ARG if the batch has
+ * not run (no counterpart in signalAlign: a diagnostic of this engine) */
+sa_status sa_batch_kernel_ms(const sa_batch *b, double *emission_ms, double *worker_ms, double *gather_ms);
 void sa_batch_destroy(sa_batch *b);
 
 /* ---- batched FP32 form without device allocation (no counterpart in signalAlign) ---- */

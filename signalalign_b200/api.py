@@ -96,6 +96,7 @@ def _bind(L):
         "sa_batch_log_likelihood": (C.c_double, [vp, C.c_int64]),
         "sa_batch_cells": (C.c_int64, [vp]),
         "sa_batch_regions": (C.c_int64, [vp]),
+        "sa_batch_kernel_ms": (C.c_int, [vp, _f64p, _f64p, _f64p]),
         "sa_batch_transfer_bytes": (C.c_int, [vp, _i64p, _i64p]),
         "sa_batch_destroy": (None, [vp]),
         "sa_align_batch_noalloc": (C.c_int, [C.POINTER(Read), C.c_int64, C.POINTER(Params), vp,
@@ -371,6 +372,12 @@ class Batch:
     @property
     def regions(self):
         return lib().sa_batch_regions(self._h)
+
+    def kernel_ms(self):
+        """(emission, worker, gather) device milliseconds of the last run"""
+        e, w, g = C.c_double(0), C.c_double(0), C.c_double(0)
+        _check(lib().sa_batch_kernel_ms(self._h, C.byref(e), C.byref(w), C.byref(g)), "batch_kernel_ms")
+        return e.value, w.value, g.value
 
     def transfer_bytes(self):
         h, d = C.c_int64(0), C.c_int64(0)

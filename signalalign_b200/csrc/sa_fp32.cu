@@ -132,8 +132,13 @@ struct sa_batch {
     unsigned char *dev_base = nullptr;
     std::vector<double> read_ll;
     bool downloaded = false;
+    // device timing of the last run's kernels (batches that own their device memory only)
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool timed = false;
 
     ~sa_batch() {
+        for (cudaEvent_t &e : ev)
+            if (e) cudaEventDestroy(e);
         mem_put(host_in);
         mem_put(host_res);
         mem_put(host_pairs);
@@ -555,8 +560,15 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
         sms = std::max(1, sms);
-        emission_kernel<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(sms * 8, (a.n_chunks + 7) / 8)), 256, 0,
-                          s>>>(a);
+        b->timed = false;
+        if (b->owns_device && !b->ev[0])
+            for (cudaEvent_t &e : b->ev) cudaEventCreate(&e);
+        const bool timing = b->owns_device && b->ev[3];
+        if (timing) cudaEventRecord(b->ev[0], s);
+        emission_kernel<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(sms * 16, (a.n_chunks + kEmitWarps - 1) /
+                                                                                            kEmitWarps)),
+                          32 * kEmitWarps, 0, s>>>(a);
+        if (timing) cudaEventRecord(b->ev[1], s);
         auto launch = [&](auto kern) {
             if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
@@ -566,7 +578,12 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         if (cpt_pow2 == 1) launch(worker_kernel<1>);
         else if (cpt_pow2 == 2) launch(worker_kernel<2>);
         else launch(worker_kernel<4>);
+        if (timing) cudaEventRecord(b->ev[2], s);
         gather_pairs<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(b->n_reads, sms * 4)), 256, 0, s>>>(a);
+        if (timing) {
+            cudaEventRecord(b->ev[3], s);
+            b->timed = true;
+        }
         count_launch(3);
         if (cudaGetLastError() != cudaSuccess) st = SA_E_CUDA;
     }
@@ -644,6 +661,19 @@ double sa_batch_log_likelihood(const sa_batch *b, int64_t read) {
 }
 
 int64_t sa_batch_cells(const sa_batch *b) { return b ? b->cells : 0; }
+
+sa_status sa_batch_kernel_ms(const sa_batch *b, double *emission_ms, double *worker_ms, double *gather_ms) {
+    if (!b || !emission_ms || !worker_ms || !gather_ms) return SA_E_ARG;
+    if (!b->timed) return SA_E_ARG;
+    float t[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k)
+        if (cudaEventSynchronize(b->ev[k + 1]) != cudaSuccess || cudaEventElapsedTime(&t[k], b->ev[k], b->ev[k + 1]) != cudaSuccess)
+            return SA_E_CUDA;
+    *emission_ms = t[0];
+    *worker_ms = t[1];
+    *gather_ms = t[2];
+    return SA_OK;
+}
 
 sa_status sa_batch_transfer_bytes(const sa_batch *b, int64_t *h2d_bytes, int64_t *d2h_bytes) {
     if (!b || !h2d_bytes || !d2h_bytes) return SA_E_ARG;

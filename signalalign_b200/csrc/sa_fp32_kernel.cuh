@@ -425,30 +425,37 @@ __device__ __forceinline__ void ring_init(float *base, int wmax) {
 // ------------------------------------------------------------------------------------------------
 // emission kernel: match / extra-event emissions of every band cell
 // ------------------------------------------------------------------------------------------------
-// match / extra-event emissions of column x against row y (the emission calls of
-// stateMachine3_cellCalculate, stateMachine.c:1194-1257, and of its HDP form, :1259-1325); -inf
-// without a k-mer (x = 0) or without an event (y = 0)
-__device__ __forceinline__ void cell_emissions(const Ctx &c, int32_t x, int32_t y, float &em, float &ey) {
-    const Args &A = *c.A;
-    if (x < 1 || x > c.R.lX || y < 1 || y > c.R.lY) {
-        em = ey = kNegInf;
-        return;
-    }
-    const int32_t kid = __ldg(A.kmer + c.R.kmer_base + x - 1);
-    const float4 ev4 = __ldg(reinterpret_cast<const float4 *>(A.events + c.R.event_base + y - 1));
-    const float4 *kp = reinterpret_cast<const float4 *>(c.M->kc + kid);
-    const float4 ka = __ldg(kp), kb = __ldg(kp + 1);
-    const KmerConst32 k{ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
-    const Event32 ev{ev4.x, ev4.y, ev4.z, ev4.w};
+// match / extra-event emissions of every band cell (the emission calls of stateMachine3_cellCalculate,
+// stateMachine.c:1194-1257, and of its HDP form, :1259-1325); -inf without a k-mer (x = 0) or
+// without an event (y = 0)
+// Per warp, one chunk of anti-diagonals at a time.  The chunk's cells cover a small range of
+// columns and rows (the band drifts by under one cell per anti-diagonal), so the k-mer constants of
+// its columns and the events of its rows are gathered once into the warp's shared memory and every
+// cell reads them from there; a chunk whose ranges exceed kEmitSpan reads global memory per cell.
+constexpr int kEmitWarps = 4;
+constexpr int kEmitSpan = 192;
+struct EmitStage {
+    KmerConst32 kc[kEmitSpan];
+    float4 ev[kEmitSpan];
+    int32_t kid[kEmitSpan];
+};
+
+__device__ __forceinline__ void emit_cell(const Ctx &c, const KmerConst32 &k, int32_t kid, const float4 &v, bool ok,
+                                          float &em, float &ey) {
+    em = ey = kNegInf;
+    if (!ok) return;
+    const Event32 e{v.x, v.y, v.z, v.w};
     if (c.hdp) {
-        em = ey = emit_hdp(c.M->hdp, k, kid, ev, c.rs);
+        em = ey = emit_hdp(c.M->hdp, k, kid, e, c.rs);
     } else {
-        emit_gauss(k, ev, c.rs, em, ey);
+        emit_gauss(k, e, c.rs, em, ey);
     }
 }
 
-__global__ void __launch_bounds__(256) emission_kernel(const __grid_constant__ Args A) {
+__global__ void __launch_bounds__(32 * kEmitWarps) emission_kernel(const __grid_constant__ Args A) {
+    __shared__ EmitStage stage[kEmitWarps];
     const int lane = threadIdx.x & 31;
+    EmitStage &st = stage[threadIdx.x >> 5];
     const int64_t warps = (int64_t) gridDim.x * (blockDim.x >> 5);
     for (int64_t ch = blockIdx.x * (int64_t) (blockDim.x >> 5) + (threadIdx.x >> 5); ch < A.n_chunks; ch += warps) {
         const Chunk C = A.chunks[ch];
@@ -463,20 +470,59 @@ __global__ void __launch_bounds__(256) emission_kernel(const __grid_constant__ A
             if (lane >= o) off += t;
         }
         off -= w;
+        // column and row ranges of the chunk's cells, over all its anti-diagonals
+        int32_t xlo, xhi, ylo, yhi;
+        {
+            const int32_t dk = C.d0 + lane, Lk = mt.x, Rk = mt.x + 2 * (w - 1);
+            const bool in = lane < C.nd;
+            xlo = __reduce_min_sync(0xffffffffu, in ? (dk + Lk) >> 1 : INT32_MAX);
+            xhi = __reduce_max_sync(0xffffffffu, in ? (dk + Rk) >> 1 : INT32_MIN);
+            ylo = __reduce_min_sync(0xffffffffu, in ? (dk - Rk) >> 1 : INT32_MAX);
+            yhi = __reduce_max_sync(0xffffffffu, in ? (dk - Lk) >> 1 : INT32_MIN);
+        }
+        const bool staged = xhi - xlo < kEmitSpan && yhi - ylo < kEmitSpan;
+        if (staged) {
+            for (int q = lane; q <= xhi - xlo; q += 32) {
+                const int32_t x = xlo + q;
+                const bool ok = x >= 1 && x <= c.R.lX;
+                const int32_t kid = ok ? __ldg(A.kmer + c.R.kmer_base + x - 1) : 0;
+                const float4 *kp = reinterpret_cast<const float4 *>(c.M->kc + kid);
+                const float4 ka = __ldg(kp), kb = __ldg(kp + 1);
+                st.kc[q] = KmerConst32{ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
+                st.kid[q] = kid;
+            }
+            for (int q = lane; q <= yhi - ylo; q += 32) {
+                const int32_t y = ylo + q;
+                const int32_t yc = clampi(y - 1, 0, max(c.R.lY - 1, 0));
+                st.ev[q] = __ldg(reinterpret_cast<const float4 *>(A.events + c.R.event_base + yc));
+            }
+            __syncwarp();
+        }
         for (int k = 0; k < C.nd; ++k) {
             const int32_t d = C.d0 + k;
             const int32_t L = __shfl_sync(0xffffffffu, mt.x, k);
             const int32_t W = __shfl_sync(0xffffffffu, w, k);
-            const int64_t cell = C.cell + __shfl_sync(0xffffffffu, off, k);
-            float *Ed = A.E + 2 * cell;
+            float *Ed = A.E + 2 * (C.cell + __shfl_sync(0xffffffffu, off, k));
             for (int i = lane; i < W; i += 32) {
-                const int32_t xmy = L + 2 * i;
+                const int32_t xmy = L + 2 * i, x = (d + xmy) >> 1, y = (d - xmy) >> 1;
+                const bool ok = x >= 1 && x <= c.R.lX && y >= 1 && y <= c.R.lY;
                 float em, ey;
-                cell_emissions(c, (d + xmy) >> 1, (d - xmy) >> 1, em, ey);
+                if (staged) {
+                    emit_cell(c, st.kc[x - xlo], st.kid[x - xlo], st.ev[y - ylo], ok, em, ey);
+                } else {
+                    const int32_t kid = ok ? __ldg(A.kmer + c.R.kmer_base + x - 1) : 0;
+                    const float4 *kp = reinterpret_cast<const float4 *>(c.M->kc + kid);
+                    const float4 ka = __ldg(kp), kb = __ldg(kp + 1);
+                    const KmerConst32 kk{ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
+                    const float4 v = __ldg(reinterpret_cast<const float4 *>(
+                        A.events + c.R.event_base + clampi(y - 1, 0, max(c.R.lY - 1, 0))));
+                    emit_cell(c, kk, kid, v, ok, em, ey);
+                }
                 Ed[SE_M * W + i] = em;
                 Ed[SE_Y * W + i] = ey;
             }
         }
+        __syncwarp();   // the stage is rewritten by the warp's next chunk
     }
 }
 
