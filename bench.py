@@ -46,6 +46,11 @@ def parse_args():
     ap.add_argument("--reads", type=int, default=256)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--quick", action="store_true", help="skip the CPU baseline and accuracy legs")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving run instead: Poisson arrivals at --load of the measured capacity, p50/p99 latency")
+    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--load", type=float, default=0.8)
+    ap.add_argument("--serve-budget", type=int, default=200_000_000, help="band cells in flight")
     return ap.parse_args()
 
 
@@ -168,8 +173,94 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args):
+    """Serving workload: log-normal spans (median 8 kb, clipped to 500 bp - 100 kb), per-request model
+    choice (6-mer ACGT or 6-mer ACEGT Gaussian table), Poisson arrivals.  Capacity is measured first
+    (all requests of a saturation set submitted at once); the timed run offers --load of it.  Latency
+    is submission to completion as the server records it (planning, upload, kernels, download)."""
+    import torch
+    from oracle import formats
+    from signalalign_b200 import api, synth
+    torch.cuda.set_device(0)
+    r = np.random.Generator(np.random.PCG64(args.seed + 404))
+    models = []
+    for alphabet in ("ACGT", "ACEGT"):
+        table = synth.gaussian_table(alphabet, 6, 1000 + len(alphabet))
+        m = formats.parse_model_lines(*synth.model_text(alphabet, 6, table).split("\n")[:3])
+        sm = api.StateMachine.from_tables(alphabet, 6, m["t"], m["match"], m["gapy"], m["gapx"],
+                                          emission=api.EMIT_DESCALED)
+        models.append((alphabet, table, sm))
+    n = args.serve_requests
+    spans = np.clip(np.exp(np.log(8000.0) + 0.6 * r.standard_normal(n)), 500, 100000).astype(int)
+    reqs = []
+    for L in spans:
+        alphabet, table, sm = models[int(r.integers(0, 2))]
+        seq = synth.random_reference(int(L), r, alphabet)
+        rd = synth.make_read(seq, alphabet, 6, table[:, 0], table[:, 1], table[:, 2], table[:, 3], r)
+        lo, hi = api.band_construct(rd["anchors"], len(seq) - 5, len(rd["events"]), 50)
+        reqs.append((api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                                   scale=rd["scale"], shift=rd["shift"]), int(L), int(np.sum((hi - lo) // 2 + 1))))
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    srv = api.Server(device=0, max_inflight_cells=args.serve_budget, max_batches=8)
+    try:
+        for q, _, _ in reqs[:8]:                       # warm-up: tables resident, pools filled
+            t = srv.submit(q, p)
+            srv.wait(t)
+            srv.result(t)
+        sat = reqs[: max(16, n // 2)]
+        t0 = time.perf_counter()
+        ts = [srv.submit(q, p) for q, _, _ in sat]
+        for t in ts:
+            srv.wait(t)
+            srv.result(t)
+        cap = len(sat) / (time.perf_counter() - t0)
+        rate = args.load * cap
+        arrivals = np.cumsum(r.exponential(1.0 / rate, n))
+        sampler = ClockSampler(0)
+        sampler.start()
+        tickets = []
+        t0 = time.perf_counter()
+        for (q, L, c), at in zip(reqs, arrivals):
+            while True:
+                dt = at - (time.perf_counter() - t0)
+                if dt <= 0:
+                    break
+                time.sleep(min(dt, 0.0005))
+            tickets.append((srv.submit(q, p), L, c))
+        res = []
+        for t, L, c in tickets:
+            srv.wait(t, 600000.0)
+            st, pairs, ll, lat = srv.result(t)
+            res.append((st, L, c, lat))
+        wall = time.perf_counter() - t0
+        clocks = sampler.stop()
+    finally:
+        srv.close()
+    lat = np.array([x[3] for x in res])
+    spans_ok = np.array([x[1] for x in res])
+    ten = lat[(spans_ok >= 8000) & (spans_ok <= 12000)]
+    cells = sum(x[2] for x in res)
+    line = {"metric": "serving_p99_latency_ms", "value": float(np.percentile(lat, 99)), "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "%d requests, log-normal spans (median 8 kb, sigma 0.6, clipped 500 bp-100 kb), "
+                                   "6-mer ACGT / ACEGT Gaussian tables per request, Poisson arrivals at %.0f%% of "
+                                   "measured capacity" % (n, 100 * args.load),
+                       "band_cell_budget": args.serve_budget, "streams": 8},
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p50_ms_8to12kb": float(np.percentile(ten, 50)) if len(ten) else None,
+            "p99_ms_8to12kb": float(np.percentile(ten, 99)) if len(ten) else None,
+            "reads_8to12kb": int(len(ten)),
+            "capacity_reads_per_sec": cap, "offered_reads_per_sec": rate,
+            "achieved_reads_per_sec": n / wall, "cells_per_sec": cells / wall,
+            "errors": int(sum(1 for x in res if x[0] != 0)), "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.serve:
+        run_serve(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

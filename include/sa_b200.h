@@ -265,6 +265,26 @@ sa_status sa_align_batch_noalloc(const sa_read *reads, int64_t n_reads, const sa
                                  sa_aligned_pair *pairs, int64_t pair_capacity, int64_t *pair_offsets,
                                  int32_t *read_status, double *log_likelihood, int64_t *scratch_bytes);
 
+/* ---- serving: reads aligned as they arrive, with continuous batching ----
+ * No counterpart in signalAlign, which aligns one read per process (scripts/runSignalAlign.py:176-224).
+ * A dispatcher thread admits waiting reads into a new micro-batch whenever a stream is free and the
+ * band cells in flight (estimated as (reference_length + n_events + 1) x (diagonal_expansion + 1)
+ * per read) stay within max_inflight_cells; each micro-batch runs on its own stream, beside the ones
+ * already on the device.  A read's result does not depend on which reads share its micro-batch. */
+typedef struct sa_server sa_server;
+sa_status sa_server_create(int32_t device, int64_t max_inflight_cells, int32_t max_batches, sa_server **out);
+/* queue one read (its arrays are copied); *ticket identifies it */
+sa_status sa_server_submit(sa_server *s, const sa_read *read, const sa_params *p, int64_t *ticket);
+/* block until the read is done or timeout_ms passed (SA_E_TIMEOUT) */
+sa_status sa_server_wait(sa_server *s, int64_t ticket, double timeout_ms);
+/* a finished read: its status, pairs (owned by the server until sa_server_release), log-likelihood
+ * and latency from submission to completion in milliseconds (either may be NULL) */
+sa_status sa_server_result(sa_server *s, int64_t ticket, int32_t *status, const sa_aligned_pair **pairs,
+                           int64_t *n_pairs, double *log_likelihood, double *latency_ms);
+sa_status sa_server_release(sa_server *s, int64_t ticket);
+/* finishes the queued reads, then stops the dispatcher */
+void sa_server_destroy(sa_server *s);
+
 /* ---- diagnostics ---- */
 const char *sa_status_string(sa_status s);
 /* number of kernel launches this process has made through the library (all entry points) */

@@ -102,6 +102,13 @@ def _bind(L):
         "sa_align_batch_noalloc": (C.c_int, [C.POINTER(Read), C.c_int64, C.POINTER(Params), vp,
                                              C.POINTER(AlignedPair), C.c_int64, _i64p, C.POINTER(C.c_int32), _f64p,
                                              _i64p]),
+        "sa_server_create": (C.c_int, [C.c_int32, C.c_int64, C.c_int32, C.POINTER(vp)]),
+        "sa_server_submit": (C.c_int, [vp, C.POINTER(Read), C.POINTER(Params), _i64p]),
+        "sa_server_wait": (C.c_int, [vp, C.c_int64, C.c_double]),
+        "sa_server_result": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.POINTER(AlignedPair)), _i64p,
+                                       _f64p, _f64p]),
+        "sa_server_release": (C.c_int, [vp, C.c_int64]),
+        "sa_server_destroy": (None, [vp]),
         "sa_status_string": (C.c_char_p, [C.c_int]),
         "sa_kernel_launch_count": (C.c_int64, []),
         "sa_measure_fp32_peak": (C.c_int, [C.c_int32, _f64p]),
@@ -454,6 +461,50 @@ def align_batch_noalloc(reads, p, stream=None, pair_capacity=None):
         _check(st, "align_batch_noalloc")
         return NoallocResult(pairs, off, status, ll, need.value)
     raise SAError(6, "align_batch_noalloc")
+
+
+class Server:
+    """Continuous-batching serving loop (sa_server_*): submit reads as they arrive, wait for each."""
+
+    def __init__(self, device=0, max_inflight_cells=200_000_000, max_batches=8):
+        h = C.c_void_p()
+        _check(lib().sa_server_create(device, max_inflight_cells, max_batches, C.byref(h)), "server_create")
+        self._h = h
+
+    def submit(self, read, p):
+        keep = []
+        arr = _read_array([read], keep)
+        t = C.c_int64(0)
+        _check(lib().sa_server_submit(self._h, arr, C.byref(p), C.byref(t)), "server_submit")
+        return t.value
+
+    def wait(self, ticket, timeout_ms=60000.0):
+        _check(lib().sa_server_wait(self._h, ticket, timeout_ms), "server_wait")
+
+    def result(self, ticket, release=True):
+        """(status, pairs, log_likelihood, latency_ms) of a finished read"""
+        st = C.c_int32(0)
+        ptr = C.POINTER(AlignedPair)()
+        n = C.c_int64(0)
+        ll, lat = C.c_double(0), C.c_double(0)
+        _check(lib().sa_server_result(self._h, ticket, C.byref(st), C.byref(ptr), C.byref(n), C.byref(ll),
+                                      C.byref(lat)), "server_result")
+        if n.value > 0:
+            pairs = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_int64)), shape=(n.value * 4,)).copy()
+            pairs = pairs.view(PAIR_DTYPE).reshape(-1)
+        else:
+            pairs = np.zeros(0, PAIR_DTYPE)
+        if release:
+            lib().sa_server_release(self._h, ticket)
+        return st.value, pairs, ll.value, lat.value
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.sa_server_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        self.close()
 
 
 def kernel_launch_count():

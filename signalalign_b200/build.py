@@ -16,6 +16,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.pat
 SOURCES = [
     ("sa_host.cpp", []),
     ("sa_memory.cpp", []),
+    ("sa_server.cpp", []),
     ("sa_fp64.cu", ["-fmad=false"]),
     ("sa_fp32.cu", []),
     ("sa_noalloc.cu", []),

@@ -572,7 +572,9 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         auto launch = [&](auto kern) {
             if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
-            const int64_t grid = (int64_t) sms * std::max(1, per_sm);
+            // a small batch takes a forward CTA and about two CTAs of window warps per region, so
+            // small batches on other streams run beside it
+            const int64_t grid = std::min<int64_t>((int64_t) sms * std::max(1, per_sm), 3 * (int64_t) nr);
             kern<<<(unsigned) grid, kThreads, smem, s>>>(a);
         };
         if (cpt_pow2 == 1) launch(worker_kernel<1>);

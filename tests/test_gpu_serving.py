@@ -1,0 +1,83 @@
+"""Serving loop (sa_server_*): reads submitted as they arrive, continuous batching.
+
+A read's result must be the same alone and in a mix of concurrent reads (the FP32 form's tolerance:
+posterior error <= 1e-4, log-likelihood 1e-3 relative), and the same as the batch entry point's.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from signalalign_b200 import synth
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from signalalign_b200 import api as a
+    return a
+
+
+def _inputs(api, sm, reads):
+    return [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                          scale=rd["scale"], shift=rd["shift"]) for rd in reads]
+
+
+def _same(api, a, b, thr):
+    st_a, pa, lla, _ = a
+    st_b, pb, llb, _ = b
+    assert st_a == 0 and st_b == 0
+    assert len(pa) > 0
+    assert W.max_posterior_error(pa, pb, thr) <= FP32_TOL
+    assert abs(lla - llb) <= 1e-3 * abs(lla)
+
+
+def test_result_same_alone_and_in_mix(api):
+    cfg = synth.config1(seed=31, n_reads=9, span=(500, 4000))
+    sm = W.gpu_model(api, W.gaussian_model(cfg), orc.EMIT_DESCALED)
+    reads = _inputs(api, sm, cfg["reads"])
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    srv = api.Server(max_inflight_cells=50_000_000, max_batches=4)
+    try:
+        t = srv.submit(reads[0], p)
+        srv.wait(t)
+        alone = srv.result(t)
+        # the same read again, submitted in the middle of a stream of others
+        tickets = [srv.submit(r, p) for r in reads[1:5]] + [srv.submit(reads[0], p)] + \
+                  [srv.submit(r, p) for r in reads[5:]]
+        for tk in tickets:
+            srv.wait(tk)
+        mixed = [srv.result(tk) for tk in tickets]
+    finally:
+        srv.close()
+    _same(api, alone, mixed[4], p.threshold)
+    assert all(m[3] > 0 for m in mixed)
+    # and each read as the batch entry point gives it
+    batch = api.align_batch(reads, p)
+    order = [1, 2, 3, 4, 0, 5, 6, 7, 8]
+    for k, r in enumerate(order):
+        _same(api, (batch.status(r), batch.pairs(r), batch.log_likelihood(r), 0.0), mixed[k], p.threshold)
+
+
+def test_server_reports_per_read_errors(api):
+    cfg = synth.config1(seed=32, n_reads=2, span=(500, 800))
+    sm = W.gpu_model(api, W.gaussian_model(cfg), orc.EMIT_DESCALED)
+    reads = _inputs(api, sm, cfg["reads"])
+    bad = api.ReadInput(sm=sm, reference="ACGTNNACGTACGTACGT", events=reads[0].events[:20], anchors=np.zeros((0, 2)))
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    srv = api.Server(max_inflight_cells=10_000_000, max_batches=2)
+    try:
+        tickets = [srv.submit(reads[0], p), srv.submit(bad, p), srv.submit(reads[1], p)]
+        for tk in tickets:
+            srv.wait(tk)
+        res = [srv.result(tk) for tk in tickets]
+    finally:
+        srv.close()
+    assert res[0][0] == 0 and res[2][0] == 0
+    assert res[1][0] == 2    # SA_E_ALPHABET, the other reads unaffected
