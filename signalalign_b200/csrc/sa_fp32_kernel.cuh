@@ -1176,6 +1176,9 @@ struct WarpWindow {
             }
         } else {
             const float shU = -gamma0, shM = -gamma1 - gamma0;
+            // all ring reads first, then the arithmetic, then the ring writes: the cells' chains are
+            // independent, and no shared-memory store sits between them to order them
+            float bme[WCPT], bue[WCPT], ble[WCPT];
 #pragma unroll
             for (int j = 0; j < WCPT; ++j) {
                 const int i = lane + 32 * j;
@@ -1183,26 +1186,36 @@ struct WarpWindow {
                 const int ipp = clampi((xmy - mpp.L) >> 1, -1, wmax);
                 const int iu = clampi((xmy - 1 - mp.L) >> 1, -1, wmax);
                 const int il = clampi((xmy + 1 - mp.L) >> 1, -1, wmax);
+                bme[j] = s2[ipp];
+                bue[j] = s1[2 * stride + iu];
+                ble[j] = s1[stride + il];
+            }
+#pragma unroll
+            for (int j = 0; j < WCPT; ++j) {
                 // each successor's backward value plus its emission, shared by the transitions into it
-                const float bme = s2[ipp] + (qM[K][j] + shM);
-                float vM = bme + t[T_MC];
-                float vX = bme + t[T_MFGX];
-                float vY = bme + t[T_MFGY];
-                const float bue = s1[2 * stride + iu] + (qY[K][j] + shU);
-                vM = lae(tab, vM, bue + t[T_OY]);
-                vY = lae(tab, vY, bue + t[T_EY]);
-                const float ble = s1[stride + il] + (qX[K][j] + shU);
-                vM = lae(tab, vM, ble + t[T_OX]);
-                vX = lae(tab, vX, ble + t[T_EX]);
-                vY = lae(tab, vY, ble + t[T_SX]);
-                if (i >= W0) vM = vX = vY = kNegInf;
-                s0[i] = vM;
-                s0[stride + i] = vX;
-                s0[2 * stride + i] = vY;
-                bM[j] = vM;
-                bX[j] = vX;
-                bY[j] = vY;
-                lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
+                const float me = bme[j] + (qM[K][j] + shM);
+                float vM = me + t[T_MC];
+                float vX = me + t[T_MFGX];
+                float vY = me + t[T_MFGY];
+                const float ue = bue[j] + (qY[K][j] + shU);
+                vM = lae(tab, vM, ue + t[T_OY]);
+                vY = lae(tab, vY, ue + t[T_EY]);
+                const float le = ble[j] + (qX[K][j] + shU);
+                vM = lae(tab, vM, le + t[T_OX]);
+                vX = lae(tab, vX, le + t[T_EX]);
+                vY = lae(tab, vY, le + t[T_SX]);
+                const bool in = lane + 32 * j < W0;
+                bM[j] = in ? vM : kNegInf;
+                bX[j] = in ? vX : kNegInf;
+                bY[j] = in ? vY : kNegInf;
+                lm = fmaxf(lm, fmaxf(bM[j], fmaxf(bX[j], bY[j])));
+            }
+#pragma unroll
+            for (int j = 0; j < WCPT; ++j) {
+                const int i = lane + 32 * j;
+                s0[i] = bM[j];
+                s0[stride + i] = bX[j];
+                s0[2 * stride + i] = bY[j];
             }
         }
         __syncwarp();
@@ -1213,35 +1226,43 @@ struct WarpWindow {
                 // diagonalCalculationTotalProbability (pairwiseAligner.c:1182-1200): F.B on d in
                 // ascending cell order, then the matches from d-1 over d into d+1, dotted with B(d+1)
                 const float *stg = chain + 2 * wmax;
+                const bool have_next = d < D;
+                const int32_t Wm = mm.W;
+                float sx[WCPT], sy[WCPT], tm[WCPT], tx[WCPT], ty[WCPT], te[WCPT], b1[WCPT];
 #pragma unroll
                 for (int j = 0; j < WCPT; ++j) {
                     const int i = lane + 32 * j;
-                    if (i < W0) {
-                        float s = qF[K][j] + bM[j];
-                        s = lae(tab, s, stg[i] + bX[j]);
-                        s = lae(tab, s, stg[wmax + i] + bY[j]);
-                        chain[i] = s;
-                    }
+                    sx[j] = stg[i];
+                    sy[j] = stg[wmax + i];
+                    tm[j] = stg[2 * wmax + i];
+                    tx[j] = stg[3 * wmax + i];
+                    ty[j] = stg[4 * wmax + i];
+                    te[j] = stg[5 * wmax + i];
+                    b1[j] = s1[i];
                 }
-                const bool have_next = d < D;
-                if (have_next) {
-                    const int32_t Wm = mm.W;
+                float c0[WCPT], c1[WCPT];
 #pragma unroll
-                    for (int j = 0; j < WCPT; ++j) {
-                        const int i = lane + 32 * j;
-                        if (i < Wp) {
-                            const int32_t xmy1 = mp.L + 2 * i;
-                            const int32_t r = (xmy1 - mm.L) >> 1;
-                            float mth = kNegInf;
-                            if (Wm > 0 && xmy1 >= mm.L && r < Wm) {
-                                const float e = stg[5 * wmax + i];
-                                mth = stg[2 * wmax + i] + (e + t[T_MC]);
-                                mth = lae(tab, mth, stg[3 * wmax + i] + (e + t[T_MFGX]));
-                                mth = lae(tab, mth, stg[4 * wmax + i] + (e + t[T_MFGY]));
-                            }
-                            chain[wmax + i] = mth + s1[i];
-                        }
+                for (int j = 0; j < WCPT; ++j) {
+                    const int i = lane + 32 * j;
+                    float v = qF[K][j] + bM[j];
+                    v = lae(tab, v, sx[j] + bX[j]);
+                    c0[j] = lae(tab, v, sy[j] + bY[j]);
+                    const int32_t xmy1 = mp.L + 2 * i;
+                    const int32_t r = (xmy1 - mm.L) >> 1;
+                    float mth = kNegInf;
+                    if (Wm > 0 && xmy1 >= mm.L && r < Wm) {
+                        const float e = te[j];
+                        mth = tm[j] + (e + t[T_MC]);
+                        mth = lae(tab, mth, tx[j] + (e + t[T_MFGX]));
+                        mth = lae(tab, mth, ty[j] + (e + t[T_MFGY]));
                     }
+                    c1[j] = mth + b1[j];
+                }
+#pragma unroll
+                for (int j = 0; j < WCPT; ++j) {
+                    const int i = lane + 32 * j;
+                    if (i < W0) chain[i] = c0[j];
+                    if (have_next && i < Wp) chain[wmax + i] = c1[j];
                 }
                 __syncwarp();
                 const float2 ff = ordered_fold2(tab, chain, W0, chain + wmax, have_next ? Wp : 0);
