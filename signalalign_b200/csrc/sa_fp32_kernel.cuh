@@ -583,10 +583,33 @@ struct ForwardSweep {
     __device__ __forceinline__ void step(int32_t d) {
         constexpr int S0 = P, S1 = (P + 2) % 3, S2 = (P + 1) % 3;   // slots of d, d-1, d-2
         const float *t = c.t;
-        // maximum of d-1 (one instruction per warp), published for the shift of d+2
-        {
-            const float wm = warp_max1(lm_prev);
-            if (lane == 0) sh->part[S1][warp] = wm;
+        // the recursion's operands first: ring reads right after the barrier, ahead of any
+        // shared-memory store of this step that would have to be ordered before them
+        const int32_t W0 = m0.W;
+        const int32_t dl = (m0.L - 1 - m1.L) >> 1, du = (m0.L + 1 - m1.L) >> 1, dm = (m0.L - m2.L) >> 1;
+        float lM[CPT], lX[CPT], lY[CPT], mM[CPT], mX[CPT], mY[CPT], uM[CPT], uY[CPT];
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+            const int i = tid + j * kThreads;
+            const int il = clampi(i + dl, -1, wmax);
+            const int iu = clampi(i + du, -1, wmax);
+            const int im = clampi(i + dm, -1, wmax);
+            lM[j] = slot(S1, 0)[il];
+            lX[j] = slot(S1, 1)[il];
+            lY[j] = slot(S1, 2)[il];
+            mM[j] = slot(S2, 0)[im];
+            mX[j] = slot(S2, 1)[im];
+            mY[j] = slot(S2, 2)[im];
+            uM[j] = slot(S1, 0)[iu];
+            uY[j] = slot(S1, 2)[iu];
+        }
+        // emissions of d (landed three steps ago)
+        float eM[CPT], eY[CPT], eX[CPT];
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+            eM[j] = pM[P][j];
+            eY[j] = pY[P][j];
+            eX[j] = pV[P][j] ? pX[P][j] : kNegInf;
         }
         // shift of d+1 from the maximum of d-2 (complete since the last barrier):
         // base(d+1) - base(d) = max(d-2) - delta(d) - delta(d-1)
@@ -596,54 +619,45 @@ struct ForwardSweep {
             const float mx = fmaxf(fmaxf(fp[0], fp[1]), fmaxf(fp[2], fp[3]));
             delta_next = ((mx > kNegInf ? mx : 0.0f) - delta0) - delta1;
         }
-        // band facts: d+3 decoded (loaded three steps ago), d+6 requested
+        // band facts: d+3 decoded (loaded three steps ago), d+6 requested; loads of d+3
         const Meta m3 = decode_meta(raw[P], d + 3 <= n);
         near[P] = m3;
         raw[P] = raw_meta(A, db, d + 6, n);
-        // emissions of d (landed), then the loads of d+3 into the same phase
-        float eM[CPT], eY[CPT], eX[CPT];
-#pragma unroll
-        for (int j = 0; j < CPT; ++j) {
-            eM[j] = pM[P][j];
-            eY[j] = pY[P][j];
-            eX[j] = pV[P][j] ? pX[P][j] : kNegInf;
-        }
         prefetch<P>(d + 3, m3, eoff3);
         eoff3 += m3.W;
         // the recursion on d (stateMachine3_cellCalculate order: lower -> gap-X, middle -> match,
         // upper -> gap-Y, each state accumulated from LOG_ZERO)
-        const int32_t W0 = m0.W;
         const float shL = -delta0, shM = -delta1 - delta0;
         const bool store_gaps = (m0.flags & kFlagStoreGaps) != 0;
-        const int32_t dl = (m0.L - 1 - m1.L) >> 1, du = (m0.L + 1 - m1.L) >> 1, dm = (m0.L - m2.L) >> 1;
         float lm = kNegInf;
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
             const int i = tid + j * kThreads;
-            const int il = clampi(i + dl, -1, wmax);
-            const int iu = clampi(i + du, -1, wmax);
-            const int im = clampi(i + dm, -1, wmax);
             // logAdd depends only on the difference of its arguments, so the cell's emission (and
             // the shift to this anti-diagonal's base) is added once after each state's fold
-            float vX = lae(tab, slot(S1, 0)[il] + t[T_OX], slot(S1, 1)[il] + t[T_EX]);
-            vX = lae(tab, vX, slot(S1, 2)[il] + t[T_SX]) + (eX[j] + shL);
-            float vM = lae(tab, slot(S2, 0)[im] + t[T_MC], slot(S2, 1)[im] + t[T_MFGX]);
-            vM = lae(tab, vM, slot(S2, 2)[im] + t[T_MFGY]) + (eM[j] + shM);
-            const float vY = lae(tab, slot(S1, 0)[iu] + t[T_OY], slot(S1, 2)[iu] + t[T_EY]) + (eY[j] + shL);
+            float vX = lae(tab, lM[j] + t[T_OX], lX[j] + t[T_EX]);
+            vX = lae(tab, vX, lY[j] + t[T_SX]) + (eX[j] + shL);
+            float vM = lae(tab, mM[j] + t[T_MC], mX[j] + t[T_MFGX]);
+            vM = lae(tab, vM, mY[j] + t[T_MFGY]) + (eM[j] + shM);
+            float vY = lae(tab, uM[j] + t[T_OY], uY[j] + t[T_EY]) + (eY[j] + shL);
             const bool in = i < W0;
-            if (!in) vM = vX = kNegInf;
-            const float vYs = in ? vY : kNegInf;
+            if (!in) vM = vX = vY = kNegInf;
             slot(S0, 0)[i] = vM;
             slot(S0, 1)[i] = vX;
-            slot(S0, 2)[i] = vYs;
+            slot(S0, 2)[i] = vY;
             if (in) {
                 Fd[ST_M * W0 + i] = vM;
                 if (store_gaps) {
                     Fd[ST_X * W0 + i] = vX;
-                    Fd[ST_Y * W0 + i] = vYs;
+                    Fd[ST_Y * W0 + i] = vY;
                 }
             }
-            lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vYs)));
+            lm = fmaxf(lm, fmaxf(vM, fmaxf(vX, vY)));
+        }
+        // maximum of d-1 (one instruction per warp), published for the shift of d+2
+        {
+            const float wm = warp_max1(lm_prev);
+            if (lane == 0) sh->part[S1][warp] = wm;
         }
         if (tid == 0) {
             A.base[db + d] = base0;
