@@ -46,6 +46,9 @@ def parse_args():
     ap.add_argument("--reads", type=int, default=256)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--quick", action="store_true", help="skip the CPU baseline and accuracy legs")
+    ap.add_argument("--config", type=int, default=1, choices=[1, 2, 3],
+                    help="1: the 256-read Gaussian batch (default); 2: 128 HDP reads (6-mer ACEGT, 2000-point "
+                         "grid); 3: 512 2D reads x {C, E} hypotheses, Gaussian and HDP mixed")
     ap.add_argument("--serve", action="store_true",
                     help="serving run instead: Poisson arrivals at --load of the measured capacity, p50/p99 latency")
     ap.add_argument("--serve-requests", type=int, default=400)
@@ -256,10 +259,93 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_config(args):
+    """Configs 2 and 3 on one GPU: the device time of sa_batch_run over every alignment (config 3 in
+    sub-batches of 512 alignments, which bounds the stores to ~40 GB), the end-to-end time of
+    sa_align_batch, and the posterior error against the FP64 oracle on the shortest alignments."""
+    import torch
+    from oracle import formats
+    from oracle import oracle as orc
+    from signalalign_b200 import api, synth
+    torch.cuda.set_device(0)
+    tests_dir = os.path.join(ROOT, "tests")
+    sys.path.insert(0, tests_dir)
+    import workloads as W
+    if args.config == 2:
+        cfg = synth.config2(seed=args.seed + 1)
+        hdp = W.hdp_dict(cfg["hdp"], 5 ** 6)
+        m = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["table"]).split("\n")[:3])
+        sm = W.gpu_model(api, m, orc.EMIT_HDP, None, hdp)
+        als = [dict(rd, model="hdp") for rd in cfg["reads"]]
+        models = {"hdp": (sm, m, orc.EMIT_HDP, hdp)}
+        workload = "128 reads x U(5kb,15kb), 6-mer ACEGT HDP (15,625 k-mers, 2000-point grid), expansion 50"
+        sub = len(als)
+    else:
+        cfg = synth.config3(seed=args.seed + 2)
+        hdp = W.hdp_dict(cfg["hdp"], 5 ** 6)
+        gm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["gauss_table"]).split("\n")[:3])
+        hm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["hdp_table"]).split("\n")[:3])
+        models = {"gauss": (W.gpu_model(api, gm, orc.EMIT_DESCALED), gm, orc.EMIT_DESCALED, None),
+                  "hdp": (W.gpu_model(api, hm, orc.EMIT_HDP, None, hdp), hm, orc.EMIT_HDP, hdp)}
+        als = cfg["alignments"]
+        workload = ("512 reads x U(1kb,30kb) x {template, complement} x {all-C, all-E} at CCWGG sites = 2048 "
+                    "alignments, 6-mer ACEGT Gaussian and HDP machines mixed")
+        sub = 512
+    p = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=50, threshold=0.01)
+    inputs = [api.ReadInput(sm=models[a["model"]][0], reference=a["reference"], events=a["events"],
+                            anchors=a["anchors"], scale=a["scale"], shift=a["shift"]) for a in als]
+    groups = [inputs[i:i + sub] for i in range(0, len(inputs), sub)]
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    cells, dev_ms, e2e_ms = 0, 0.0, 0.0
+    launches0 = api.kernel_launch_count()
+    for g in groups:
+        b = api.Batch(g, p)
+        b.upload(sptr)
+        for _ in range(max(3, args.warmup)):
+            b.run(sptr)
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.run(sptr)
+            e1.record(stream)
+            e1.synchronize()
+            dev_ms += e0.elapsed_time(e1) / args.steps
+        cells += b.cells
+        del b
+        t0 = time.perf_counter()
+        bb = api.align_batch(g, p, sptr)
+        torch.cuda.synchronize()
+        e2e_ms += (time.perf_counter() - t0) * 1e3
+        del bb
+    # accuracy on the 4 shortest alignments
+    order = np.argsort([len(a["events"]) for a in als])[:4]
+    bb = api.align_batch([inputs[i] for i in order], p, sptr)
+    errs = []
+    for k, i in enumerate(order):
+        a = als[i]
+        _, mm, emis, hh = models[a["model"]]
+        om = W.oracle_model(mm, emis, a, hh)
+        want = orc.aligned_pairs(om, a["reference"], a["events"], a["anchors"], orc.params(threshold=0.01, expansion=50))
+        errs.append(W.max_posterior_error(want, bb.pairs(k), 0.01))
+    line = {"metric": METRIC, "value": cells / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload, "alignments": len(als), "cells": cells, "sub_batches": len(groups)},
+            "e2e": {"value": cells / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms},
+            "accuracy": {"max_posterior_err": max(errs), "alignments": len(errs), "vs": "FP64 CPU oracle"},
+            "gpu_launches": api.kernel_launch_count() - launches0}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.serve:
         run_serve(args)
+        return
+    if args.config != 1 and args.impl == "ours":
+        run_config(args)
         return
     if args.impl == "reference":
         run_reference(args)

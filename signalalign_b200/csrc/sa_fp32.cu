@@ -90,6 +90,7 @@ struct sa_batch {
     Span<int32_t> order;
     Span<ModelDesc> mdesc;
     Span<ReadScale32> read_scale;
+    Span<ReadScale64> read_scale64;
     Span<int2> meta;
     Span<Window> windows;
     Span<WindowTask> wtask;
@@ -109,6 +110,7 @@ struct sa_batch {
     int32_t *d_order = nullptr;
     ModelDesc *d_models = nullptr;
     ReadScale32 *d_read_scale = nullptr;
+    ReadScale64 *d_read_scale64 = nullptr;
     int2 *d_meta = nullptr;
     Window *d_windows = nullptr;
     WindowTask *d_wtask = nullptr;
@@ -175,6 +177,7 @@ size_t layout(sa_batch *b, unsigned char *host_in, unsigned char *host_res, unsi
     place(b->order, b->d_order, nr, host_in, 0);
     place(b->mdesc, b->d_models, b->models.size(), host_in, 0);
     place(b->read_scale, b->d_read_scale, nreads, host_in, 0);
+    place(b->read_scale64, b->d_read_scale64, nreads, host_in, 0);
     place(b->meta, b->d_meta, nd, host_in, 0);
     place(b->windows, b->d_windows, nw, host_in, 0);
     place(b->wtask, b->d_wtask, nw, host_in, 0);
@@ -254,6 +257,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     b->read_first_region.assign(n_reads, 0);
     b->read_n_regions.assign(n_reads, 0);
     std::vector<ReadScale32> scale(n_reads);
+    std::vector<ReadScale64> scale64(n_reads);
     std::vector<ReadPlan> plan(n_reads);
     // arguments, devices and models (serial: models are shared)
     int device = -1;
@@ -262,6 +266,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         ReadPlan &rp = plan[r];
         auto *sm = const_cast<sa_state_machine *>(rd.sm);
         std::memset(&scale[r], 0, sizeof(ReadScale32));
+        scale64[r] = ReadScale64{1.0, 0.0, 1.0, 0.0};
         if (!sm || rd.reference_length < 0 || rd.n_events < 0 || rd.n_anchors < 0 ||
             (rd.reference_length > 0 && !rd.reference) || (rd.n_events > 0 && !rd.events) ||
             (rd.n_anchors > 0 && !rd.anchors) || !(rd.var != 0.0)) {
@@ -283,6 +288,8 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         rs.shift = sm->emission == SA_EMIT_PLAIN ? 0.0f : (float) rd.shift;
         rs.inv_var = (float) (1.0 / var);
         rs.log_inv_var = (float) std::log(1.0 / var);
+        scale64[r] = ReadScale64{sm->emission == SA_EMIT_PLAIN ? 1.0 : rd.scale, sm->emission == SA_EMIT_PLAIN ? 0.0 : rd.shift,
+                                 var, 0.0};
     }
     const int threads = planning_threads();
     // k-mer ids, regions and windows of each read
@@ -342,6 +349,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     layout(b, static_cast<unsigned char *>(b->host_in.ptr), nullptr, nullptr);
     for (int64_t r = 0; r < n_reads; ++r) {
         b->read_scale[r] = scale[r];
+        b->read_scale64[r] = scale64[r];
         b->read_win[2 * r] = plan[r].win_base;
         b->read_win[2 * r + 1] = plan[r].windows;
     }
@@ -488,6 +496,12 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
             m.hdp.inv_dx = (float) (1.0 / (h.grid[1] - h.grid[0]));
             m.hdp.x_last = (float) h.grid[h.grid_length - 1];
             m.hdp.grid_length = (int32_t) h.grid_length;
+            m.hdp64.match = sm->dev.match;
+            m.hdp64.grid = sm->dev.hdp_grid;
+            m.hdp64.density = sm->dev.hdp_density;
+            m.hdp64.slope = sm->dev.hdp_slope;
+            m.hdp64.kmer_row = sm->dev.hdp_kmer_row;
+            m.hdp64.grid_length = h.grid_length;
         }
     }
     sa_status st = SA_OK;
@@ -527,6 +541,8 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         a.n_regions = (int64_t) nr;
         a.models = b->d_models;
         a.read_scale = b->d_read_scale;
+        a.read_scale64 = b->d_read_scale64;
+        a.events_raw = b->d_events_raw;
         a.meta = b->d_meta;
         a.windows = b->d_windows;
         a.wtask = b->d_wtask;

@@ -62,13 +62,30 @@ constexpr int32_t kFlagRefresh = 1 << 22;     // total-probability refresh in it
 
 enum { T_MC = 0, T_MFGX, T_MFGY, T_OX, T_OY, T_EX, T_EY, T_SX, T_SY };
 
+// FP64 HDP tables of a model (the emission kernel evaluates HDP densities in FP64: they reach far
+// below the FP32 range in the tails, and the spline's terms cancel there)
+struct Hdp64 {
+    const double *match;      // n_kmers x 5 (level mean in column 0)
+    const double *grid;       // grid_length knots
+    const double *density;    // rows x grid_length
+    const double *slope;      // rows x grid_length
+    const int64_t *kmer_row;  // n_kmers
+    int64_t grid_length;
+};
+
 struct ModelDesc {
     const KmerConst32 *kc;
     Hdp32 hdp;
+    Hdp64 hdp64;
     int32_t emission;
     int32_t pad;
     float t[9];
     float pad2;
+};
+
+// per-read FP64 descaling parameters (HDP emissions)
+struct ReadScale64 {
+    double scale, shift, var, pad;
 };
 
 struct RegionDesc {
@@ -127,6 +144,8 @@ struct Args {
     int64_t n_regions;
     const ModelDesc *models;
     const ReadScale32 *read_scale;
+    const ReadScale64 *read_scale64;
+    const double2 *events_raw;      // per event FP64 (mean, noise)
     const int2 *meta;               // per anti-diagonal {xmy of first cell, width | flags}
     const Window *windows;
     const WindowTask *wtask;
@@ -437,17 +456,44 @@ constexpr int kEmitSpan = 192;
 struct EmitStage {
     KmerConst32 kc[kEmitSpan];
     float4 ev[kEmitSpan];
+    double mean[kEmitSpan];     // FP64 event means (HDP)
     int32_t kid[kEmitSpan];
 };
 
-__device__ __forceinline__ void emit_cell(const Ctx &c, const KmerConst32 &k, int32_t kid, const float4 &v, bool ok,
-                                          float &em, float &ey) {
+// getHdpKmerDensity (stateMachine.c:468-495): log((1/var) * max(0, spline(descaled mean))) with the
+// spline of grid_spline_interp (hdp_math_utils.c:471-495), in FP64 as the reference computes it
+__device__ __forceinline__ float emit_hdp64(const Hdp64 &h, int32_t kid, double mean, const ReadScale64 &rs) {
+    const int64_t row = h.kmer_row[kid];
+    if (row < 0) return kNegInf;
+    const double mu = h.match[(int64_t) kid * 5];
+    const double u = (mean + rs.var * mu - rs.scale * mu - rs.shift) / rs.var;
+    const double *x = h.grid, *y = h.density + row * h.grid_length, *sl = h.slope + row * h.grid_length;
+    const int64_t len = h.grid_length;
+    double d;
+    if (u <= x[0]) {
+        d = y[0] - sl[0] * (x[0] - u);
+    } else if (u >= x[len - 1]) {
+        d = y[len - 1] + sl[len - 1] * (u - x[len - 1]);
+    } else {
+        const double dx = x[1] - x[0];
+        int64_t il = (int64_t) ((u - x[0]) / dx);
+        il = il > len - 2 ? len - 2 : (il < 0 ? 0 : il);
+        const double dy = y[il + 1] - y[il];
+        const double a = sl[il] * dx - dy, b = dy - sl[il + 1] * dx;
+        const double tl = (u - x[il]) / dx, tr = 1.0 - tl;
+        d = tr * y[il] + tl * y[il + 1] + tl * tr * (a * tr + b * tl);
+    }
+    return d > 0.0 ? (float) log((1.0 / rs.var) * d) : kNegInf;
+}
+
+__device__ __forceinline__ void emit_cell(const Ctx &c, const KmerConst32 &k, int32_t kid, const float4 &v,
+                                          double mean64, bool ok, float &em, float &ey) {
     em = ey = kNegInf;
     if (!ok) return;
-    const Event32 e{v.x, v.y, v.z, v.w};
     if (c.hdp) {
-        em = ey = emit_hdp(c.M->hdp, k, kid, e, c.rs);
+        em = ey = emit_hdp64(c.M->hdp64, kid, mean64, c.A->read_scale64[c.R.read]);
     } else {
+        const Event32 e{v.x, v.y, v.z, v.w};
         emit_gauss(k, e, c.rs, em, ey);
     }
 }
@@ -495,6 +541,7 @@ __global__ void __launch_bounds__(32 * kEmitWarps) emission_kernel(const __grid_
                 const int32_t y = ylo + q;
                 const int32_t yc = clampi(y - 1, 0, max(c.R.lY - 1, 0));
                 st.ev[q] = __ldg(reinterpret_cast<const float4 *>(A.events + c.R.event_base + yc));
+                if (c.hdp) st.mean[q] = __ldg(A.events_raw + c.R.event_base + yc).x;
             }
             __syncwarp();
         }
@@ -508,15 +555,16 @@ __global__ void __launch_bounds__(32 * kEmitWarps) emission_kernel(const __grid_
                 const bool ok = x >= 1 && x <= c.R.lX && y >= 1 && y <= c.R.lY;
                 float em, ey;
                 if (staged) {
-                    emit_cell(c, st.kc[x - xlo], st.kid[x - xlo], st.ev[y - ylo], ok, em, ey);
+                    emit_cell(c, st.kc[x - xlo], st.kid[x - xlo], st.ev[y - ylo], c.hdp ? st.mean[y - ylo] : 0.0, ok,
+                              em, ey);
                 } else {
                     const int32_t kid = ok ? __ldg(A.kmer + c.R.kmer_base + x - 1) : 0;
                     const float4 *kp = reinterpret_cast<const float4 *>(c.M->kc + kid);
                     const float4 ka = __ldg(kp), kb = __ldg(kp + 1);
                     const KmerConst32 kk{ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
-                    const float4 v = __ldg(reinterpret_cast<const float4 *>(
-                        A.events + c.R.event_base + clampi(y - 1, 0, max(c.R.lY - 1, 0))));
-                    emit_cell(c, kk, kid, v, ok, em, ey);
+                    const int32_t yc = clampi(y - 1, 0, max(c.R.lY - 1, 0));
+                    const float4 v = __ldg(reinterpret_cast<const float4 *>(A.events + c.R.event_base + yc));
+                    emit_cell(c, kk, kid, v, c.hdp ? __ldg(A.events_raw + c.R.event_base + yc).x : 0.0, ok, em, ey);
                 }
                 Ed[SE_M * W + i] = em;
                 Ed[SE_Y * W + i] = ey;

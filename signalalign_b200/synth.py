@@ -273,6 +273,66 @@ def config2(seed=2, n_reads=128, span=(5000, 15000), grid_length=2000):
     return dict(alphabet=alphabet, k=6, table=table, hdp=hdp, reads=reads)
 
 
+def _hdp_drawer(hdp):
+    def drawer(ev_kmer, rr):
+        w = hdp["weights"][ev_kmer]
+        u = rr.random(len(ev_kmer))[:, None]
+        comp = np.minimum((np.cumsum(w, axis=1) < u).sum(axis=1), 7)
+        return rr.normal(hdp["comp_means"][ev_kmer, comp], hdp["comp_sds"][ev_kmer, comp])
+    return drawer
+
+
+_COMPLEMENT = str.maketrans("ACGT", "TGCA")
+
+
+def config3(seed=3, n_reads=512, span=(1000, 30000), grid_length=2000):
+    """Methylation hypotheses with 2D reads: per read a template and a complement event stream (each
+    with its own scale/shift), CCWGG motifs placed about once per 256 bp and their second C
+    methylated (E) with probability 1/2 on each strand; every stream aligned under the all-C and
+    the all-E hypothesis (substituted references).  Half of the reads use the 6-mer ACEGT Gaussian
+    table, half the 6-mer ACEGT HDP tables.  Returns 4 alignments per read."""
+    alphabet, k = "ACEGT", 6
+    n = len(alphabet) ** k
+    r = _rng(seed)
+    gauss = gaussian_table(alphabet, k, seed + 100)
+    hdp = hdp_tables(alphabet, k, seed + 500, grid_length=grid_length)
+    htable = np.zeros((n, 5))
+    htable[:, 0], htable[:, 1] = hdp["mean"], hdp["sd"]
+    htable[:, 2] = r.uniform(0.5, 2.0, n)
+    htable[:, 3] = 0.3 * htable[:, 2]
+    htable[:, 4] = htable[:, 2] ** 3 / htable[:, 3] ** 2
+    drawer = _hdp_drawer(hdp)
+    motifs = ("CCAGG", "CCTGG")
+    alignments = []
+    for ri in range(n_reads):
+        L = int(r.integers(span[0], span[1] + 1))
+        seq = list(random_reference(L, r))
+        sites = []
+        for pos in range(int(r.integers(0, 256)), L - 5, 256):
+            seq[pos:pos + 5] = list(motifs[int(r.integers(0, 2))])
+            sites.append(pos + 1)
+        canon = "".join(seq)
+        use_hdp = ri % 2 == 1
+        table = htable if use_hdp else gauss
+        for strand in ("template", "complement"):
+            base = canon if strand == "template" else canon.translate(_COMPLEMENT)[::-1]
+            pos_s = sites if strand == "template" else [L - s - 3 for s in sites]
+            truth = list(base)
+            for q in pos_s:
+                if truth[q] == "C" and r.random() < 0.5:
+                    truth[q] = "E"
+            rd = make_read("".join(truth), alphabet, k, table[:, 0], table[:, 1], table[:, 2], table[:, 3], r,
+                           drawer=drawer if use_hdp else None)
+            for hyp in ("C", "E"):
+                ref = list(base)
+                for q in pos_s:
+                    if ref[q] == "C":
+                        ref[q] = hyp
+                alignments.append(dict(rd, reference="".join(ref), read=ri, strand=strand, hypothesis=hyp,
+                                       model="hdp" if use_hdp else "gauss"))
+    return dict(alphabet=alphabet, k=k, gauss_table=gauss, hdp_table=htable, hdp=hdp, alignments=alignments)
+
+
 def band_cells(xmyL, xmyR):
     """DP cells of a band: sum over anti-diagonals of the width."""
     return int(np.sum((np.asarray(xmyR) - np.asarray(xmyL)) // 2 + 1))

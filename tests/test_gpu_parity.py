@@ -228,3 +228,38 @@ def test_fp32_result_independent_of_batch(api, cfg0):
     alone = api.align_batch([mk(cfg["reads"][2])], p).pairs(0)
     mixed = api.align_batch([mk(rd) for rd in cfg["reads"]], p).pairs(2)
     assert np.array_equal(alone, mixed)
+
+
+def test_fp32_config2_shape_hdp(api):
+    """HDP machine with config 2's shape: 6-mer ACEGT (15,625 k-mers), 2000-point grid, methylated
+    CpGs in the reference; short reads so the oracle is quick"""
+    cfg = synth.config2(n_reads=2, span=(400, 700))
+    hdp = W.hdp_dict(cfg["hdp"], 5 ** 6)
+    m = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["table"]).split("\n")[:3])
+    err, llerr, _ = _batch_vs_oracle(api, m, orc.EMIT_HDP, cfg["reads"], _p(api), hdp=hdp)
+    assert err <= FP32_TOL, err
+    assert llerr <= 1e-3
+
+
+def test_fp32_config3_shape_mixed_models(api):
+    """config 3's shape: template and complement streams, all-C and all-E hypotheses, Gaussian and
+    HDP machines mixed in one batch; every alignment against the oracle"""
+    cfg = synth.config3(n_reads=2, span=(400, 700), grid_length=400)
+    gm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["gauss_table"]).split("\n")[:3])
+    hm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["hdp_table"]).split("\n")[:3])
+    hdp = W.hdp_dict(cfg["hdp"], 5 ** 6)
+    sm_g = W.gpu_model(api, gm, orc.EMIT_DESCALED)
+    sm_h = W.gpu_model(api, hm, orc.EMIT_HDP, None, hdp)
+    als = cfg["alignments"]
+    assert {a["hypothesis"] for a in als} == {"C", "E"} and {a["model"] for a in als} == {"gauss", "hdp"}
+    inputs = [api.ReadInput(sm=sm_h if a["model"] == "hdp" else sm_g, reference=a["reference"], events=a["events"],
+                            anchors=a["anchors"], scale=a["scale"], shift=a["shift"]) for a in als]
+    p = _p(api)
+    b = api.align_batch(inputs, p)
+    for i, a in enumerate(als):
+        assert b.status(i) == 0
+        om = W.oracle_model(hm if a["model"] == "hdp" else gm, orc.EMIT_HDP if a["model"] == "hdp" else orc.EMIT_DESCALED,
+                            a, hdp if a["model"] == "hdp" else None)
+        want = orc.aligned_pairs(om, a["reference"], a["events"], a["anchors"], _op(p), True, True)
+        assert len(want) > 50
+        assert W.max_posterior_error(want, b.pairs(i), p.threshold) <= FP32_TOL
