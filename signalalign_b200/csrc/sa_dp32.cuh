@@ -67,40 +67,5 @@ __device__ __forceinline__ void emit_gauss(const KmerConst32 &k, const Event32 &
     e_gapy = fmaf(-0.5f * ay, ay, k.k_y + common);
 }
 
-// HDP density on a uniform grid by cubic Hermite interpolation of the stored knots (density, slope)
-// with linear extrapolation outside (grid_spline_interp, hdp_math_utils.c:471-495), clamped at 0
-// (dir_proc_density, hdp.c:2600-2606), emitted as log(density / var) (stateMachine.c:492-494).
-struct Hdp32 {
-    const float2 *knots;      // rows x grid_length
-    const int32_t *kmer_row;  // n_kmers
-    float x0, dx, inv_dx, x_last;
-    int32_t grid_length, pad;
-};
-
-__device__ __forceinline__ float emit_hdp(const Hdp32 &h, const KmerConst32 &k, int32_t kid, const Event32 &ev,
-                                          const ReadScale32 &rs) {
-    const int32_t row = __ldg(h.kmer_row + kid);
-    if (row < 0) return kNegInf;
-    const float u = fmaf(ev.mean - fmaf(rs.scale, k.mu, rs.shift), rs.inv_var, k.mu);
-    const float2 *kn = h.knots + (int64_t) row * h.grid_length;
-    float dens;
-    if (u <= h.x0) {
-        const float2 a = __ldg(kn);
-        dens = a.x - a.y * (h.x0 - u);
-    } else if (u >= h.x_last) {
-        const float2 a = __ldg(kn + h.grid_length - 1);
-        dens = a.x + a.y * (u - h.x_last);
-    } else {
-        int32_t il = (int32_t) ((u - h.x0) * h.inv_dx);
-        il = max(0, min(il, h.grid_length - 2));
-        const float2 a = __ldg(kn + il), b = __ldg(kn + il + 1);
-        const float dy = b.x - a.x;
-        const float ca = a.y * h.dx - dy, cb = dy - b.y * h.dx;
-        const float tl = (u - fmaf((float) il, h.dx, h.x0)) * h.inv_dx, tr = 1.0f - tl;
-        dens = tr * a.x + tl * b.x + tl * tr * (ca * tr + cb * tl);
-    }
-    return dens > 0.0f ? __logf(dens) + rs.log_inv_var : kNegInf;
-}
-
 }  // namespace dp32
 }  // namespace sa

@@ -489,13 +489,6 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
         for (int j = 0; j < 9; ++j) m.t[j] = (float) sm->t[j];
         if (sm->emission == SA_EMIT_HDP) {
             const HdpTables &h = sm->hdp;
-            m.hdp.knots = sm->dev.hdp_knots32;
-            m.hdp.kmer_row = sm->dev.hdp_row32;
-            m.hdp.x0 = (float) h.grid[0];
-            m.hdp.dx = (float) (h.grid[1] - h.grid[0]);
-            m.hdp.inv_dx = (float) (1.0 / (h.grid[1] - h.grid[0]));
-            m.hdp.x_last = (float) h.grid[h.grid_length - 1];
-            m.hdp.grid_length = (int32_t) h.grid_length;
             m.hdp64.match = sm->dev.match;
             m.hdp64.grid = sm->dev.hdp_grid;
             m.hdp64.density = sm->dev.hdp_density;

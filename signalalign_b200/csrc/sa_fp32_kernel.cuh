@@ -75,7 +75,6 @@ struct Hdp64 {
 
 struct ModelDesc {
     const KmerConst32 *kc;
-    Hdp32 hdp;
     Hdp64 hdp64;
     int32_t emission;
     int32_t pad;

@@ -525,7 +525,7 @@ void free_device_model(sa_state_machine *sm) {
     cudaSetDevice(d.device);
     cudaFree(d.match); cudaFree(d.gapy); cudaFree(d.gapx);
     cudaFree(d.hdp_grid); cudaFree(d.hdp_density); cudaFree(d.hdp_slope); cudaFree(d.hdp_kmer_row);
-    cudaFree(d.kc32); cudaFree(d.gapx32); cudaFree(d.hdp_knots32); cudaFree(d.hdp_row32);
+    cudaFree(d.kc32); cudaFree(d.gapx32);
     int dev = d.device;
     d = DeviceModel();
     d.device = dev;
@@ -579,15 +579,6 @@ sa_status ensure_device_model(sa_state_machine *sm) {
         if (!st) st = upload(&d.hdp_density, h.density.data(), h.density.size());
         if (!st) st = upload(&d.hdp_slope, h.slope.data(), h.slope.size());
         if (!st) st = upload(&d.hdp_kmer_row, h.kmer_row.data(), h.kmer_row.size());
-        if (!st) {
-            std::vector<float2> knots(h.density.size());
-            for (size_t i = 0; i < knots.size(); ++i) knots[i] = make_float2((float) h.density[i], (float) h.slope[i]);
-            st = upload(&d.hdp_knots32, knots.data(), knots.size());
-        }
-        if (!st) {
-            std::vector<int32_t> row(h.kmer_row.begin(), h.kmer_row.end());
-            st = upload(&d.hdp_row32, row.data(), row.size());
-        }
     }
     cudaSetDevice(prev);
     if (st) {

@@ -50,8 +50,6 @@ struct DeviceModel {
     // FP32 tables
     KmerConst32 *kc32 = nullptr;
     float *gapx32 = nullptr;
-    float2 *hdp_knots32 = nullptr;   // n_rows x grid_length (density, slope)
-    int32_t *hdp_row32 = nullptr;
 };
 
 }  // namespace sa
