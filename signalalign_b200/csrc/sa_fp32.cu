@@ -54,6 +54,9 @@ __global__ void __launch_bounds__(256) fma_probe(float *sink, int iters, float s
 // region's last anti-diagonal stay inside the allocation.
 constexpr size_t kStoreSlack = 1024;
 
+// device memory bound of a batch's plain-form reads
+constexpr size_t kPlainBatchMaxBytes = (size_t) 64 << 30;
+
 }  // namespace fp32
 }  // namespace sa
 
@@ -137,8 +140,13 @@ struct sa_batch {
     // device timing of the last run's kernels (batches that own their device memory only)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timed = false;
+    // reads whose references have degenerate positions (multi-path cells) run in the plain FP64 form
+    std::vector<int64_t> plain_of;          // per read: its index in `plain`, or -1
+    std::vector<sa_read> plain_reads;
+    PlainSet *plain = nullptr;
 
     ~sa_batch() {
+        if (plain) plain_destroy(plain);
         for (cudaEvent_t &e : ev)
             if (e) cudaEventDestroy(e);
         mem_put(host_in);
@@ -233,6 +241,7 @@ int planning_threads() {
 // one read's plan before packing
 struct ReadPlan {
     sa_status status = SA_OK;
+    bool multi = false;         // degenerate positions: aligned by the plain form
     int32_t model = -1;
     int64_t lX = 0;
     std::vector<int32_t> kid;   // k-mer id per column 1..lX
@@ -299,7 +308,10 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         const sa_read &rd = reads[r];
         PathTable pt;
         sa_status st = build_paths(rd.sm, rd.reference, rp.lX, rd.degenerate, pt);
-        if (!st && pt.multi) st = SA_E_UNSUPPORTED;
+        if (!st && pt.multi) {
+            rp.multi = true;
+            return;
+        }
         if (!st)
             st = plan_regions(rd.anchors, rd.n_anchors, rp.lX, rd.n_events, *p, rd.ragged_left != 0,
                               rd.ragged_right != 0, rp.regs);
@@ -331,12 +343,18 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         b->read_n_regions[r] = (int64_t) rp.regs.size();
         nreg += (int64_t) rp.regs.size(); ndiag += rp.diags; ncell += rp.cells; nwin += rp.windows;
         nchunk += rp.chunks; nout += rp.out;
-        if (!rp.status) {
+        if (!rp.status && !rp.multi) {
             nkmer += rp.lX;
             nevent += reads[r].n_events;
         }
         b->max_width = std::max(b->max_width, rp.max_width);
     }
+    b->plain_of.assign(n_reads, -1);
+    for (int64_t r = 0; r < n_reads; ++r)
+        if (plan[r].multi && !plan[r].status) {
+            b->plain_of[r] = (int64_t) b->plain_reads.size();
+            b->plain_reads.push_back(reads[r]);
+        }
     if (b->max_width > kMaxCpt * kThreads) return SA_E_CAPACITY;
     b->device = device < 0 ? 0 : device;
     b->n_regions = nreg; b->n_diags = ndiag; b->n_windows = nwin; b->n_chunks = nchunk;
@@ -356,7 +374,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     // the packed inputs, read by read
     parallel_for(n_reads, threads, [&](int64_t r) {
         const ReadPlan &rp = plan[r];
-        if (rp.status) return;
+        if (rp.status || rp.multi) return;
         const sa_read &rd = reads[r];
         const sa_state_machine *sm = rd.sm;
         for (int64_t x = 0; x < rp.lX; ++x) {
@@ -462,6 +480,10 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
             if (!st) st = ensure_device_model(sm);
         cudaSetDevice(prev);
     }
+    if (!st && !b->plain_reads.empty()) {
+        st = plain_create(b->plain_reads.data(), (int64_t) b->plain_reads.size(), *p, kPlainBatchMaxBytes, &b->plain);
+        if (!st && plain_device(b->plain) != b->device) st = SA_E_ARG;
+    }
     if (!st) st = mem_get(MemKind::Device, b->device, b->dev_bytes, b->dev);
     if (!st) st = mem_get(MemKind::Pinned, b->device, b->res_bytes, b->host_res);
     if (st) {
@@ -507,6 +529,7 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
         count_launch();
         if (cudaGetLastError() != cudaSuccess) st = SA_E_CUDA;
     }
+    if (!st && b->plain) st = plain_upload(b->plain, s);
     cudaSetDevice(prev);
     b->downloaded = false;
     return st;
@@ -598,6 +621,7 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         count_launch(3);
         if (cudaGetLastError() != cudaSuccess) st = SA_E_CUDA;
     }
+    if (!st && b->plain) st = plain_run(b->plain, s);
     cudaSetDevice(prev);
     b->downloaded = false;
     return st;
@@ -631,9 +655,15 @@ sa_status sa_batch_download(sa_batch *b, void *stream) {
             cudaSuccess)
         st = SA_E_CUDA;
     if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = SA_E_CUDA;
+    if (!st && b->plain) st = plain_download(b->plain, s);
     b->read_ll.assign(b->n_reads, 0.0);
-    for (int64_t r = 0; r < b->n_reads && !st; ++r)
+    for (int64_t r = 0; r < b->n_reads && !st; ++r) {
+        if (b->plain_of[r] >= 0) {
+            b->read_ll[r] = plain_log_likelihood(b->plain, b->plain_of[r]);
+            continue;
+        }
         for (int64_t i = 0; i < b->read_n_regions[r]; ++i) b->read_ll[r] += b->loglik[b->read_first_region[r] + i];
+    }
     cudaSetDevice(prev);
     b->downloaded = st == SA_OK;
     return st;
@@ -651,18 +681,26 @@ sa_status sa_align_batch(const sa_read *reads, int64_t n_reads, const sa_params 
 sa_status sa_batch_read_status(const sa_batch *b, int64_t read) {
     if (!b || read < 0 || read >= b->n_reads) return SA_E_ARG;
     if (b->read_status[read]) return (sa_status) b->read_status[read];
+    if (!b->plain_of.empty() && b->plain_of[read] >= 0 && !b->plain) return SA_E_UNSUPPORTED;
     if (!b->downloaded) return SA_E_ARG;
+    if (!b->plain_of.empty() && b->plain_of[read] >= 0) return plain_read_status(b->plain, b->plain_of[read]);
     if (b->ctl[0].error) return SA_E_TIMEOUT;
     return (sa_status) b->dev_status[read];
 }
 
 int64_t sa_batch_pair_count(const sa_batch *b, int64_t read) {
     if (!b || read < 0 || read >= b->n_reads || !b->downloaded) return -1;
-    return b->read_status[read] ? 0 : b->read_count[read];
+    if (b->read_status[read]) return 0;
+    if (b->plain_of[read] >= 0) return b->plain ? (int64_t) plain_pairs(b->plain, b->plain_of[read]).size() : 0;
+    return b->read_count[read];
 }
 
 const sa_aligned_pair *sa_batch_pairs(const sa_batch *b, int64_t read) {
     if (!b || read < 0 || read >= b->n_reads || !b->downloaded) return nullptr;
+    if (!b->read_status[read] && b->plain_of[read] >= 0 && b->plain) {
+        const auto &v = plain_pairs(b->plain, b->plain_of[read]);
+        if (!v.empty()) return v.data();
+    }
     return static_cast<const sa_aligned_pair *>(b->host_pairs.ptr) + (b->read_status[read] ? 0 : b->read_base[read]);
 }
 
@@ -671,7 +709,7 @@ double sa_batch_log_likelihood(const sa_batch *b, int64_t read) {
     return b->read_ll[read];
 }
 
-int64_t sa_batch_cells(const sa_batch *b) { return b ? b->cells : 0; }
+int64_t sa_batch_cells(const sa_batch *b) { return b ? b->cells + (b->plain ? plain_cells(b->plain) : 0) : 0; }
 
 sa_status sa_batch_kernel_ms(const sa_batch *b, double *emission_ms, double *worker_ms, double *gather_ms) {
     if (!b || !emission_ms || !worker_ms || !gather_ms) return SA_E_ARG;

@@ -4,13 +4,22 @@
 // pairwiseAligner.c:1282-1420).  It is the parity anchor of the engine: results agree with
 // signalAlign's CPU code to rounding.  Compiled with -fmad=false.
 //
-// Device layout of a region (all global memory):
+// Plain sets: every region of every read of a set is one CTA of one launch.  Device layout of a
+// region (all global memory).  A matrix column x holds one path per k-mer its reference window can
+// spell (one, unless the window has 'X' positions: hdCell_construct, pairwiseAligner.c:605-650); a
+// band cell holds one slot of 3 states per path of its column.
 //   xl[d], xr[d]     band of anti-diagonal d (xmy range), d = 0..n
-//   coff[d]          index of anti-diagonal d's first cell (prefix sum of widths), n+2 entries
-//   kmer[x]          k-mer id of matrix column x (x = 0 is the empty prefix, id -1), lX+1 entries
+//   pfirst[x]        first path of column x (x = 0 is the empty prefix, one NULL path), lX+2 entries
+//   pid[q]           k-mer id of path q (-1 for NULL); ppre[q] = id / |alphabet|, psuf[q] =
+//                    id mod |alphabet|^(k-1): path q -> r is legal iff psuf[q] == ppre[r] (path_checkLegal)
 //   ev[y]            (mean, noise) of event y, lY entries
-//   F, B             3 doubles per cell (match, gap-X, gap-Y), forward and backward
+//   F, B             3 doubles per slot (match, gap-X, gap-Y), forward and backward, in rings of
+//                    `ring` anti-diagonals of `stride` slots: a traceback window [T, D] reads F and B
+//                    on T .. D only, and ring > D - T for every window (the reference also keeps only
+//                    the current window's forward diagonals, pairwiseAligner.c:1390-1410).  The
+//                    paths of one anti-diagonal are consecutive (x rises by one from cell to cell).
 //   P                refresh total probabilities, indexed by anti-diagonal
+//   out, tag         the set's pairs (shared, appended by atomics) and each pair's region
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -30,138 +39,192 @@ enum { T_MC = 0, T_MFGX, T_MFGY, T_OX, T_OY, T_EX, T_EY, T_SX, T_SY };
 struct Region64 {
     int32_t lX, lY, n, n_windows;
     int32_t ragged_left, ragged_right;
+    int32_t model, ring, stride, pad;
     const int32_t *xl, *xr;
-    const int64_t *coff;
-    const int32_t *kmer;
+    const int32_t *pfirst, *pid, *ppre, *psuf;
     const double2 *ev;
     const Window *win;
     double *F, *B, *P;
     double threshold;
-    sa_aligned_pair *out;
-    unsigned long long *out_count;
-    int64_t out_cap;
+    double *loglik;
     int32_t *status;
 };
 
-__device__ __forceinline__ double *cell(double *base, const Region64 &R, int32_t d, int32_t xmy) {
-    return base + 3 * (R.coff[d] + ((xmy - R.xl[d]) >> 1));
+struct SetOut {
+    sa_aligned_pair *out;
+    int32_t *tag;
+    unsigned long long *count;
+    int64_t cap;
+};
+
+// the 3 states of path q in the cell of anti-diagonal d (q must belong to that cell's column)
+__device__ __forceinline__ double *slot(double *base, const Region64 &R, int32_t d, int32_t q) {
+    return base + 3 * ((int64_t) (d % R.ring) * R.stride + (q - R.pfirst[(d + R.xl[d]) >> 1]));
 }
 
 __device__ __forceinline__ bool in_band(const Region64 &R, int32_t d, int32_t xmy) {
     return d >= 0 && d <= R.n && xmy >= R.xl[d] && xmy <= R.xr[d];
 }
 
+// path_checkLegal (pairwiseAligner.c:527-552): NULL on either side, or the (k-1)-suffix of q equal
+// to the (k-1)-prefix of r
+__device__ __forceinline__ bool legal(const Region64 &R, int32_t q, int32_t r) {
+    return R.pid[q] < 0 || R.pid[r] < 0 || R.psuf[q] == R.ppre[r];
+}
+
 // forward cell by pull: the reference's push order (lower -> gap-X, middle -> match, upper -> gap-Y,
-// stateMachine3_cellCalculate, stateMachine.c:1194-1257) with each state accumulated from LOG_ZERO
+// stateMachine3_cellCalculate, stateMachine.c:1194-1257) with each state accumulated from LOG_ZERO;
+// path r of the cell takes every legal path q of the neighbour in ascending order, the upper
+// neighbour (same column) only its own path
 __device__ void forward_cell(const Model64 &M, const Region64 &R, int32_t d, int32_t xmy) {
     const int32_t x = (d + xmy) >> 1, y = (d - xmy) >> 1;
-    const int32_t kid = R.kmer[x];
-    double vM = kNegInf, vX = kNegInf, vY = kNegInf;
-    if (in_band(R, d - 1, xmy - 1)) {
-        const double *l = cell(R.F, R, d - 1, xmy - 1);
-        double e = emit_gapx(M, kid);
-        vX = log_add(vX, l[S_M] + (e + M.t[T_OX]));
-        vX = log_add(vX, l[S_X] + (e + M.t[T_EX]));
-        vX = log_add(vX, l[S_Y] + (e + M.t[T_SX]));
+    const bool lo = in_band(R, d - 1, xmy - 1), mi = d >= 2 && in_band(R, d - 2, xmy), up = in_band(R, d - 1, xmy + 1);
+    const int32_t q0 = R.pfirst[x - (x > 0)], q1 = R.pfirst[x];
+    for (int32_t r = R.pfirst[x]; r < R.pfirst[x + 1]; ++r) {
+        const int32_t kid = R.pid[r];
+        double vM = kNegInf, vX = kNegInf, vY = kNegInf;
+        if (lo) {
+            const double e = emit_gapx(M, kid);
+            for (int32_t q = q0; q < q1; ++q) {
+                if (!legal(R, q, r)) continue;
+                const double *l = slot(R.F, R, d - 1, q);
+                vX = log_add(vX, l[S_M] + (e + M.t[T_OX]));
+                vX = log_add(vX, l[S_X] + (e + M.t[T_EX]));
+                vX = log_add(vX, l[S_Y] + (e + M.t[T_SX]));
+            }
+        }
+        if (mi) {
+            const double2 ev = R.ev[y - 1];
+            const double e = emit_event(M, kid, ev.x, ev.y, true);
+            for (int32_t q = q0; q < q1; ++q) {
+                if (!legal(R, q, r)) continue;
+                const double *m = slot(R.F, R, d - 2, q);
+                vM = log_add(vM, m[S_M] + (e + M.t[T_MC]));
+                vM = log_add(vM, m[S_X] + (e + M.t[T_MFGX]));
+                vM = log_add(vM, m[S_Y] + (e + M.t[T_MFGY]));
+            }
+        }
+        if (up) {
+            const double *u = slot(R.F, R, d - 1, r);
+            const double2 ev = R.ev[y - 1];
+            const double e = emit_event(M, kid, ev.x, ev.y, false);
+            vY = log_add(vY, u[S_M] + (e + M.t[T_OY]));
+            vY = log_add(vY, u[S_Y] + (e + M.t[T_EY]));
+        }
+        double *c = slot(R.F, R, d, r);
+        c[S_M] = vM;
+        c[S_X] = vX;
+        c[S_Y] = vY;
     }
-    if (d >= 2 && in_band(R, d - 2, xmy)) {
-        const double *m = cell(R.F, R, d - 2, xmy);
-        double2 ev = R.ev[y - 1];
-        double e = emit_event(M, kid, ev.x, ev.y, true);
-        vM = log_add(vM, m[S_M] + (e + M.t[T_MC]));
-        vM = log_add(vM, m[S_X] + (e + M.t[T_MFGX]));
-        vM = log_add(vM, m[S_Y] + (e + M.t[T_MFGY]));
-    }
-    if (in_band(R, d - 1, xmy + 1)) {
-        const double *u = cell(R.F, R, d - 1, xmy + 1);
-        double2 ev = R.ev[y - 1];
-        double e = emit_event(M, kid, ev.x, ev.y, false);
-        vY = log_add(vY, u[S_M] + (e + M.t[T_OY]));
-        vY = log_add(vY, u[S_Y] + (e + M.t[T_EY]));
-    }
-    double *c = cell(R.F, R, d, xmy);
-    c[S_M] = vM;
-    c[S_X] = vX;
-    c[S_Y] = vY;
 }
 
 // backward cell by pull.  The reference pushes from later cells into earlier ones
 // (doTransitionBackward, pairwiseAligner.c:715-720); a cell on anti-diagonal d receives, in time
 // order, the middle contribution of (x+1, y+1) on d+2, then the upper-role contribution of (x, y+1)
 // and the lower-role contribution of (x+1, y), both on d+1 (cells there are walked in ascending xmy).
+// Path r of the cell receives from every path p of the pushing cell that r may precede, in
+// ascending p, each with p's emission.
 __device__ void backward_cell(const Model64 &M, const Region64 &R, int32_t d, int32_t xmy, int32_t top) {
     const int32_t x = (d + xmy) >> 1, y = (d - xmy) >> 1;
-    double vM = kNegInf, vX = kNegInf, vY = kNegInf;
-    if (d + 2 <= top && in_band(R, d + 2, xmy)) {
-        const double *m = cell(R.B, R, d + 2, xmy);
-        double2 ev = R.ev[y];
-        double e = emit_event(M, R.kmer[x + 1], ev.x, ev.y, true);
-        vM = log_add(vM, m[S_M] + (e + M.t[T_MC]));
-        vX = log_add(vX, m[S_M] + (e + M.t[T_MFGX]));
-        vY = log_add(vY, m[S_M] + (e + M.t[T_MFGY]));
+    const bool mi = d + 2 <= top && in_band(R, d + 2, xmy), up = in_band(R, d + 1, xmy - 1),
+               lo = in_band(R, d + 1, xmy + 1);
+    // column x+1 exists whenever a cell of it is in the band
+    const int32_t p0 = (mi || lo) ? R.pfirst[x + 1] : 0, p1 = (mi || lo) ? R.pfirst[x + 2] : 0;
+    for (int32_t r = R.pfirst[x]; r < R.pfirst[x + 1]; ++r) {
+        double vM = kNegInf, vX = kNegInf, vY = kNegInf;
+        if (mi) {
+            const double2 ev = R.ev[y];
+            for (int32_t p = p0; p < p1; ++p) {
+                if (!legal(R, r, p)) continue;
+                const double *m = slot(R.B, R, d + 2, p);
+                const double e = emit_event(M, R.pid[p], ev.x, ev.y, true);
+                vM = log_add(vM, m[S_M] + (e + M.t[T_MC]));
+                vX = log_add(vX, m[S_M] + (e + M.t[T_MFGX]));
+                vY = log_add(vY, m[S_M] + (e + M.t[T_MFGY]));
+            }
+        }
+        if (up) {
+            const double *u = slot(R.B, R, d + 1, r);
+            const double2 ev = R.ev[y];
+            const double e = emit_event(M, R.pid[r], ev.x, ev.y, false);
+            vM = log_add(vM, u[S_Y] + (e + M.t[T_OY]));
+            vY = log_add(vY, u[S_Y] + (e + M.t[T_EY]));
+        }
+        if (lo) {
+            for (int32_t p = p0; p < p1; ++p) {
+                if (!legal(R, r, p)) continue;
+                const double *l = slot(R.B, R, d + 1, p);
+                const double e = emit_gapx(M, R.pid[p]);
+                vM = log_add(vM, l[S_X] + (e + M.t[T_OX]));
+                vX = log_add(vX, l[S_X] + (e + M.t[T_EX]));
+                vY = log_add(vY, l[S_X] + (e + M.t[T_SX]));
+            }
+        }
+        double *c = slot(R.B, R, d, r);
+        c[S_M] = vM;
+        c[S_X] = vX;
+        c[S_Y] = vY;
     }
-    if (in_band(R, d + 1, xmy - 1)) {
-        const double *u = cell(R.B, R, d + 1, xmy - 1);
-        double2 ev = R.ev[y];
-        double e = emit_event(M, R.kmer[x], ev.x, ev.y, false);
-        vM = log_add(vM, u[S_Y] + (e + M.t[T_OY]));
-        vY = log_add(vY, u[S_Y] + (e + M.t[T_EY]));
-    }
-    if (in_band(R, d + 1, xmy + 1)) {
-        const double *l = cell(R.B, R, d + 1, xmy + 1);
-        double e = emit_gapx(M, R.kmer[x + 1]);
-        vM = log_add(vM, l[S_X] + (e + M.t[T_OX]));
-        vX = log_add(vX, l[S_X] + (e + M.t[T_EX]));
-        vY = log_add(vY, l[S_X] + (e + M.t[T_SX]));
-    }
-    double *c = cell(R.B, R, d, xmy);
-    c[S_M] = vM;
-    c[S_X] = vX;
-    c[S_Y] = vY;
 }
 
 // diagonalCalculationTotalProbability (pairwiseAligner.c:1182-1200), sequential in the reference's
-// order: dot product of F and B on d in ascending xmy, then the matches that jump from d-1 over d
-// into d+1, dotted with B[d+1].
+// order: dot product of F and B on d in ascending xmy (a cell's paths folded first,
+// hdCell_totalProbability), then the matches that jump from d-1 over d into d+1, dotted with B[d+1].
 __device__ double total_probability(const Model64 &M, const Region64 &R, int32_t d, bool have_next) {
     double total = kNegInf;
     for (int32_t xmy = R.xl[d]; xmy <= R.xr[d]; xmy += 2) {
-        const double *f = cell(R.F, R, d, xmy), *b = cell(R.B, R, d, xmy);
-        double s = f[S_M] + b[S_M];
-        s = log_add(s, f[S_X] + b[S_X]);
-        s = log_add(s, f[S_Y] + b[S_Y]);
-        total = log_add(total, log_add(kNegInf, s));
+        const int32_t x = (d + xmy) >> 1;
+        double cell_total = kNegInf;
+        for (int32_t r = R.pfirst[x]; r < R.pfirst[x + 1]; ++r) {
+            const double *f = slot(R.F, R, d, r), *b = slot(R.B, R, d, r);
+            double s = f[S_M] + b[S_M];
+            s = log_add(s, f[S_X] + b[S_X]);
+            s = log_add(s, f[S_Y] + b[S_Y]);
+            cell_total = log_add(cell_total, s);
+        }
+        total = log_add(total, cell_total);
     }
     if (d >= 1 && have_next) {
         const int32_t dn = d + 1;
         double through = kNegInf;
         for (int32_t xmy = R.xl[dn]; xmy <= R.xr[dn]; xmy += 2) {
-            double m = kNegInf;
-            if (in_band(R, d - 1, xmy)) {
-                const int32_t x = (dn + xmy) >> 1, y = (dn - xmy) >> 1;
-                const double *f = cell(R.F, R, d - 1, xmy);
-                double2 ev = R.ev[y - 1];
-                double e = emit_event(M, R.kmer[x], ev.x, ev.y, true);
-                m = log_add(m, f[S_M] + (e + M.t[T_MC]));
-                m = log_add(m, f[S_X] + (e + M.t[T_MFGX]));
-                m = log_add(m, f[S_Y] + (e + M.t[T_MFGY]));
+            const int32_t x = (dn + xmy) >> 1, y = (dn - xmy) >> 1;
+            const bool mi = in_band(R, d - 1, xmy);
+            double cell_total = kNegInf;
+            for (int32_t r = R.pfirst[x]; r < R.pfirst[x + 1]; ++r) {
+                double m = kNegInf;
+                if (mi) {
+                    const double2 ev = R.ev[y - 1];
+                    const double e = emit_event(M, R.pid[r], ev.x, ev.y, true);
+                    for (int32_t q = R.pfirst[x - 1]; q < R.pfirst[x]; ++q) {
+                        if (!legal(R, q, r)) continue;
+                        const double *f = slot(R.F, R, d - 1, q);
+                        m = log_add(m, f[S_M] + (e + M.t[T_MC]));
+                        m = log_add(m, f[S_X] + (e + M.t[T_MFGX]));
+                        m = log_add(m, f[S_Y] + (e + M.t[T_MFGY]));
+                    }
+                }
+                const double *b = slot(R.B, R, dn, r);
+                double s = m + b[S_M];
+                s = log_add(s, kNegInf + b[S_X]);
+                s = log_add(s, kNegInf + b[S_Y]);
+                cell_total = log_add(cell_total, s);
             }
-            const double *b = cell(R.B, R, dn, xmy);
-            double s = m + b[S_M];
-            s = log_add(s, kNegInf + b[S_X]);
-            s = log_add(s, kNegInf + b[S_Y]);
-            through = log_add(through, log_add(kNegInf, s));
+            through = log_add(through, cell_total);
         }
         total = log_add(total, through);
     }
     return total;
 }
 
-__global__ void __launch_bounds__(128) region_kernel(Model64 M, Region64 R) {
+__global__ void __launch_bounds__(128) region_kernel(const Model64 *models, const Region64 *regions, SetOut O) {
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int32_t region = (int32_t) blockIdx.x;
+    const Region64 R = regions[region];
+    const Model64 M = models[R.model];
     // startStateProb / raggedStartStateProb (stateMachine.c:1022-1032) on anti-diagonal 0
     if (tid == 0) {
-        double *c = cell(R.F, R, 0, 0);
+        double *c = slot(R.F, R, 0, 0);
         c[S_M] = R.ragged_left ? kNegInf : 0.0;
         c[S_X] = R.ragged_left ? 0.0 : kNegInf;
         c[S_Y] = R.ragged_left ? 0.0 : kNegInf;
@@ -179,10 +242,13 @@ __global__ void __launch_bounds__(128) region_kernel(Model64 M, Region64 R) {
         const double e1 = ragged_end ? M.t[T_EX] : M.t[T_MFGX];
         const double e2 = ragged_end ? M.t[T_EY] : M.t[T_MFGY];
         for (int32_t xmy = R.xl[d] + 2 * tid; xmy <= R.xr[d]; xmy += 2 * nt) {
-            double *c = cell(R.B, R, d, xmy);
-            c[S_M] = e0;
-            c[S_X] = e1;
-            c[S_Y] = e2;
+            const int32_t x = (d + xmy) >> 1;
+            for (int32_t r = R.pfirst[x]; r < R.pfirst[x + 1]; ++r) {
+                double *c = slot(R.B, R, d, r);
+                c[S_M] = e0;
+                c[S_X] = e1;
+                c[S_Y] = e2;
+            }
         }
         __syncthreads();
         for (int32_t d2 = W.D - 1; d2 > W.T; --d2) {
@@ -202,20 +268,23 @@ __global__ void __launch_bounds__(128) region_kernel(Model64 M, Region64 R) {
             for (int32_t xmy = R.xl[d2] + 2 * tid; xmy <= R.xr[d2]; xmy += 2 * nt) {
                 const int32_t x = (d2 + xmy) >> 1, y = (d2 - xmy) >> 1;
                 if (!(x > 0 && y > 0)) continue;
-                const double *f = cell(R.F, R, d2, xmy), *b = cell(R.B, R, d2, xmy);
-                double p = exp((f[S_M] + b[S_M]) - total);
-                if (p >= R.threshold) {
-                    if (p > 1.0) p = 1.0;
-                    unsigned long long slot = atomicAdd(R.out_count, 1ULL);
-                    if ((int64_t) slot < R.out_cap) {
-                        sa_aligned_pair o;
-                        o.score = (int64_t) floor(p * 10000000.0);
-                        o.x = x - 1;
-                        o.y = y - 1;
-                        o.kmer = R.kmer[x];
-                        R.out[slot] = o;
-                    } else if (R.status) {
-                        atomicExch(R.status, (int32_t) SA_E_OUTPUT);
+                for (int32_t r = R.pfirst[x]; r < R.pfirst[x + 1]; ++r) {
+                    const double *f = slot(R.F, R, d2, r), *b = slot(R.B, R, d2, r);
+                    double p = exp((f[S_M] + b[S_M]) - total);
+                    if (p >= R.threshold) {
+                        if (p > 1.0) p = 1.0;
+                        unsigned long long o_at = atomicAdd(O.count, 1ULL);
+                        if ((int64_t) o_at < O.cap) {
+                            sa_aligned_pair o;
+                            o.score = (int64_t) floor(p * 10000000.0);
+                            o.x = x - 1;
+                            o.y = y - 1;
+                            o.kmer = R.pid[r];
+                            O.out[o_at] = o;
+                            O.tag[o_at] = region;
+                        } else {
+                            atomicExch(R.status, (int32_t) SA_E_OUTPUT);
+                        }
                     }
                 }
             }
@@ -224,33 +293,428 @@ __global__ void __launch_bounds__(128) region_kernel(Model64 M, Region64 R) {
         if (W.at_end) break;
         W = R.win[++wi];
     }
+    // the total probability of the last anti-diagonal is the region's log-likelihood
+    if (tid == 0) *R.loglik = R.P[R.n];
 }
 
-template <typename T>
-struct DevBuf {
-    T *p = nullptr;
-    ~DevBuf() { if (p) cudaFree(p); }
-    sa_status alloc(size_t n) {
-        if (n == 0) n = 1;
-        return cudaMalloc((void **) &p, n * sizeof(T)) == cudaSuccess ? SA_OK : SA_E_NOMEM;
-    }
-    sa_status put(const T *src, size_t n) {
-        sa_status st = alloc(n);
-        if (st) return st;
-        if (n && cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return SA_E_CUDA;
-        return SA_OK;
-    }
-};
+}  // namespace
 
-struct Emitted {
-    sa_aligned_pair pair;
-    int64_t key_window, key_diag, key_xmy;
+// ------------------------------------------------------------------------------------------------
+// plain sets: host side
+// ------------------------------------------------------------------------------------------------
+namespace {
+
+// host plan of one region: geometry (band, windows) and its paths
+struct PlainRegion {
+    int32_t read = 0, model = 0;
+    Region rg;
+    std::vector<int32_t> xl, xr, pfirst, pid, ppre, psuf;
+    int32_t ring = 3, stride = 1, max_paths = 1;
+    size_t ev_off = 0;   // first event of the region in the set's event array
 };
 
 }  // namespace
+
+struct PlainSet {
+    struct ReadModel {
+        sa_state_machine *sm;
+        double scale, shift, var;
+    };
+    int device = 0;
+    std::vector<ReadModel> models;   // one per read: the machine and the read's scaling
+    std::vector<int32_t> read_status;
+    std::vector<int64_t> read_first, read_count;   // regions of each read
+    std::vector<PlainRegion> regs;
+    std::vector<double2> events;
+    int64_t cells = 0, cap = 0;
+    double threshold = 0.01;
+    // device block: inputs (staged in `host_in` with the same layout), results, work
+    MemBlock host_in, host_res, dev;
+    size_t in_bytes = 0, res_off = 0, res_bytes = 0, dev_bytes = 0;
+    size_t res_status = 0, res_count = 0;   // offsets in the results block
+    Region64 *d_regions = nullptr;
+    Model64 *d_models = nullptr;
+    double *d_loglik = nullptr;
+    int32_t *d_status = nullptr;
+    unsigned long long *d_count = nullptr;
+    sa_aligned_pair *d_out = nullptr;
+    int32_t *d_tag = nullptr;
+    double *d_P = nullptr;
+    size_t p_bytes = 0;
+    // results
+    std::vector<std::vector<sa_aligned_pair>> pairs;
+    std::vector<double> ll;
+    std::vector<int32_t> status;
+
+    ~PlainSet() {
+        mem_put(host_in);
+        mem_put(host_res);
+        mem_put(dev);
+    }
+};
+
+namespace {
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t) 255; }
+
+// Places every buffer of the set; with non-null bases writes the staged inputs and the Region64 /
+// Model64 descriptors (device addresses).  Returns the device bytes.
+size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        at = align256(at);
+        const size_t o = at;
+        at += std::max<size_t>(bytes, 1);
+        return o;
+    };
+    const size_t nreg = s->regs.size();
+    const size_t o_regions = take(nreg * sizeof(Region64));
+    const size_t o_models = take(s->models.size() * sizeof(Model64));
+    std::vector<Region64> R(nreg);
+    struct Off { size_t xl, xr, pfirst, pid, ppre, psuf, win; };
+    std::vector<Off> off(nreg);
+    for (size_t i = 0; i < nreg; ++i) {
+        const PlainRegion &pr = s->regs[i];
+        off[i].xl = take(pr.xl.size() * sizeof(int32_t));
+        off[i].xr = take(pr.xr.size() * sizeof(int32_t));
+        off[i].pfirst = take(pr.pfirst.size() * sizeof(int32_t));
+        off[i].pid = take(pr.pid.size() * sizeof(int32_t));
+        off[i].ppre = take(pr.ppre.size() * sizeof(int32_t));
+        off[i].psuf = take(pr.psuf.size() * sizeof(int32_t));
+        off[i].win = take(pr.rg.windows.size() * sizeof(Window));
+    }
+    const size_t o_events = take(s->events.size() * sizeof(double2));
+    s->in_bytes = align256(at);
+    at = s->in_bytes;
+    s->res_off = at;
+    const size_t o_loglik = take(nreg * sizeof(double));
+    const size_t o_status = take(nreg * sizeof(int32_t));
+    const size_t o_count = take(sizeof(unsigned long long));
+    s->res_bytes = align256(at) - s->res_off;
+    s->res_status = o_status - s->res_off;
+    s->res_count = o_count - s->res_off;
+    at = s->res_off + s->res_bytes;
+    size_t p_total = 0;
+    for (const PlainRegion &pr : s->regs) p_total += (size_t) (pr.rg.lX + pr.rg.lY + 1);
+    const size_t o_P = take(p_total * sizeof(double));
+    s->p_bytes = p_total * sizeof(double);
+    std::vector<size_t> o_F(nreg), o_B(nreg);
+    for (size_t i = 0; i < nreg; ++i) {
+        const size_t ring_bytes = 3 * sizeof(double) * (size_t) s->regs[i].ring * (size_t) s->regs[i].stride;
+        o_F[i] = take(ring_bytes);
+        o_B[i] = take(ring_bytes);
+    }
+    const size_t o_out = take((size_t) s->cap * sizeof(sa_aligned_pair));
+    const size_t o_tag = take((size_t) s->cap * sizeof(int32_t));
+    s->dev_bytes = align256(at);
+    if (dev) {
+        s->d_regions = reinterpret_cast<Region64 *>(dev + o_regions);
+        s->d_models = reinterpret_cast<Model64 *>(dev + o_models);
+        s->d_loglik = reinterpret_cast<double *>(dev + o_loglik);
+        s->d_status = reinterpret_cast<int32_t *>(dev + o_status);
+        s->d_count = reinterpret_cast<unsigned long long *>(dev + o_count);
+        s->d_P = reinterpret_cast<double *>(dev + o_P);
+        s->d_out = reinterpret_cast<sa_aligned_pair *>(dev + o_out);
+        s->d_tag = reinterpret_cast<int32_t *>(dev + o_tag);
+    }
+    if (host && dev) {
+        size_t p_at = 0;
+        for (size_t i = 0; i < nreg; ++i) {
+            const PlainRegion &pr = s->regs[i];
+            auto put = [&](size_t o, const void *src, size_t bytes) {
+                if (bytes) std::memcpy(host + o, src, bytes);
+            };
+            put(off[i].xl, pr.xl.data(), pr.xl.size() * sizeof(int32_t));
+            put(off[i].xr, pr.xr.data(), pr.xr.size() * sizeof(int32_t));
+            put(off[i].pfirst, pr.pfirst.data(), pr.pfirst.size() * sizeof(int32_t));
+            put(off[i].pid, pr.pid.data(), pr.pid.size() * sizeof(int32_t));
+            put(off[i].ppre, pr.ppre.data(), pr.ppre.size() * sizeof(int32_t));
+            put(off[i].psuf, pr.psuf.data(), pr.psuf.size() * sizeof(int32_t));
+            put(off[i].win, pr.rg.windows.data(), pr.rg.windows.size() * sizeof(Window));
+            Region64 &r = R[i];
+            std::memset(&r, 0, sizeof(r));
+            r.lX = (int32_t) pr.rg.lX;
+            r.lY = (int32_t) pr.rg.lY;
+            r.n = (int32_t) (pr.rg.lX + pr.rg.lY);
+            r.n_windows = (int32_t) pr.rg.windows.size();
+            r.ragged_left = pr.rg.ragged_left;
+            r.ragged_right = pr.rg.ragged_right;
+            r.model = pr.model;
+            r.threshold = s->threshold;
+            r.ring = pr.ring;
+            r.stride = pr.stride;
+            r.xl = reinterpret_cast<const int32_t *>(dev + off[i].xl);
+            r.xr = reinterpret_cast<const int32_t *>(dev + off[i].xr);
+            r.pfirst = reinterpret_cast<const int32_t *>(dev + off[i].pfirst);
+            r.pid = reinterpret_cast<const int32_t *>(dev + off[i].pid);
+            r.ppre = reinterpret_cast<const int32_t *>(dev + off[i].ppre);
+            r.psuf = reinterpret_cast<const int32_t *>(dev + off[i].psuf);
+            r.ev = reinterpret_cast<const double2 *>(dev + o_events) + pr.ev_off;
+            r.win = reinterpret_cast<const Window *>(dev + off[i].win);
+            r.F = reinterpret_cast<double *>(dev + o_F[i]);
+            r.B = reinterpret_cast<double *>(dev + o_B[i]);
+            r.P = s->d_P + p_at;
+            p_at += (size_t) r.n + 1;
+            r.loglik = s->d_loglik + i;
+            r.status = s->d_status + i;
+        }
+        std::memcpy(host + o_regions, R.data(), nreg * sizeof(Region64));
+        for (size_t m = 0; m < s->models.size(); ++m) {
+            const sa_state_machine *sm = s->models[m].sm;
+            Model64 M;
+            std::memset(&M, 0, sizeof(M));
+            M.emission = sm->emission;
+            for (int i = 0; i < 9; ++i) M.t[i] = sm->t[i];
+            M.match = sm->dev.match;
+            M.gapy = sm->dev.gapy;
+            M.gapx = sm->dev.gapx;
+            M.scale = s->models[m].scale;
+            M.shift = s->models[m].shift;
+            M.var = s->models[m].var;
+            if (sm->emission == SA_EMIT_HDP) {
+                M.grid_length = sm->hdp.grid_length;
+                M.grid = sm->dev.hdp_grid;
+                M.density = sm->dev.hdp_density;
+                M.slope = sm->dev.hdp_slope;
+                M.kmer_row = sm->dev.hdp_kmer_row;
+            }
+            std::memcpy(host + o_models + m * sizeof(Model64), &M, sizeof(M));
+        }
+        if (!s->events.empty()) std::memcpy(host + o_events, s->events.data(), s->events.size() * sizeof(double2));
+    }
+    return s->dev_bytes;
+}
+
+}  // namespace
+
+namespace {
+
+// reference emission order of a region's pairs: window by window, anti-diagonals descending, xmy
+// ascending, a cell's paths in order (diagonalCalculationPosteriorMatchProbs, pairwiseAligner.c:1202-1253)
+struct Emitted {
+    sa_aligned_pair pair;
+    int64_t key_window, key_diag, key_xmy, key_path;
+};
+
+// Plans one region of the set: band, paths, ring geometry.
+void plan_region(const PathTable &pt, int32_t asz, int64_t kpow, PlainRegion &pr) {
+    const Region &rg = pr.rg;
+    const int32_t n = (int32_t) (rg.lX + rg.lY);
+    pr.xl.assign(rg.xmy_l.begin(), rg.xmy_l.end());
+    pr.xr.assign(rg.xmy_r.begin(), rg.xmy_r.end());
+    // column 0 is the NULL path, column x the reference column x1 + x
+    pr.pfirst.assign(rg.lX + 2, 0);
+    pr.pid.assign(1, -1);
+    for (int64_t x = 1; x <= rg.lX; ++x) {
+        pr.pfirst[x] = (int32_t) pr.pid.size();
+        for (int32_t q = pt.first[rg.x1 + x]; q < pt.first[rg.x1 + x + 1]; ++q) pr.pid.push_back(pt.ids[q]);
+    }
+    pr.pfirst[rg.lX + 1] = (int32_t) pr.pid.size();
+    pr.ppre.resize(pr.pid.size());
+    pr.psuf.resize(pr.pid.size());
+    for (size_t q = 0; q < pr.pid.size(); ++q) {
+        pr.ppre[q] = pr.pid[q] < 0 ? -1 : pr.pid[q] / asz;
+        pr.psuf[q] = pr.pid[q] < 0 ? -1 : (int32_t) (pr.pid[q] % kpow);
+    }
+    pr.stride = 1;
+    for (int32_t d = 0; d <= n; ++d) {
+        const int64_t x0 = (d + rg.xmy_l[d]) / 2, x1 = (d + rg.xmy_r[d]) / 2;
+        pr.stride = std::max<int32_t>(pr.stride, pr.pfirst[x1 + 1] - pr.pfirst[x0]);
+    }
+    pr.max_paths = 1;
+    for (int64_t x = 0; x <= rg.lX; ++x) pr.max_paths = std::max(pr.max_paths, pr.pfirst[x + 1] - pr.pfirst[x]);
+    int32_t span = 0;
+    for (const Window &w : rg.windows) span = std::max(span, w.D - w.T + 1);
+    pr.ring = std::max(3, span) + 1;
+}
+
+}  // namespace
+
+// Plans a set of reads for the plain form.  Reads that fail planning keep their status and get no
+// regions.  `max_bytes` bounds the device block (SA_E_CAPACITY above it).
+sa_status plain_create(const sa_read *reads, int64_t n_reads, const sa_params &p, size_t max_bytes, PlainSet **out) {
+    *out = nullptr;
+    auto *s = new (std::nothrow) PlainSet();
+    if (!s) return SA_E_NOMEM;
+    s->threshold = p.threshold;
+    s->read_status.assign(n_reads, SA_OK);
+    s->read_first.assign(n_reads, 0);
+    s->read_count.assign(n_reads, 0);
+    int device = -1;
+    int64_t cap = 0;
+    for (int64_t r = 0; r < n_reads; ++r) {
+        const sa_read &rd = reads[r];
+        auto *sm = const_cast<sa_state_machine *>(rd.sm);
+        s->models.push_back(PlainSet::ReadModel{sm, rd.scale, rd.shift, rd.var});
+        s->read_first[r] = (int64_t) s->regs.size();
+        sa_status st = SA_OK;
+        if (!sm || rd.reference_length < 0 || rd.n_events < 0 || rd.n_anchors < 0 ||
+            (rd.reference_length > 0 && !rd.reference) || (rd.n_events > 0 && !rd.events) ||
+            (rd.n_anchors > 0 && !rd.anchors))
+            st = SA_E_ARG;
+        if (!st && device >= 0 && sm->dev.device != device) st = SA_E_ARG;
+        if (!st && sm->emission == SA_EMIT_HDP && !sm->hdp.present) st = SA_E_UNSUPPORTED;
+        const int k = sm ? sm->kmer_length : 1;
+        // sequence_correctSeqLength (pairwiseAligner.c:456-471)
+        const int64_t lX = rd.reference_length == 0 ? 0 : rd.reference_length - (k - 1);
+        if (!st && lX < 0) st = SA_E_ARG;
+        PathTable pt;
+        std::vector<Region> regions;
+        if (!st) st = build_paths(sm, rd.reference, lX, rd.degenerate, pt);
+        if (!st)
+            st = plan_regions(rd.anchors, rd.n_anchors, lX, rd.n_events, p, rd.ragged_left != 0, rd.ragged_right != 0,
+                              regions);
+        if (st) {
+            s->read_status[r] = st;
+            continue;
+        }
+        if (device < 0) device = sm->dev.device;
+        // path_checkLegal on k-mer ids: the (k-1)-prefix of id is id / |alphabet|, the (k-1)-suffix
+        // id mod |alphabet|^(k-1)
+        const int32_t asz = (int32_t) sm->alphabet.size();
+        int64_t kpow = 1;
+        for (int i = 0; i < k - 1; ++i) kpow *= asz;
+        for (Region &rg : regions) {
+            PlainRegion pr;
+            pr.read = (int32_t) r;
+            pr.model = (int32_t) r;
+            pr.rg = std::move(rg);
+            plan_region(pt, asz, kpow, pr);
+            pr.ev_off = s->events.size();
+            for (int64_t y = 0; y < pr.rg.lY; ++y) {
+                const double *e = rd.events + (pr.rg.y1 + y) * kEventParams;
+                s->events.push_back(make_double2(e[0], e[1]));
+            }
+            const int64_t n = pr.rg.lX + pr.rg.lY;
+            cap += 4 * (n + 1) * std::min<int64_t>(pr.max_paths, 4) + 256;
+            for (int32_t d = 0; d <= n; ++d) {
+                const int64_t x0 = (d + pr.xl[d]) / 2, x1 = (d + pr.xr[d]) / 2;
+                s->cells += pr.pfirst[x1 + 1] - pr.pfirst[x0];
+            }
+            s->regs.push_back(std::move(pr));
+        }
+        s->read_count[r] = (int64_t) s->regs.size() - s->read_first[r];
+    }
+    s->device = device < 0 ? 0 : device;
+    s->cap = cap;
+    plain_layout(s, nullptr, nullptr);
+    if (s->dev_bytes > max_bytes) {
+        delete s;
+        return SA_E_CAPACITY;
+    }
+    *out = s;
+    return SA_OK;
+}
+
+// Device block, staged inputs and their upload (async on `stream`); models must be resident.
+sa_status plain_upload(PlainSet *s, cudaStream_t stream) {
+    sa_status st = mem_get(MemKind::Device, s->device, s->dev_bytes, s->dev);
+    if (!st) st = mem_get(MemKind::Pinned, s->device, s->in_bytes, s->host_in);
+    if (!st) st = mem_get(MemKind::Pinned, s->device, s->res_bytes, s->host_res);
+    if (st) return st;
+    plain_layout(s, static_cast<unsigned char *>(s->host_in.ptr), static_cast<unsigned char *>(s->dev.ptr));
+    if (cudaMemcpyAsync(s->dev.ptr, s->host_in.ptr, s->in_bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+        return SA_E_CUDA;
+    return SA_OK;
+}
+
+// One launch: every region one CTA.
+sa_status plain_run(PlainSet *s, cudaStream_t stream) {
+    auto *dev = static_cast<unsigned char *>(s->dev.ptr);
+    if (cudaMemsetAsync(dev + s->res_off, 0, s->res_bytes, stream) != cudaSuccess ||
+        cudaMemsetAsync(s->d_P, 0, std::max<size_t>(s->p_bytes, 1), stream) != cudaSuccess)
+        return SA_E_CUDA;
+    if (s->regs.empty()) return SA_OK;
+    SetOut O;
+    O.out = s->d_out;
+    O.tag = s->d_tag;
+    O.count = s->d_count;
+    O.cap = s->cap;
+    region_kernel<<<(unsigned) s->regs.size(), 128, 0, stream>>>(s->d_models, s->d_regions, O);
+    count_launch();
+    return cudaGetLastError() == cudaSuccess ? SA_OK : SA_E_CUDA;
+}
+
+// Results to the host (synchronises `stream`): per read its pairs in the reference's emission
+// order, coordinates shifted back from the regions (alignedPairCoordinateCorrectionFn,
+// pairwiseAligner.c:1763-1771), its status and log-likelihood.
+sa_status plain_download(PlainSet *s, cudaStream_t stream) {
+    if (cudaMemcpyAsync(s->host_res.ptr, static_cast<unsigned char *>(s->dev.ptr) + s->res_off, s->res_bytes,
+                        cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+        return SA_E_CUDA;
+    const auto *res = static_cast<const unsigned char *>(s->host_res.ptr);
+    const auto *loglik = reinterpret_cast<const double *>(res);
+    const auto *rstatus = reinterpret_cast<const int32_t *>(res + s->res_status);
+    const auto count = *reinterpret_cast<const unsigned long long *>(res + s->res_count);
+    const size_t npairs = (size_t) std::min<unsigned long long>(count, (unsigned long long) s->cap);
+    std::vector<sa_aligned_pair> got(npairs);
+    std::vector<int32_t> tag(npairs);
+    if (npairs &&
+        (cudaMemcpyAsync(got.data(), s->d_out, npairs * sizeof(sa_aligned_pair), cudaMemcpyDeviceToHost, stream) !=
+             cudaSuccess ||
+         cudaMemcpyAsync(tag.data(), s->d_tag, npairs * sizeof(int32_t), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+         cudaStreamSynchronize(stream) != cudaSuccess))
+        return SA_E_CUDA;
+    const int64_t n_reads = (int64_t) s->read_status.size();
+    std::vector<std::vector<Emitted>> per_read(n_reads);
+    for (size_t i = 0; i < npairs; ++i) {
+        const int32_t ri = tag[i];
+        const PlainRegion &pr = s->regs[ri];
+        const sa_aligned_pair &g = got[i];
+        Emitted e;
+        const int64_t d = g.x + g.y + 2, xmy = g.x - g.y;
+        int64_t w = 0;
+        while (w < (int64_t) pr.rg.windows.size() && d > pr.rg.windows[w].from) ++w;
+        int32_t r = pr.pfirst[g.x + 1];
+        while (r + 1 < pr.pfirst[g.x + 2] && pr.pid[r] != g.kmer) ++r;
+        e.key_window = ((int64_t) ri << 32) | w;
+        e.key_diag = -d;
+        e.key_xmy = xmy;
+        e.key_path = r;
+        e.pair = g;
+        e.pair.x += pr.rg.x1;
+        e.pair.y += pr.rg.y1;
+        per_read[pr.read].push_back(e);
+    }
+    s->pairs.assign(n_reads, {});
+    s->ll.assign(n_reads, 0.0);
+    s->status = s->read_status;
+    for (int64_t r = 0; r < n_reads; ++r) {
+        for (int64_t i = 0; i < s->read_count[r]; ++i) {
+            const int64_t ri = s->read_first[r] + i;
+            if (rstatus[ri] && !s->status[r]) s->status[r] = rstatus[ri];
+            s->ll[r] += loglik[ri];
+        }
+        if (count > (unsigned long long) s->cap && s->read_count[r] && !s->status[r]) s->status[r] = SA_E_OUTPUT;
+        auto &v = per_read[r];
+        std::sort(v.begin(), v.end(), [](const Emitted &a, const Emitted &b) {
+            if (a.key_window != b.key_window) return a.key_window < b.key_window;
+            if (a.key_diag != b.key_diag) return a.key_diag < b.key_diag;
+            if (a.key_xmy != b.key_xmy) return a.key_xmy < b.key_xmy;
+            return a.key_path < b.key_path;
+        });
+        s->pairs[r].resize(v.size());
+        for (size_t i = 0; i < v.size(); ++i) s->pairs[r][i] = v[i].pair;
+    }
+    return SA_OK;
+}
+
+int plain_device(const PlainSet *s) { return s->device; }
+int64_t plain_cells(const PlainSet *s) { return s->cells; }
+size_t plain_in_bytes(const PlainSet *s) { return s->in_bytes; }
+sa_status plain_read_status(const PlainSet *s, int64_t r) { return (sa_status) s->status[r]; }
+const std::vector<sa_aligned_pair> &plain_pairs(const PlainSet *s, int64_t r) { return s->pairs[r]; }
+double plain_log_likelihood(const PlainSet *s, int64_t r) { return s->ll[r]; }
+void plain_destroy(PlainSet *s) { delete s; }
+
 }  // namespace sa
 
 using namespace sa;
+
+// Device memory bound of one plain call (the forward and backward rings of a 20 kb read take tens
+// of MB; a pathological band of many-path cells is refused rather than allowed to take the GPU).
+static constexpr size_t kPlainMaxBytes = (size_t) 32 << 30;
 
 extern "C" sa_status sa_getAlignedPairsUsingAnchors(const sa_state_machine *sm_c, const char *reference,
                                                     int64_t reference_length, sa_degenerate degenerate,
@@ -266,133 +730,57 @@ extern "C" sa_status sa_getAlignedPairsUsingAnchors(const sa_state_machine *sm_c
     *pairs_out = nullptr;
     *n_pairs_out = 0;
     if (log_likelihood) *log_likelihood = 0.0;
+    sa_status st = check_params(*p);
+    if (st) return st;
     auto *sm = const_cast<sa_state_machine *>(sm_c);
-    const int k = sm->kmer_length;
-    // sequence_correctSeqLength (pairwiseAligner.c:456-471)
-    const int64_t lX = reference_length == 0 ? 0 : reference_length - (k - 1);
-    if (lX < 0) return SA_E_ARG;
-    const int64_t lY = n_events;
-    PathTable pt;
-    sa_status st = build_paths(sm, reference, lX, degenerate, pt);
+    sa_read rd;
+    std::memset(&rd, 0, sizeof(rd));
+    rd.sm = sm;
+    rd.reference = reference;
+    rd.reference_length = reference_length;
+    rd.events = events;
+    rd.n_events = n_events;
+    rd.anchors = anchors;
+    rd.n_anchors = n_anchors;
+    rd.scale = sm->scale;
+    rd.shift = sm->shift;
+    rd.var = sm->var;
+    rd.ragged_left = ragged_left;
+    rd.ragged_right = ragged_right;
+    rd.degenerate = degenerate;
+    PlainSet *s = nullptr;
+    st = plain_create(&rd, 1, *p, kPlainMaxBytes, &s);
     if (st) return st;
-    if (pt.multi) return SA_E_UNSUPPORTED;
-    std::vector<Region> regions;
-    st = plan_regions(anchors, n_anchors, lX, lY, *p, ragged_left != 0, ragged_right != 0, regions);
-    if (st) return st;
+    if (s->read_status[0]) {
+        st = (sa_status) s->read_status[0];
+        plain_destroy(s);
+        return st;
+    }
     st = ensure_device_model(sm);
-    if (st) return st;
     int prev_dev = 0;
-    if (cudaGetDevice(&prev_dev) != cudaSuccess) return SA_E_CUDA;
-    if (cudaSetDevice(sm->dev.device) != cudaSuccess) return SA_E_CUDA;
-
-    dp64::Model64 M;
-    std::memset(&M, 0, sizeof(M));
-    M.emission = sm->emission;
-    for (int i = 0; i < 9; ++i) M.t[i] = sm->t[i];
-    M.match = sm->dev.match;
-    M.gapy = sm->dev.gapy;
-    M.gapx = sm->dev.gapx;
-    M.scale = sm->scale;
-    M.shift = sm->shift;
-    M.var = sm->var;
-    if (sm->emission == SA_EMIT_HDP) {
-        if (!sm->hdp.present) { cudaSetDevice(prev_dev); return SA_E_UNSUPPORTED; }
-        M.grid_length = sm->hdp.grid_length;
-        M.grid = sm->dev.hdp_grid;
-        M.density = sm->dev.hdp_density;
-        M.slope = sm->dev.hdp_slope;
-        M.kmer_row = sm->dev.hdp_kmer_row;
+    if (!st && cudaGetDevice(&prev_dev) != cudaSuccess) st = SA_E_CUDA;
+    if (!st && cudaSetDevice(s->device) != cudaSuccess) st = SA_E_CUDA;
+    if (!st) {
+        st = plain_upload(s, nullptr);
+        if (!st) st = plain_run(s, nullptr);
+        if (!st) st = plain_download(s, nullptr);
+        if (!st) st = plain_read_status(s, 0);
+        cudaSetDevice(prev_dev);
     }
-
-    std::vector<Emitted> all;
-    double ll = 0.0;
-    for (size_t ri = 0; ri < regions.size() && st == SA_OK; ++ri) {
-        const Region &rg = regions[ri];
-        const int32_t n = (int32_t) (rg.lX + rg.lY);
-        std::vector<int64_t> coff(n + 2, 0);
-        for (int32_t d = 0; d <= n; ++d) coff[d + 1] = coff[d] + (rg.xmy_r[d] - rg.xmy_l[d]) / 2 + 1;
-        std::vector<int32_t> kmer(rg.lX + 1);
-        kmer[0] = -1;
-        for (int64_t x = 1; x <= rg.lX; ++x) kmer[x] = pt.ids[pt.first[rg.x1 + x]];
-        std::vector<double2> ev(rg.lY);
-        for (int64_t y = 0; y < rg.lY; ++y)
-            ev[y] = make_double2(events[(rg.y1 + y) * kEventParams], events[(rg.y1 + y) * kEventParams + 1]);
-        const int64_t cap = 8 * (int64_t) n + 1024;
-        DevBuf<int32_t> d_xl, d_xr, d_kmer, d_status;
-        DevBuf<int64_t> d_coff;
-        DevBuf<double2> d_ev;
-        DevBuf<Window> d_win;
-        DevBuf<double> d_F, d_B, d_P;
-        DevBuf<sa_aligned_pair> d_out;
-        DevBuf<unsigned long long> d_count;
-        if (!st) st = d_xl.put(rg.xmy_l.data(), rg.xmy_l.size());
-        if (!st) st = d_xr.put(rg.xmy_r.data(), rg.xmy_r.size());
-        if (!st) st = d_coff.put(coff.data(), coff.size());
-        if (!st) st = d_kmer.put(kmer.data(), kmer.size());
-        if (!st) st = d_ev.put(ev.data(), ev.size());
-        if (!st) st = d_win.put(rg.windows.data(), rg.windows.size());
-        if (!st) st = d_F.alloc(3 * (size_t) coff[n + 1]);
-        if (!st) st = d_B.alloc(3 * (size_t) coff[n + 1]);
-        if (!st) st = d_P.alloc(n + 1);
-        if (!st) st = d_out.alloc(cap);
-        if (!st) st = d_count.alloc(1);
-        if (!st) st = d_status.alloc(1);
-        if (st) break;
-        if (cudaMemset(d_count.p, 0, sizeof(unsigned long long)) != cudaSuccess ||
-            cudaMemset(d_status.p, 0, sizeof(int32_t)) != cudaSuccess) { st = SA_E_CUDA; break; }
-        Region64 R;
-        R.lX = (int32_t) rg.lX; R.lY = (int32_t) rg.lY; R.n = n; R.n_windows = (int32_t) rg.windows.size();
-        R.ragged_left = rg.ragged_left; R.ragged_right = rg.ragged_right;
-        R.xl = d_xl.p; R.xr = d_xr.p; R.coff = d_coff.p; R.kmer = d_kmer.p; R.ev = d_ev.p; R.win = d_win.p;
-        R.F = d_F.p; R.B = d_B.p; R.P = d_P.p;
-        R.threshold = p->threshold;
-        R.out = d_out.p; R.out_count = d_count.p; R.out_cap = cap; R.status = d_status.p;
-        region_kernel<<<1, 128>>>(M, R);
-        count_launch();
-        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) { st = SA_E_CUDA; break; }
-        unsigned long long cnt = 0;
-        int32_t kst = 0;
-        double top_p = 0.0;
-        if (cudaMemcpy(&cnt, d_count.p, sizeof(cnt), cudaMemcpyDeviceToHost) != cudaSuccess ||
-            cudaMemcpy(&kst, d_status.p, sizeof(kst), cudaMemcpyDeviceToHost) != cudaSuccess ||
-            cudaMemcpy(&top_p, d_P.p + n, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) {
-            st = SA_E_CUDA;
-            break;
-        }
-        if (kst) { st = (sa_status) kst; break; }
-        ll += top_p;
-        std::vector<sa_aligned_pair> got(cnt);
-        if (cnt && cudaMemcpy(got.data(), d_out.p, cnt * sizeof(sa_aligned_pair), cudaMemcpyDeviceToHost) != cudaSuccess) {
-            st = SA_E_CUDA;
-            break;
-        }
-        // reference emission order: window by window, anti-diagonals descending, xmy ascending
-        for (auto &g : got) {
-            Emitted e;
-            const int64_t d = g.x + g.y + 2, xmy = g.x - g.y;
-            int64_t w = 0;
-            while (w < (int64_t) rg.windows.size() && d > rg.windows[w].from) ++w;
-            e.key_window = ((int64_t) ri << 32) | w;
-            e.key_diag = -d;
-            e.key_xmy = xmy;
-            e.pair = g;
-            e.pair.x += rg.x1;
-            e.pair.y += rg.y1;
-            all.push_back(e);
-        }
+    if (st) {
+        plain_destroy(s);
+        return st;
     }
-    cudaSetDevice(prev_dev);
-    if (st) return st;
-    std::sort(all.begin(), all.end(), [](const Emitted &a, const Emitted &b) {
-        if (a.key_window != b.key_window) return a.key_window < b.key_window;
-        if (a.key_diag != b.key_diag) return a.key_diag < b.key_diag;
-        return a.key_xmy < b.key_xmy;
-    });
-    auto *outp = (sa_aligned_pair *) std::malloc(std::max<size_t>(1, all.size()) * sizeof(sa_aligned_pair));
-    if (!outp) return SA_E_NOMEM;
-    for (size_t i = 0; i < all.size(); ++i) outp[i] = all[i].pair;
+    const auto &v = plain_pairs(s, 0);
+    auto *outp = (sa_aligned_pair *) std::malloc(std::max<size_t>(1, v.size()) * sizeof(sa_aligned_pair));
+    if (!outp) {
+        plain_destroy(s);
+        return SA_E_NOMEM;
+    }
+    if (!v.empty()) std::memcpy(outp, v.data(), v.size() * sizeof(sa_aligned_pair));
     *pairs_out = outp;
-    *n_pairs_out = (int64_t) all.size();
-    if (log_likelihood) *log_likelihood = ll;
+    *n_pairs_out = (int64_t) v.size();
+    if (log_likelihood) *log_likelihood = plain_log_likelihood(s, 0);
+    plain_destroy(s);
     return SA_OK;
 }

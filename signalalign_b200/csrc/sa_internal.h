@@ -147,6 +147,22 @@ size_t batch_bind_scratch(sa_batch *b, unsigned char *base);
 // frees the host side only (the device area belongs to the caller)
 void batch_release_host(sa_batch *b);
 
+// the plain FP64 form over a set of reads (sa_fp64.cu): every region one CTA of one launch, F and
+// B in rings of the longest traceback window.  Used by the single-read entry and, inside batches,
+// for reads whose references have degenerate ('X') positions.
+struct PlainSet;
+sa_status plain_create(const sa_read *reads, int64_t n_reads, const sa_params &p, size_t max_bytes, PlainSet **out);
+sa_status plain_upload(PlainSet *s, cudaStream_t stream);
+sa_status plain_run(PlainSet *s, cudaStream_t stream);
+sa_status plain_download(PlainSet *s, cudaStream_t stream);
+int plain_device(const PlainSet *s);
+int64_t plain_cells(const PlainSet *s);
+size_t plain_in_bytes(const PlainSet *s);
+sa_status plain_read_status(const PlainSet *s, int64_t r);
+const std::vector<sa_aligned_pair> &plain_pairs(const PlainSet *s, int64_t r);
+double plain_log_likelihood(const PlainSet *s, int64_t r);
+void plain_destroy(PlainSet *s);
+
 #define SA_CUDA_TRY(expr)                                   \
     do {                                                    \
         cudaError_t _e = (expr);                            \

@@ -285,12 +285,16 @@ def _hdp_drawer(hdp):
 _COMPLEMENT = str.maketrans("ACGT", "TGCA")
 
 
-def config3(seed=3, n_reads=512, span=(1000, 30000), grid_length=2000):
+def config3(seed=3, n_reads=512, span=(1000, 30000), grid_length=2000, route="substitute"):
     """Methylation hypotheses with 2D reads: per read a template and a complement event stream (each
     with its own scale/shift), CCWGG motifs placed about once per 256 bp and their second C
-    methylated (E) with probability 1/2 on each strand; every stream aligned under the all-C and
-    the all-E hypothesis (substituted references).  Half of the reads use the 6-mer ACEGT Gaussian
-    table, half the 6-mer ACEGT HDP tables.  Returns 4 alignments per read."""
+    methylated (E) with probability 1/2 on each strand.  With route "substitute" every stream is
+    aligned under the all-C and the all-E hypothesis (substituted references, 4 alignments per
+    read); with route "degenerate" each stream is aligned once against a reference with 'X' at the
+    sites and degenerate type cytosine2 (C or E), so the cells over a site hold two paths (2
+    alignments per read, each with "degenerate": "CE").  Half of the reads use the 6-mer ACEGT
+    Gaussian table, half the 6-mer ACEGT HDP tables."""
+    assert route in ("substitute", "degenerate")
     alphabet, k = "ACEGT", 6
     n = len(alphabet) ** k
     r = _rng(seed)
@@ -323,13 +327,14 @@ def config3(seed=3, n_reads=512, span=(1000, 30000), grid_length=2000):
                     truth[q] = "E"
             rd = make_read("".join(truth), alphabet, k, table[:, 0], table[:, 1], table[:, 2], table[:, 3], r,
                            drawer=drawer if use_hdp else None)
-            for hyp in ("C", "E"):
+            for hyp in (("C", "E") if route == "substitute" else ("X",)):
                 ref = list(base)
                 for q in pos_s:
                     if ref[q] == "C":
                         ref[q] = hyp
+                extra = dict(degenerate="CE") if hyp == "X" else {}
                 alignments.append(dict(rd, reference="".join(ref), read=ri, strand=strand, hypothesis=hyp,
-                                       model="hdp" if use_hdp else "gauss"))
+                                       model="hdp" if use_hdp else "gauss", **extra))
     return dict(alphabet=alphabet, k=k, gauss_table=gauss, hdp_table=htable, hdp=hdp, alignments=alignments)
 
 

@@ -182,3 +182,32 @@ def test_status_strings(api):
     lib = api.lib()
     for s in range(12):
         assert lib.sa_status_string(s).decode() == api.STATUS[s]
+
+
+def test_batch_planning_with_degenerate_reads(api):
+    """Host planning of a batch that mixes reads with degenerate ('X') positions, which go to the
+    plain FP64 form, with ordinary reads: planning completes (on a host without a GPU the create
+    call then stops at the first pinned or device allocation, the no-allocation entry at the
+    models' device tables)."""
+    cfg = synth.config3(seed=5, n_reads=1, span=(300, 400), grid_length=50, route="degenerate")
+    sub = synth.config3(seed=5, n_reads=1, span=(300, 400), grid_length=50)["alignments"]
+    m = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["gauss_table"]).split("\n")[:3])
+    sm = api.StateMachine.from_tables("ACEGT", 6, m["t"], m["match"], m["gapy"], m["gapx"],
+                                      emission=api.EMIT_DESCALED)
+    als = cfg["alignments"] + sub
+    reads = [api.ReadInput(sm=sm, reference=a["reference"], events=a["events"], anchors=a["anchors"],
+                           scale=a["scale"], shift=a["shift"], degenerate=0) for a in als]
+    assert sum("X" in a["reference"] for a in als) == 2
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    try:
+        b = api.Batch(reads, p)
+    except api.SAError as e:
+        assert e.status in (4, 5), e   # pinned staging or device step: no device here
+    else:
+        assert b.cells > 0
+    # the no-allocation entry packs on the heap before it looks at the device: the packing runs here
+    # and the call stops at the models' device tables
+    try:
+        api.align_batch_noalloc(reads, p)
+    except api.SAError as e:
+        assert e.status in (1, 4, 5), e

@@ -51,11 +51,16 @@ def _op(p):
                       traceback=p.traceback_diagonals, split=p.split_matrix_bigger_than_this)
 
 
-def _fp64_case(api, m, emission, rd, p, ragged=(True, True), hdp=None):
+DEGENERATE = {"CE": 0, "CEO": 1, "AI": 2}   # sa_degenerate codes of the options strings
+
+
+def _fp64_case(api, m, emission, rd, p, ragged=(True, True), hdp=None, options="CEO"):
     om = W.oracle_model(m, emission, rd, hdp)
     sm = W.gpu_model(api, m, emission, rd, hdp)
-    want = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], _op(p), ragged[0], ragged[1])
-    got = api.getAlignedPairsUsingAnchors(sm, rd["reference"], rd["events"], rd["anchors"], p, ragged[0], ragged[1])
+    want = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], _op(p), ragged[0], ragged[1],
+                             options=options)
+    got = api.getAlignedPairsUsingAnchors(sm, rd["reference"], rd["events"], rd["anchors"], p, ragged[0], ragged[1],
+                                          degenerate=DEGENERATE[options])
     return want, got
 
 
@@ -128,6 +133,58 @@ def test_fp64_hdp_small(api):
         want, got = _fp64_case(api, m, orc.EMIT_HDP, rd, p, hdp=hdp)
         assert len(want) > 50
         _assert_fp64(want, got, p.threshold)
+
+
+def test_fp64_multipath_toy6(api):
+    """Variable-order cells (hdCell_construct, pairwiseAligner.c:605-650): the toy 6-mer case of
+    test_sm3_diagonalDPCalculations (stateMachineTests.c:443-560), reference "ACGATAXGGACAT" with
+    X -> C/E/O, so the six columns over the X hold three paths each.  The banded routine with no
+    anchors gives the golden 14 pairs, each (x, y) in the expected set, identical to the oracle."""
+    from golden_models import load_fixture, model_from_fixture
+    fx = load_fixture("toy6")
+    m = model_from_fixture(fx)
+    rd = dict(reference=fx["sequence"], events=np.array(fx["events"]), anchors=np.zeros((0, 2), np.int64),
+              scale=1.0, shift=0.0)
+    p = _p(api, expansion=2, threshold=fx["threshold"])
+    want, got = _fp64_case(api, m, orc.EMIT_PLAIN, rd, p, ragged=(False, False), options="CEO")
+    assert len(got) == fx["expected_pairs"]
+    allowed = {tuple(a) for a in fx["allowed"]}
+    assert all((int(q["x"]), int(q["y"])) in allowed for q in got)
+    assert len({int(q["kmer"]) for q in got if (int(q["x"]), int(q["y"])) == (6, 5)}) == 3
+    _assert_fp64(want, got, p.threshold)
+
+
+@pytest.mark.parametrize("model", ["gauss", "hdp"])
+def test_fp64_multipath_methylation_sites(api, model):
+    """Methylation calling with degenerate positions (cytosine2: X -> C or E) at CCWGG sites on both
+    strands, Gaussian and HDP machines: the cells over a site hold two paths and each emits its
+    own posterior; FP64 GPU against the oracle."""
+    cfg = synth.config3(seed=11, n_reads=2, span=(700, 1400), grid_length=200, route="degenerate")
+    alphabet, k = cfg["alphabet"], cfg["k"]
+    n = len(alphabet) ** k
+    p = _p(api)
+    site_bases = {"C": 0, "E": 0}
+    for rd in cfg["alignments"]:
+        if rd["model"] != model:
+            continue
+        assert "X" in rd["reference"] and rd["degenerate"] == "CE"
+        table = cfg["hdp_table"] if model == "hdp" else cfg["gauss_table"]
+        text = synth.model_text(cfg["alphabet"], cfg["k"], table)
+        m = formats.parse_model_lines(*text.split("\n")[:3])
+        hdp = W.hdp_dict(cfg["hdp"], n) if model == "hdp" else None
+        emission = orc.EMIT_HDP if model == "hdp" else orc.EMIT_DESCALED
+        want, got = _fp64_case(api, m, emission, rd, p, hdp=hdp, options="CE")
+        assert len(want) > 50
+        _assert_fp64(want, got, p.threshold)
+        # the path each pair over a site took: the site's base in the pair's k-mer
+        sites = [i for i, ch in enumerate(rd["reference"]) if ch == "X"]
+        for q in got:
+            x, kid = int(q["x"]), int(q["kmer"])
+            kmer = "".join(alphabet[(kid // len(alphabet) ** (k - 1 - i)) % len(alphabet)] for i in range(k))
+            for s_ in sites:
+                if x <= s_ < x + k:
+                    site_bases[kmer[s_ - x]] += 1
+    assert site_bases["C"] > 0 and site_bases["E"] > 0
 
 
 def test_fp64_edge_cases(api, cfg0):
@@ -263,3 +320,42 @@ def test_fp32_config3_shape_mixed_models(api):
         want = orc.aligned_pairs(om, a["reference"], a["events"], a["anchors"], _op(p), True, True)
         assert len(want) > 50
         assert W.max_posterior_error(want, b.pairs(i), p.threshold) <= FP32_TOL
+
+
+def test_batch_degenerate_reads_run_in_plain_form(api):
+    """Reads with degenerate positions (route (ii) of methylation calling: 'X' at the CCWGG sites,
+    cytosine2) in one batch with substituted-reference reads: the multi-path reads are aligned by
+    the plain FP64 form inside the batch (FP64 tolerance against the oracle, and identical to the
+    single-read entry), the others by the FP32 kernels (FP32 tolerance)."""
+    sub = synth.config3(seed=5, n_reads=1, span=(500, 800), grid_length=300)["alignments"]
+    deg_cfg = synth.config3(seed=5, n_reads=2, span=(500, 800), grid_length=300, route="degenerate")
+    deg = deg_cfg["alignments"]
+    gm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, deg_cfg["gauss_table"]).split("\n")[:3])
+    hm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, deg_cfg["hdp_table"]).split("\n")[:3])
+    hdp = W.hdp_dict(deg_cfg["hdp"], 5 ** 6)
+    sm_g = W.gpu_model(api, gm, orc.EMIT_DESCALED)
+    sm_h = W.gpu_model(api, hm, orc.EMIT_HDP, None, hdp)
+    als = [a for pair in zip(deg, sub) for a in pair]   # interleaved
+    inputs = [api.ReadInput(sm=sm_h if a["model"] == "hdp" else sm_g, reference=a["reference"], events=a["events"],
+                            anchors=a["anchors"], scale=a["scale"], shift=a["shift"],
+                            degenerate=DEGENERATE[a.get("degenerate", "CEO")]) for a in als]
+    p = _p(api)
+    b = api.align_batch(inputs, p)
+    n_multi = 0
+    for i, a in enumerate(als):
+        assert b.status(i) == 0
+        hd = a["model"] == "hdp"
+        om = W.oracle_model(hm if hd else gm, orc.EMIT_HDP if hd else orc.EMIT_DESCALED, a, hdp if hd else None)
+        options = a.get("degenerate", "CEO")
+        want = orc.aligned_pairs(om, a["reference"], a["events"], a["anchors"], _op(p), True, True, options=options)
+        assert len(want) > 50
+        if "X" in a["reference"]:
+            n_multi += 1
+            _assert_fp64(want, b.pairs(i), p.threshold)
+            sm = W.gpu_model(api, hm if hd else gm, orc.EMIT_HDP if hd else orc.EMIT_DESCALED, a, hdp if hd else None)
+            alone = api.getAlignedPairsUsingAnchors(sm, a["reference"], a["events"], a["anchors"], p,
+                                                    degenerate=DEGENERATE[options])
+            assert np.array_equal(alone, b.pairs(i))
+        else:
+            assert W.max_posterior_error(want, b.pairs(i), p.threshold) <= FP32_TOL
+    assert n_multi == len(deg)
