@@ -604,6 +604,8 @@ struct ForwardSweep {
     float lm_prev;
     float delta0, delta1;         // delta(d) = base(d) - base(d-1), delta(d-1)
     double base0;                 // base(d)
+    double qbase;                 // lane q of warp 0: base and shift of the last anti-diagonal d
+    float qshift;                 // with d mod 32 == q
     int32_t wi;
 
     __device__ __forceinline__ ForwardSweep(const Ctx &cc, Shared *s, float *r)
@@ -706,11 +708,20 @@ struct ForwardSweep {
             const float wm = warp_max1(lm_prev);
             if (lane == 0) sh->part[S1][warp] = wm;
         }
-        if (tid == 0) {
-            A.base[db + d] = base0;
-            A.fshift[db + d] = delta0;
-        }
+        // base and shift of d: lane d mod 32 of warp 0 keeps them, and the warp writes them out 32
+        // at a time and before a window is published (its backward sweep reads them)
         const bool window_end = (m0.flags & kFlagWindowEnd) != 0;
+        if (warp == 0) {
+            const int q = d & 31;
+            if (lane == q) {
+                qbase = base0;
+                qshift = delta0;
+            }
+            if ((q == 31 || window_end || d == n) && lane <= q) {
+                A.base[db + (d - q) + lane] = qbase;
+                A.fshift[db + (d - q) + lane] = qshift;
+            }
+        }
         if (window_end) __threadfence();   // this anti-diagonal and all before it, device-wide
         __syncthreads();
         if (window_end && tid == 0) {
@@ -721,7 +732,7 @@ struct ForwardSweep {
         lm_prev = lm;
         delta1 = delta0;
         delta0 = delta_next;
-        base0 += (double) delta_next;   // only thread 0 stores it
+        base0 += (double) delta_next;   // only warp 0 stores it
         Fd += 3 * W0;
         m2 = m1;
         m1 = m0;
@@ -778,6 +789,8 @@ struct ForwardSweep {
         // path.  delta(d) = base(d) - base(d-1) is a float and base(d) = base(d-1) + delta(d).
         delta0 = delta1 = 0.0f;
         base0 = 0.0;
+        qbase = 0.0;   // anti-diagonal 0 (lane 0 of the first block): base 0, shift 0
+        qshift = 0.0f;
         wi = 0;
         __syncthreads();
         for (int32_t d = 1; d <= n; d += 3) {
