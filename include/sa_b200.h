@@ -285,6 +285,92 @@ sa_status sa_server_release(sa_server *s, int64_t ticket);
 /* finishes the queued reads, then stops the dispatcher */
 void sa_server_destroy(sa_server *s);
 
+/* ---- before the path: anchor pairs from the guide alignment (signalMachine.c:615, :343-344) ---- */
+
+/* one cigar operation of the guide alignment (AlignmentOperation of sonLib's PairwiseAlignment) */
+typedef enum {
+    SA_CIGAR_MATCH = 0,      /* PAIRWISE_MATCH: advances both sequences */
+    SA_CIGAR_INDEL_X = 1,    /* PAIRWISE_INDEL_X: advances sequence 1 (the reference) only */
+    SA_CIGAR_INDEL_Y = 2     /* PAIRWISE_INDEL_Y: advances sequence 2 (the read) only */
+} sa_cigar_op_type;
+
+typedef struct {
+    int32_t op;              /* sa_cigar_op_type */
+    int32_t pad;
+    int64_t length;
+} sa_cigar_op;
+
+/* coordinates of a guide alignment (sonLib PairwiseAlignment: sequence 1 = reference, 2 = read) */
+typedef struct {
+    int64_t start1, end1;
+    int32_t strand1;         /* 1 forward, 0 reverse (then start1 >= end1) */
+    int32_t pad1;
+    int64_t start2, end2;
+    int32_t strand2;         /* must be 1 */
+    int32_t pad2;
+} sa_guide_alignment;
+
+/* filterToRemoveOverlap (pairwiseAligner.c:1575-1616): from pairs sorted by (x, y), the ones that are
+ * strictly increasing in both coordinates against every other pair kept.  out may alias pairs;
+ * SA_E_ANCHORS if the input is not sorted. */
+sa_status sa_filterToRemoveOverlap(const int64_t *pairs, int64_t n_pairs, int64_t *out, int64_t *n_out);
+
+/* signalUtils_guideAlignmentToRebasedAnchorPairs (signalMachineUtils.c:142-164): rebases the
+ * reference coordinates of *ga to 0 (flipping a reverse strand, as the reference does in place),
+ * converts the cigar's match runs, less `trim` at both ends of each, into pairs
+ * (convertPairwiseForwardStrandAlignmentToAnchorPairs, pairwiseAligner.c:1454-1478), sorts them and
+ * filters overlaps.  out holds up to `capacity` pairs (SA_E_OUTPUT beyond, with *n_out the count
+ * needed); SA_E_ARG if the cigar does not span the alignment's coordinates. */
+sa_status sa_guideAlignmentToRebasedAnchorPairs(sa_guide_alignment *ga, const sa_cigar_op *ops, int64_t n_ops,
+                                                int64_t trim, int64_t *out, int64_t capacity, int64_t *n_out);
+
+/* signalUtils_getRemappedAnchorPairs (signalMachineUtils.c:166-170): (x, y) -> (x, event_map[y] -
+ * event_map[map_offset]) (nanopore_remapAnchorPairsWithOffset, nanopore.c:438-450), then overlaps
+ * filtered.  SA_E_ARG for an index outside event_map. */
+sa_status sa_getRemappedAnchorPairs(const int64_t *anchors, int64_t n_anchors, const int64_t *event_map,
+                                    int64_t map_length, int64_t map_offset, int64_t *out, int64_t *n_out);
+
+/* ---- after the path: ordering, score and the posterior files (signalMachine.c:68-260, :715-728) ---- */
+
+/* stList_sort(alignedPairs, sortByXPlusYCoordinate2) (pairwiseAligner.c:1434-1438): ascending x + y.
+ * The reference sorts with qsort, which leaves the order of equal keys unspecified; this sort keeps
+ * their input order. */
+void sa_sortByXPlusYCoordinate(sa_aligned_pair *pairs, int64_t n_pairs);
+
+/* scoreByPosteriorProbabilityIgnoringGaps (signalMachine.c:317-331): 100 x mean posterior */
+double sa_scoreByPosteriorProbabilityIgnoringGaps(const sa_aligned_pair *pairs, int64_t n_pairs);
+
+typedef enum {
+    SA_OUTPUT_FULL = 0,             /* writePosteriorProbsFull */
+    SA_OUTPUT_VARIANT_CALLER = 1,   /* writePosteriorProbsVC */
+    SA_OUTPUT_ASSIGNMENTS = 2       /* writeAssignments */
+} sa_output_format;
+
+/* what outputAlignment needs besides the pairs and the model */
+typedef struct {
+    const char *read_label;
+    const char *contig;
+    const char *target;           /* the reference sequence the read was aligned to ('X' at degenerate sites) */
+    int64_t target_length;
+    int32_t strand;               /* 0 template, 1 complement */
+    int32_t forward;              /* the guide alignment's strand */
+    int64_t event_offset;         /* added to a pair's event index (the read's event map at the alignment start) */
+    int64_t reference_offset;     /* the reference coordinate shift */
+    const double *events;         /* the strand's whole event table, 4 doubles per event (mean, noise, duration, start) */
+    int64_t n_events;
+    double scale, shift, var, scale_sd;   /* NanoporeReadAdjustmentParameters */
+} sa_output_read;
+
+/* outputAlignment (signalMachine.c:240-260): the lines the reference appends to its posterior file,
+ * byte for byte (printf formats of the reference), into a malloc'd NUL-terminated buffer (release with
+ * sa_free_text).  Model means and noise come from sm's match table. */
+sa_status sa_formatAlignment(sa_output_format fmt, const sa_state_machine *sm, const sa_output_read *rd,
+                             const sa_aligned_pair *pairs, int64_t n_pairs, char **text, int64_t *length);
+/* the same lines appended to the file at `path` */
+sa_status sa_outputAlignment(sa_output_format fmt, const char *path, const sa_state_machine *sm,
+                             const sa_output_read *rd, const sa_aligned_pair *pairs, int64_t n_pairs);
+void sa_free_text(char *text);
+
 /* ---- diagnostics ---- */
 const char *sa_status_string(sa_status s);
 /* number of kernel launches this process has made through the library (all entry points) */

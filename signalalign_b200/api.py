@@ -56,6 +56,26 @@ class Read(C.Structure):
 
 
 _lib = None
+class CigarOp(C.Structure):
+    _fields_ = [("op", C.c_int32), ("pad", C.c_int32), ("length", C.c_int64)]
+
+
+class GuideAlignment(C.Structure):
+    _fields_ = [("start1", C.c_int64), ("end1", C.c_int64), ("strand1", C.c_int32), ("pad1", C.c_int32),
+                ("start2", C.c_int64), ("end2", C.c_int64), ("strand2", C.c_int32), ("pad2", C.c_int32)]
+
+
+class OutputRead(C.Structure):
+    _fields_ = [("read_label", C.c_char_p), ("contig", C.c_char_p), ("target", C.c_char_p), ("target_length", C.c_int64),
+                ("strand", C.c_int32), ("forward", C.c_int32), ("event_offset", C.c_int64),
+                ("reference_offset", C.c_int64), ("events", C.POINTER(C.c_double)), ("n_events", C.c_int64),
+                ("scale", C.c_double), ("shift", C.c_double), ("var", C.c_double), ("scale_sd", C.c_double)]
+
+
+CIGAR_MATCH, CIGAR_INDEL_X, CIGAR_INDEL_Y = 0, 1, 2
+OUTPUT_FULL, OUTPUT_VARIANT_CALLER, OUTPUT_ASSIGNMENTS = 0, 1, 2
+TEMPLATE, COMPLEMENT = 0, 1
+
 _i64p = C.POINTER(C.c_int64)
 _f64p = C.POINTER(C.c_double)
 
@@ -109,6 +129,17 @@ def _bind(L):
                                        _f64p, _f64p]),
         "sa_server_release": (C.c_int, [vp, C.c_int64]),
         "sa_server_destroy": (None, [vp]),
+        "sa_filterToRemoveOverlap": (C.c_int, [_i64p, C.c_int64, _i64p, _i64p]),
+        "sa_guideAlignmentToRebasedAnchorPairs": (C.c_int, [C.POINTER(GuideAlignment), C.POINTER(CigarOp), C.c_int64,
+                                                            C.c_int64, _i64p, C.c_int64, _i64p]),
+        "sa_getRemappedAnchorPairs": (C.c_int, [_i64p, C.c_int64, _i64p, C.c_int64, C.c_int64, _i64p, _i64p]),
+        "sa_sortByXPlusYCoordinate": (None, [C.POINTER(AlignedPair), C.c_int64]),
+        "sa_scoreByPosteriorProbabilityIgnoringGaps": (C.c_double, [C.POINTER(AlignedPair), C.c_int64]),
+        "sa_formatAlignment": (C.c_int, [C.c_int, vp, C.POINTER(OutputRead), C.POINTER(AlignedPair), C.c_int64,
+                                         C.POINTER(C.c_void_p), _i64p]),
+        "sa_outputAlignment": (C.c_int, [C.c_int, C.c_char_p, vp, C.POINTER(OutputRead), C.POINTER(AlignedPair),
+                                         C.c_int64]),
+        "sa_free_text": (None, [C.c_void_p]),
         "sa_status_string": (C.c_char_p, [C.c_int]),
         "sa_kernel_launch_count": (C.c_int64, []),
         "sa_measure_fp32_peak": (C.c_int, [C.c_int32, _f64p]),
@@ -516,3 +547,102 @@ def measure_fp32_peak(device=0):
     v = C.c_double(0)
     _check(lib().sa_measure_fp32_peak(device, C.byref(v)), "measure_fp32_peak")
     return v.value
+
+
+# ------------------------------------------------------------------------------------------------
+# before the path: anchor pairs (signalMachine.c:615, :343-344)
+# ------------------------------------------------------------------------------------------------
+def filterToRemoveOverlap(pairs):
+    """filterToRemoveOverlap (pairwiseAligner.c:1575-1616) on (x, y) pairs sorted by (x, y)."""
+    a = _anchors(pairs)
+    out = np.zeros((max(len(a), 1), 2), np.int64)
+    n = C.c_int64(0)
+    _check(lib().sa_filterToRemoveOverlap(a.ctypes.data_as(_i64p), len(a), out.ctypes.data_as(_i64p), C.byref(n)),
+           "filterToRemoveOverlap")
+    return [tuple(int(v) for v in r) for r in out[:n.value]]
+
+
+def guideAlignmentToRebasedAnchorPairs(start1, end1, strand1, start2, end2, ops, trim, strand2=1):
+    """signalUtils_guideAlignmentToRebasedAnchorPairs (signalMachineUtils.c:142-164).  ops: (op, length)
+    cigar operations (CIGAR_MATCH / CIGAR_INDEL_X / CIGAR_INDEL_Y).  Returns (anchor pairs, rebased
+    (start1, end1, strand1))."""
+    ga = GuideAlignment(start1, end1, int(strand1), 0, start2, end2, int(strand2), 0)
+    arr = (CigarOp * max(len(ops), 1))()
+    for i, (op, length) in enumerate(ops):
+        arr[i].op, arr[i].length = op, length
+    cap = sum(l for o, l in ops if o == CIGAR_MATCH) + 1
+    out = np.zeros((cap, 2), np.int64)
+    n = C.c_int64(0)
+    _check(lib().sa_guideAlignmentToRebasedAnchorPairs(C.byref(ga), arr, len(ops), trim, out.ctypes.data_as(_i64p),
+                                                       cap, C.byref(n)), "guideAlignmentToRebasedAnchorPairs")
+    return [tuple(int(v) for v in r) for r in out[:n.value]], (ga.start1, ga.end1, ga.strand1)
+
+
+def getRemappedAnchorPairs(anchors, event_map, map_offset):
+    """signalUtils_getRemappedAnchorPairs (signalMachineUtils.c:166-170)."""
+    a = _anchors(anchors)
+    em = np.ascontiguousarray(event_map, dtype=np.int64)
+    out = np.zeros((max(len(a), 1), 2), np.int64)
+    n = C.c_int64(0)
+    _check(lib().sa_getRemappedAnchorPairs(a.ctypes.data_as(_i64p), len(a), em.ctypes.data_as(_i64p), len(em),
+                                           map_offset, out.ctypes.data_as(_i64p), C.byref(n)), "getRemappedAnchorPairs")
+    return [tuple(int(v) for v in r) for r in out[:n.value]]
+
+
+# ------------------------------------------------------------------------------------------------
+# after the path: ordering, score and posterior files (signalMachine.c:68-260, :715-728)
+# ------------------------------------------------------------------------------------------------
+def _pair_array(pairs):
+    a = np.ascontiguousarray(np.asarray(pairs, dtype=PAIR_DTYPE) if not isinstance(pairs, np.ndarray) or
+                             pairs.dtype != PAIR_DTYPE else pairs)
+    return a
+
+
+def sortByXPlusYCoordinate(pairs):
+    """stList_sort(..., sortByXPlusYCoordinate2): ascending x + y (equal keys keep their order)."""
+    a = _pair_array(pairs).copy()
+    lib().sa_sortByXPlusYCoordinate(a.ctypes.data_as(C.POINTER(AlignedPair)), len(a))
+    return a
+
+
+def scoreByPosteriorProbabilityIgnoringGaps(pairs):
+    a = _pair_array(pairs)
+    return lib().sa_scoreByPosteriorProbabilityIgnoringGaps(a.ctypes.data_as(C.POINTER(AlignedPair)), len(a))
+
+
+def _output_read(target, strand, forward, event_offset, reference_offset, events, scale, shift, var, scale_sd,
+                 read_label, contig, keep):
+    ev = _f64(events, 4)
+    t = target.encode()
+    lab, con = read_label.encode(), contig.encode()
+    keep += [ev, t, lab, con]
+    return OutputRead(lab, con, t, len(t), int(strand), int(forward), event_offset, reference_offset,
+                      ev.ctypes.data_as(_f64p), len(ev), scale, shift, var, scale_sd)
+
+
+def formatAlignment(fmt, sm, pairs, target, strand, forward, event_offset, reference_offset, events, scale=1.0,
+                    shift=0.0, var=1.0, scale_sd=1.0, read_label="", contig=""):
+    """The text outputAlignment (signalMachine.c:240-260) appends for one strand of one read."""
+    keep = []
+    rd = _output_read(target, strand, forward, event_offset, reference_offset, events, scale, shift, var, scale_sd,
+                      read_label, contig, keep)
+    a = _pair_array(pairs)
+    text = C.c_void_p()
+    n = C.c_int64(0)
+    _check(lib().sa_formatAlignment(fmt, sm.handle, C.byref(rd), a.ctypes.data_as(C.POINTER(AlignedPair)), len(a),
+                                    C.byref(text), C.byref(n)), "formatAlignment")
+    try:
+        return C.string_at(text, n.value).decode() if n.value else ""
+    finally:
+        lib().sa_free_text(text)
+
+
+def outputAlignment(fmt, path, sm, pairs, target, strand, forward, event_offset, reference_offset, events, scale=1.0,
+                    shift=0.0, var=1.0, scale_sd=1.0, read_label="", contig=""):
+    """outputAlignment: the lines appended to the posterior file at `path`."""
+    keep = []
+    rd = _output_read(target, strand, forward, event_offset, reference_offset, events, scale, shift, var, scale_sd,
+                      read_label, contig, keep)
+    a = _pair_array(pairs)
+    _check(lib().sa_outputAlignment(fmt, str(path).encode(), sm.handle, C.byref(rd),
+                                    a.ctypes.data_as(C.POINTER(AlignedPair)), len(a)), "outputAlignment")

@@ -17,6 +17,7 @@ SOURCES = [
     ("sa_host.cpp", []),
     ("sa_memory.cpp", []),
     ("sa_server.cpp", []),
+    ("sa_io.cpp", []),
     ("sa_fp64.cu", ["-fmad=false"]),
     ("sa_fp32.cu", []),
     ("sa_noalloc.cu", []),
