@@ -330,6 +330,44 @@ sa_status sa_guideAlignmentToRebasedAnchorPairs(sa_guide_alignment *ga, const sa
 sa_status sa_getRemappedAnchorPairs(const int64_t *anchors, int64_t n_anchors, const int64_t *event_map,
                                     int64_t map_length, int64_t map_offset, int64_t *out, int64_t *n_out);
 
+/* ---- before the path: per-read scale / shift / drift / variance (signalMachineUtils.c:186-223) ---- */
+
+/* NanoporeReadAdjustmentParameters (inc/nanopore.h:11-19) */
+typedef struct {
+    double scale, shift, var, shift_sd, scale_sd, var_sd, drift;
+} sa_read_params;
+
+/* one strand of a read for the estimation: its basecalled sequence, the event of each sequence
+ * position (strand event map), and its event table (4 doubles per event: mean, noise, duration,
+ * delta time) */
+typedef struct {
+    const sa_state_machine *sm;   /* the model: match table rows (mean, sd, noise mean, noise sd, lambda) */
+    const char *read;
+    int64_t read_length;
+    const int64_t *event_map;     /* read_length entries */
+    const double *events;
+    int64_t n_events;
+} sa_param_read;
+
+/* nanopore_getOneDAssignmentsFromRead (nanopore.c:503-533): per k-mer of the read its event, the first
+ * position of each event only; k-mer ids and (mean, noise, delta time) per assignment, up to
+ * `capacity` (SA_E_OUTPUT beyond, *n_out the count); either output may be NULL */
+sa_status sa_oneDAssignmentsFromRead(const sa_param_read *read, int64_t *kmer_ids, double *event_params,
+                                     int64_t capacity, int64_t *n_out);
+
+/* signalUtils_estimateNanoporeParams' fits for a batch of reads on the GPU, one CTA per read:
+ * nanopore_compute_mean_scale_params with drift and variance (nanopore.c:650-781) and
+ * nanopore_compute_noise_scale_params (:783-848) over the read's 1D assignments.  params[i] is
+ * updated in place (scale, shift, drift, var, shift_sd, scale_sd, var_sd); read_status[i] is
+ * SA_E_ARG for a read without assignments or with a singular system (the reference exits).  The
+ * machine updates that follow in the reference are sa_stateMachine_setScaling and
+ * sa_stateMachine_scaleNoise, and the drift correction sa_adjustEventsForDrift. */
+sa_status sa_estimateNanoporeParams(const sa_param_read *reads, int64_t n_reads, sa_read_params *params,
+                                    int32_t *read_status, void *stream);
+
+/* nanopore_adjustEventsForDriftP (nanopore.c:535-540): mean -= delta time x drift, in place */
+sa_status sa_adjustEventsForDrift(double *events, int64_t n_events, double drift);
+
 /* ---- after the path: ordering, score and the posterior files (signalMachine.c:68-260, :715-728) ---- */
 
 /* stList_sort(alignedPairs, sortByXPlusYCoordinate2) (pairwiseAligner.c:1434-1438): ascending x + y.

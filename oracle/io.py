@@ -10,6 +10,11 @@ imports this).  Plain-Python restatements of the reference, line for line:
   (signalMachine.c:317-331)
 * writePosteriorProbsFull / writePosteriorProbsVC / writeAssignments (signalMachine.c:33-238), with
   the reference's printf formats.
+* nanopore_getOneDAssignmentsFromRead (impl/nanopore.c:503-533), nanopore_lineq_solve (:586-648),
+  nanopore_compute_mean_scale_params with drift and variance (:650-781),
+  nanopore_compute_noise_scale_params (:783-848), nanopore_adjustEventsForDriftP (:535-540): the
+  fits of signalUtils_estimateNanoporeParams (impl/signalMachineUtils.c:186-223), sums in the
+  reference's sequential order.
 
 The reverse complement is sonLib's stString_reverseComplementString (sonLib is not vendored in the
 reference tree): A/C/G/T in either case complemented, other characters kept.
@@ -128,3 +133,80 @@ def format_alignment(fmt, pairs, alphabet, k, match_table, target, strand, forwa
                 lines.append("%d\t%d\t%s\t%f\t%s\t%s\t%s\n" % (y, x_adj + q, path_kmer[qpos], p, strand_label,
                                                                 forward_label, read_label))
     return "".join(lines)
+
+
+# ------------------------------------------------------------------------------------------------
+# per-read parameter estimation (impl/nanopore.c:503-540, :586-848)
+# ------------------------------------------------------------------------------------------------
+def one_d_assignments(read, event_map, events, alphabet, k):
+    """nanopore_getOneDAssignmentsFromRead: [(kmer id, mean, sd, delta time)]"""
+    out = []
+    prev = -1
+    for i in range(len(read) - (k - 1)):
+        ev = event_map[i]
+        kid = 0
+        for c in read[i:i + k]:
+            kid = kid * len(alphabet) + alphabet.index(c)
+        if ev > prev:
+            out.append((kid, events[ev][0], events[ev][1], events[ev][3]))
+            prev = ev
+    return out
+
+
+def lineq_solve(a, b):
+    """nanopore_lineq_solve (Gauss-Jordan, no pivoting needed for these systems)"""
+    n = len(b)
+    a = [row[:] for row in a]
+    x = list(b)
+    for i in range(n):
+        f = 1.0 / a[i][i]
+        x[i] *= f
+        a[i] = [v * f for v in a[i]]
+        for s in range(i + 1, n):
+            g = a[s][i]
+            x[s] -= g * x[i]
+            a[s] = [a[s][j] - g * a[i][j] for j in range(n)]
+    for i in range(n - 1, -1, -1):
+        for s in range(i - 1, -1, -1):
+            g = a[s][i]
+            x[s] -= g * x[i]
+            a[s] = [a[s][j] - g * a[i][j] for j in range(n)]
+    return x
+
+
+def estimate_params(assignments, model):
+    """nanopore_compute_mean_scale_params (drift and var) + nanopore_compute_noise_scale_params:
+    returns dict(shift, scale, drift, var, shift_sd, scale_sd, var_sd); model rows of 5"""
+    xwx = [[0.0] * 3 for _ in range(3)]
+    xwy = [0.0] * 3
+    nwx = [[0.0] * 2 for _ in range(2)]
+    nwy = [0.0] * 2
+    for kid, mean, sd, dt in assignments:
+        lm, lsd, nm, nsd = model[kid][0], model[kid][1], model[kid][2], model[kid][3]
+        iv = 1.0 / (lsd * lsd)
+        sm, st = lm * iv, dt * iv
+        xwx[0][0] += iv; xwx[0][1] += sm; xwx[0][2] += st
+        xwx[1][1] += sm * lm; xwx[1][2] += sm * dt; xwx[2][2] += st * dt
+        xwy[0] += iv * mean; xwy[1] += sm * mean; xwy[2] += st * mean
+        inv = 1.0 / (nsd * nsd)
+        snm = nm * inv
+        nwx[0][0] += inv; nwx[0][1] += snm; nwx[1][1] += snm * nm
+        nwy[0] += inv * sd; nwy[1] += snm * sd
+    xwx[1][0], xwx[2][0], xwx[2][1] = xwx[0][1], xwx[0][2], xwx[1][2]
+    nwx[1][0] = nwx[0][1]
+    beta = lineq_solve(xwx, xwy)
+    gamma = lineq_solve(nwx, nwy)
+    disp = disp_n = 0.0
+    for kid, mean, sd, dt in assignments:
+        lm, lsd, nm, nsd = model[kid][0], model[kid][1], model[kid][2], model[kid][3]
+        r = mean - (beta[0] + beta[1] * lm + beta[2] * dt)
+        disp += (r * r) / (lsd * lsd)
+        rn = sd - (gamma[0] + gamma[1] * nm)
+        disp_n += (rn * rn) / (nsd * nsd)
+    n = len(assignments)
+    return dict(shift=beta[0], scale=beta[1], drift=beta[2], var=(disp / n) ** 0.5, shift_sd=gamma[0],
+                scale_sd=gamma[1], var_sd=(disp_n / n) ** 0.5)
+
+
+def adjust_events_for_drift(events, drift):
+    return [[e[0] - e[3] * drift, e[1], e[2], e[3]] for e in events]

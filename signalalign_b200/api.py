@@ -65,6 +65,15 @@ class GuideAlignment(C.Structure):
                 ("start2", C.c_int64), ("end2", C.c_int64), ("strand2", C.c_int32), ("pad2", C.c_int32)]
 
 
+class ReadParams(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("scale", "shift", "var", "shift_sd", "scale_sd", "var_sd", "drift")]
+
+
+class ParamRead(C.Structure):
+    _fields_ = [("sm", C.c_void_p), ("read", C.c_char_p), ("read_length", C.c_int64),
+                ("event_map", C.POINTER(C.c_int64)), ("events", C.POINTER(C.c_double)), ("n_events", C.c_int64)]
+
+
 class OutputRead(C.Structure):
     _fields_ = [("read_label", C.c_char_p), ("contig", C.c_char_p), ("target", C.c_char_p), ("target_length", C.c_int64),
                 ("strand", C.c_int32), ("forward", C.c_int32), ("event_offset", C.c_int64),
@@ -140,6 +149,10 @@ def _bind(L):
         "sa_outputAlignment": (C.c_int, [C.c_int, C.c_char_p, vp, C.POINTER(OutputRead), C.POINTER(AlignedPair),
                                          C.c_int64]),
         "sa_free_text": (None, [C.c_void_p]),
+        "sa_oneDAssignmentsFromRead": (C.c_int, [C.POINTER(ParamRead), _i64p, _f64p, C.c_int64, _i64p]),
+        "sa_estimateNanoporeParams": (C.c_int, [C.POINTER(ParamRead), C.c_int64, C.POINTER(ReadParams),
+                                                C.POINTER(C.c_int32), vp]),
+        "sa_adjustEventsForDrift": (C.c_int, [_f64p, C.c_int64, C.c_double]),
         "sa_status_string": (C.c_char_p, [C.c_int]),
         "sa_kernel_launch_count": (C.c_int64, []),
         "sa_measure_fp32_peak": (C.c_int, [C.c_int32, _f64p]),
@@ -646,3 +659,50 @@ def outputAlignment(fmt, path, sm, pairs, target, strand, forward, event_offset,
     a = _pair_array(pairs)
     _check(lib().sa_outputAlignment(fmt, str(path).encode(), sm.handle, C.byref(rd),
                                     a.ctypes.data_as(C.POINTER(AlignedPair)), len(a)), "outputAlignment")
+
+
+# ------------------------------------------------------------------------------------------------
+# before the path: per-read scale / shift / drift / variance (signalMachineUtils.c:186-223)
+# ------------------------------------------------------------------------------------------------
+def _param_read(sm, read, event_map, events, keep):
+    em = np.ascontiguousarray(event_map, dtype=np.int64)
+    ev = _f64(events, 4)
+    rb = read.encode()
+    keep += [em, ev, rb]
+    return ParamRead(sm.handle, rb, len(rb), em.ctypes.data_as(_i64p), ev.ctypes.data_as(_f64p), len(ev))
+
+
+def oneDAssignmentsFromRead(sm, read, event_map, events):
+    """nanopore_getOneDAssignmentsFromRead: (k-mer ids, [(mean, noise, delta time)])"""
+    keep = []
+    pr = _param_read(sm, read, event_map, events, keep)
+    cap = max(len(read), 1)
+    ids = np.zeros(cap, np.int64)
+    ep = np.zeros((cap, 3), np.float64)
+    n = C.c_int64(0)
+    _check(lib().sa_oneDAssignmentsFromRead(C.byref(pr), ids.ctypes.data_as(_i64p), ep.ctypes.data_as(_f64p), cap,
+                                            C.byref(n)), "oneDAssignmentsFromRead")
+    return ids[:n.value], ep[:n.value]
+
+
+def estimateNanoporeParams(items, stream=None):
+    """Batched fits on the GPU.  items: [(sm, read, event_map, events, initial params dict)].
+    Returns [(status, params dict)]."""
+    keep = []
+    arr = (ParamRead * max(len(items), 1))()
+    prm = (ReadParams * max(len(items), 1))()
+    for i, (sm, read, em, ev, init) in enumerate(items):
+        arr[i] = _param_read(sm, read, em, ev, keep)
+        for k, v in (init or {}).items():
+            setattr(prm[i], k, v)
+    status = (C.c_int32 * max(len(items), 1))()
+    _check(lib().sa_estimateNanoporeParams(arr, len(items), prm, status, stream), "estimateNanoporeParams")
+    names = [f[0] for f in ReadParams._fields_]
+    return [(status[i], {k: getattr(prm[i], k) for k in names}) for i in range(len(items))]
+
+
+def adjustEventsForDrift(events, drift):
+    """nanopore_adjustEventsForDriftP on a copy of the event table"""
+    ev = _f64(events, 4).copy()
+    _check(lib().sa_adjustEventsForDrift(ev.ctypes.data_as(_f64p), len(ev), drift), "adjustEventsForDrift")
+    return ev
