@@ -285,6 +285,29 @@ sa_status sa_server_release(sa_server *s, int64_t ticket);
 /* finishes the queued reads, then stops the dispatcher */
 void sa_server_destroy(sa_server *s);
 
+/* ---- EM expectations: the same path with the expectation epilogue (pairwiseAligner.c:1983-2003) ---- */
+
+/* the accumulators of a continuous pair HMM (continuousPairHmm_construct, continuousHmm.c:84-141);
+ * the caller owns the arrays and initialises them (transitions and posteriors to the pseudocounts,
+ * the rest to zero, as hmmContinuous_getExpectationsHmm does); calls accumulate into them */
+typedef struct {
+    double likelihood;            /* += the total probability of every posterior anti-diagonal */
+    double transitions[9];        /* from * 3 + to; states: 0 match, 1 skip (gap-X), 2 extra event (gap-Y) */
+    double *event_expectations;   /* n_kmers x 2: weighted descaled event means, weighted spread */
+    double *posteriors;           /* n_kmers: weights */
+    uint8_t *observed;            /* n_kmers */
+} sa_expectations;
+
+/* getExpectationsUsingAnchors with diagonalCalculation_Expectations (pairwiseAligner.c:1255-1275,
+ * cell_signal_updateExpectations :763-793) on the plain FP64 form: the read's regions run in order in
+ * one CTA; every transition posterior of the window's anti-diagonals is added in the reference's
+ * order.  Gaussian machines (SA_THREE_STATE) and canonical references only (SA_E_UNSUPPORTED
+ * otherwise). */
+sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm, const char *reference, int64_t reference_length,
+                                         const double *events, int64_t n_events, const int64_t *anchors,
+                                         int64_t n_anchors, const sa_params *p, int32_t ragged_left,
+                                         int32_t ragged_right, sa_expectations *ex);
+
 /* ---- before the path: anchor pairs from the guide alignment (signalMachine.c:615, :343-344) ---- */
 
 /* one cigar operation of the guide alignment (AlignmentOperation of sonLib's PairwiseAlignment) */

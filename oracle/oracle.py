@@ -70,6 +70,10 @@ def lib():
         L.orc_full_matrix.argtypes = [C.POINTER(_Model), C.c_char_p, C.c_int64, _f64p, C.c_int64, C.c_double,
                                       C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_void_p, C.c_int64, _i64p,
                                       _f64p, _f64p, _f64p]
+        L.orc_expectations.restype = C.c_int
+        L.orc_expectations.argtypes = [C.POINTER(_Model), C.c_char_p, C.c_int64, _f64p, C.c_int64, _i64p,
+                                       C.c_int64, C.POINTER(_Params), C.c_int, C.c_int, _f64p, _f64p, _f64p, _f64p,
+                                       C.POINTER(C.c_uint8)]
         L.orc_emission.restype = C.c_double
         L.orc_emission.argtypes = [C.POINTER(_Model), C.c_int64, C.c_double, C.c_double, C.c_int]
         L.orc_log_gauss_pdf.restype = C.c_double
@@ -188,6 +192,36 @@ def aligned_pairs(om, ref, events, anchors, p, ragged_left=True, ragged_right=Tr
     if with_total_probs:
         return pairs, tp[:n_tp.value].copy()
     return pairs
+
+
+def expectations(om, ref, events, anchors, p, ragged_left=True, ragged_right=True, transition_pseudocount=0.001,
+                 emission_pseudocount=0.001, state=None):
+    """getExpectationsUsingAnchors (pairwiseAligner.c:1983-2003) with diagonalCalculation_Expectations
+    into a continuous pair HMM (continuousPairHmm_construct's pseudocounts, continuousHmm.c:84-141).
+    state: a previous result to accumulate into.  Returns dict(likelihood, transitions (3x3),
+    event_expectations (n_kmers x 2), posteriors (n_kmers), observed (n_kmers))."""
+    k = om.model["kmer_length"]
+    n = om.model["n_kmers"]
+    lX = max(len(ref) - (k - 1), 0) if len(ref) > 0 else 0
+    ev = np.ascontiguousarray(np.asarray(events, dtype=np.float64).reshape(-1, 4))
+    a = np.ascontiguousarray(np.asarray(anchors, dtype=np.int64).reshape(-1, 2))
+    if state is None:
+        state = dict(likelihood=0.0, transitions=np.full((3, 3), transition_pseudocount),
+                     event_expectations=np.zeros((n, 2)), posteriors=np.full(n, emission_pseudocount),
+                     observed=np.zeros(n, np.uint8))
+    st = {key: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for key, v in state.items()}
+    ll = np.array([st["likelihood"]], np.float64)
+    tr = np.ascontiguousarray(st["transitions"], dtype=np.float64)
+    ee = np.ascontiguousarray(st["event_expectations"], dtype=np.float64)
+    po = np.ascontiguousarray(st["posteriors"], dtype=np.float64)
+    ob = np.ascontiguousarray(st["observed"], dtype=np.uint8)
+    ps = _params_struct(p)
+    rc = lib().orc_expectations(C.byref(om.s), ref.encode(), lX, _p(ev, C.c_double), len(ev), _p(a, C.c_int64), len(a),
+                                C.byref(ps), int(ragged_left), int(ragged_right), _p(ll, C.c_double),
+                                _p(tr, C.c_double), _p(ee, C.c_double), _p(po, C.c_double), _p(ob, C.c_uint8))
+    if rc:
+        raise OracleError("orc_expectations rc=%d" % rc)
+    return dict(likelihood=float(ll[0]), transitions=tr, event_expectations=ee, posteriors=po, observed=ob)
 
 
 def full_matrix(om, ref, events, threshold, ragged_left=False, ragged_right=False, options="CEO", p_mode=0):

@@ -555,6 +555,77 @@ static int orc_posteriors(orc_dp *dp, int64_t xay, double total, double threshol
     return ORC_OK;
 }
 
+/* Expectations of a continuous pair HMM (continuousPairHmm_construct, continuousHmm.c:84-141):
+ * transition expectations (from * 3 + to), per k-mer weighted event sums (mean, spread) and weights;
+ * the caller initialises them (pseudocounts) */
+typedef struct {
+    double likelihood;
+    double transitions[9];
+    double *event_exp;          /* n_kmers x 2 */
+    double *posteriors;         /* n_kmers */
+    unsigned char *observed;    /* n_kmers */
+} orc_expect;
+
+/* cell_signal_updateExpectations (pairwiseAligner.c:763-793): one transition of the cell's
+ * calculation, its posterior added to the transition expectations and, into match, to the k-mer's
+ * emission expectation (continuousPairHmm_addToEmissionExpectation, continuousHmm.c:160-169: the
+ * spread uses the running mean, so the order of the updates matters) */
+static void orc_expect_update(const orc_model *m, orc_expect *ex, double from_v, double to_v, int from, int to,
+                              double e, double t, double total, int64_t kmer, const double *ev) {
+    double p = exp(from_v + to_v + (e + t) - total);
+    ex->transitions[from * 3 + to] += p;
+    if (to == S_MATCH) {
+        double mu = m->match[kmer * 5];
+        double x = (ev[0] + m->var * mu - m->scale * mu - m->shift) / m->var;
+        ex->event_exp[2 * kmer] += p * x;
+        ex->posteriors[kmer] += p;
+        double uk = ex->event_exp[2 * kmer] / ex->posteriors[kmer];
+        ex->event_exp[2 * kmer + 1] += p * (x - uk) * (x - uk);
+        ex->observed[kmer] = 1;
+    }
+}
+
+/* diagonalCalculation_Expectations (pairwiseAligner.c:1255-1275): the likelihood takes the diagonal's
+ * total; the cells of B[xay] in ascending xmy are recalculated against the forward neighbours
+ * (lower and upper F[xay-1], middle F[xay-2]) in stateMachine3_cellCalculate's order, each
+ * transition reported to orc_expect_update.  The reference frees a forward diagonal after its last
+ * posterior use (pairwiseAligner.c:1384-1387), so in a window traced back to T the middle
+ * neighbours of xay = T+1 (F[T-1]) are gone and their transitions are skipped.  Single-path cells
+ * only. */
+static void orc_expect_diag(orc_dp *dp, int64_t xay, double total, orc_expect *ex, int64_t traced_back_to) {
+    const orc_model *m = dp->m;
+    const orc_paths *P = dp->P;
+    const double *t = m->t;
+    ex->likelihood += total;
+    orc_diag *b = &dp->B[xay];
+    for (int64_t xmy = b->xmyL; xmy <= b->xmyR; xmy += 2) {
+        int64_t x = orc_xcoord(xay, xmy), y = orc_ycoord(xay, xmy);
+        double *cur = orc_cell(b, xmy);
+        double *lo = xay >= 1 ? orc_cell(&dp->F[xay - 1], xmy - 1) : NULL;
+        double *mi = xay - 2 >= traced_back_to ? orc_cell(&dp->F[xay - 2], xmy) : NULL;
+        double *up = xay >= 1 ? orc_cell(&dp->F[xay - 1], xmy + 1) : NULL;
+        int64_t kid = P->ids[P->pos[x].first];
+        const double *ev = orc_event(dp, y);
+        if (lo) {
+            double e = orc_emit_gapx(m, kid);
+            orc_expect_update(m, ex, lo[S_MATCH], cur[S_GAPX], S_MATCH, S_GAPX, e, t[T_GAP_OPEN_X], total, kid, ev);
+            orc_expect_update(m, ex, lo[S_GAPX], cur[S_GAPX], S_GAPX, S_GAPX, e, t[T_GAP_EXTEND_X], total, kid, ev);
+            orc_expect_update(m, ex, lo[S_GAPY], cur[S_GAPX], S_GAPY, S_GAPX, e, t[T_GAP_SWITCH_TO_X], total, kid, ev);
+        }
+        if (mi) {
+            double e = orc_emit_event(m, kid, ev, 1);
+            orc_expect_update(m, ex, mi[S_MATCH], cur[S_MATCH], S_MATCH, S_MATCH, e, t[T_MATCH_CONTINUE], total, kid, ev);
+            orc_expect_update(m, ex, mi[S_GAPX], cur[S_MATCH], S_GAPX, S_MATCH, e, t[T_MATCH_FROM_GAP_X], total, kid, ev);
+            orc_expect_update(m, ex, mi[S_GAPY], cur[S_MATCH], S_GAPY, S_MATCH, e, t[T_MATCH_FROM_GAP_Y], total, kid, ev);
+        }
+        if (up) {
+            double e = orc_emit_event(m, kid, ev, 0);
+            orc_expect_update(m, ex, up[S_MATCH], cur[S_GAPY], S_MATCH, S_GAPY, e, t[T_GAP_OPEN_Y], total, kid, ev);
+            orc_expect_update(m, ex, up[S_GAPY], cur[S_GAPY], S_GAPY, S_GAPY, e, t[T_GAP_EXTEND_Y], total, kid, ev);
+        }
+    }
+}
+
 static void orc_dp_free(orc_dp *dp) {
     if (dp->F) for (int64_t i = 0; i <= dp->n; i++) { free(dp->F[i].poff); free(dp->F[i].v); }
     if (dp->B) for (int64_t i = 0; i <= dp->n; i++) { free(dp->B[i].poff); free(dp->B[i].v); }
@@ -583,7 +654,7 @@ static int orc_banded_region(const orc_model *m, const char *seq, int64_t lX, co
                              const int64_t *anchors, int64_t n_anchors, const orc_params *p,
                              int ragged_left, int ragged_right, const char *options, int nopt,
                              orc_pair *out, int64_t *n_out, int64_t max_out, int64_t ox, int64_t oy,
-                             double *tp_out, int64_t *n_tp, int64_t max_tp) {
+                             double *tp_out, int64_t *n_tp, int64_t max_tp, orc_expect *ex) {
     int64_t n = lX + lY;
     if (n == 0) return ORC_OK;
     if (p->traceback_diagonals < 1 || p->diagonal_expansion < 0 || p->diagonal_expansion % 2 != 0 ||
@@ -647,7 +718,8 @@ static int orc_banded_region(const orc_model *m, const char *seq, int64_t lX, co
                         (*n_tp)++;
                     }
                 }
-                rc = orc_posteriors(&dp, d2, total, p->threshold, out, n_out, max_out, ox, oy);
+                if (ex) orc_expect_diag(&dp, d2, total, ex, traced_back_to);
+                else rc = orc_posteriors(&dp, d2, total, p->threshold, out, n_out, max_out, ox, oy);
                 if (rc) goto done;
             }
         }
@@ -666,11 +738,47 @@ done:
 /* getAlignedPairsUsingAnchors -> getPosteriorProbsWithBandingSplittingAlignmentsByLargeGaps
  * (pairwiseAligner.c:1773-1837, 1871-1899).  seq is the reference nucleotide string, lX the
  * number of k-mers in it.  Returns ORC_OK and fills out[0..*n_out). */
+static int orc_split_run(const orc_model *m, const char *seq, int64_t lX, const double *events, int64_t lY,
+                         const int64_t *anchors, int64_t n_anchors, const orc_params *p,
+                         int ragged_left, int ragged_right, const char *options,
+                         orc_pair *out, int64_t max_out, int64_t *n_out,
+                         double *tp_out, int64_t max_tp, int64_t *n_tp, orc_expect *ex);
+
 int orc_aligned_pairs(const orc_model *m, const char *seq, int64_t lX, const double *events, int64_t lY,
                       const int64_t *anchors, int64_t n_anchors, const orc_params *p,
                       int ragged_left, int ragged_right, const char *options,
                       orc_pair *out, int64_t max_out, int64_t *n_out,
                       double *tp_out, int64_t max_tp, int64_t *n_tp) {
+    return orc_split_run(m, seq, lX, events, lY, anchors, n_anchors, p, ragged_left, ragged_right, options, out,
+                         max_out, n_out, tp_out, max_tp, n_tp, NULL);
+}
+
+/* getExpectationsUsingAnchors (pairwiseAligner.c:1983-2003): the banded routine with
+ * diagonalCalculation_Expectations in place of the posterior callback.  The expectation arrays are
+ * the caller's (initialised with its pseudocounts); canonical references only (no 'X'). */
+int orc_expectations(const orc_model *m, const char *seq, int64_t lX, const double *events, int64_t lY,
+                     const int64_t *anchors, int64_t n_anchors, const orc_params *p, int ragged_left,
+                     int ragged_right, double *likelihood, double *transitions, double *event_exp,
+                     double *posteriors, unsigned char *observed) {
+    orc_expect ex;
+    ex.likelihood = *likelihood;
+    for (int i = 0; i < 9; i++) ex.transitions[i] = transitions[i];
+    ex.event_exp = event_exp;
+    ex.posteriors = posteriors;
+    ex.observed = observed;
+    int64_t n_out = 0;
+    int rc = orc_split_run(m, seq, lX, events, lY, anchors, n_anchors, p, ragged_left, ragged_right, "CEO", NULL, 0,
+                           &n_out, NULL, 0, NULL, &ex);
+    *likelihood = ex.likelihood;
+    for (int i = 0; i < 9; i++) transitions[i] = ex.transitions[i];
+    return rc;
+}
+
+static int orc_split_run(const orc_model *m, const char *seq, int64_t lX, const double *events, int64_t lY,
+                         const int64_t *anchors, int64_t n_anchors, const orc_params *p,
+                         int ragged_left, int ragged_right, const char *options,
+                         orc_pair *out, int64_t max_out, int64_t *n_out,
+                         double *tp_out, int64_t max_tp, int64_t *n_tp, orc_expect *ex) {
     *n_out = 0;
     if (n_tp) *n_tp = 0;
     int64_t n_tp_local = 0;
@@ -698,7 +806,7 @@ int orc_aligned_pairs(const orc_model *m, const char *seq, int64_t lX, const dou
         if (rc) break;
         rc = orc_banded_region(m, seq + x1, x2 - x1, events + y1 * ORC_NB_EVENT_PARAMS, y2 - y1, sub, nsub, p,
                                ragged_left || i > 0, ragged_right || i < ns - 1, options, nopt,
-                               out, n_out, max_out, x1, y1, tp_out, n_tp ? n_tp : &n_tp_local, max_tp);
+                               out, n_out, max_out, x1, y1, tp_out, n_tp ? n_tp : &n_tp_local, max_tp, ex);
     }
     if (rc == ORC_OK && j != n_anchors) rc = ORC_E_ANCHORS;
     free(sub);

@@ -74,6 +74,12 @@ class ParamRead(C.Structure):
                 ("event_map", C.POINTER(C.c_int64)), ("events", C.POINTER(C.c_double)), ("n_events", C.c_int64)]
 
 
+class Expectations(C.Structure):
+    _fields_ = [("likelihood", C.c_double), ("transitions", C.c_double * 9),
+                ("event_expectations", C.POINTER(C.c_double)), ("posteriors", C.POINTER(C.c_double)),
+                ("observed", C.POINTER(C.c_uint8))]
+
+
 class OutputRead(C.Structure):
     _fields_ = [("read_label", C.c_char_p), ("contig", C.c_char_p), ("target", C.c_char_p), ("target_length", C.c_int64),
                 ("strand", C.c_int32), ("forward", C.c_int32), ("event_offset", C.c_int64),
@@ -153,6 +159,9 @@ def _bind(L):
         "sa_estimateNanoporeParams": (C.c_int, [C.POINTER(ParamRead), C.c_int64, C.POINTER(ReadParams),
                                                 C.POINTER(C.c_int32), vp]),
         "sa_adjustEventsForDrift": (C.c_int, [_f64p, C.c_int64, C.c_double]),
+        "sa_getExpectationsUsingAnchors": (C.c_int, [vp, C.c_char_p, C.c_int64, _f64p, C.c_int64, _i64p, C.c_int64,
+                                                     C.POINTER(Params), C.c_int32, C.c_int32,
+                                                     C.POINTER(Expectations)]),
         "sa_status_string": (C.c_char_p, [C.c_int]),
         "sa_kernel_launch_count": (C.c_int64, []),
         "sa_measure_fp32_peak": (C.c_int, [C.c_int32, _f64p]),
@@ -706,3 +715,37 @@ def adjustEventsForDrift(events, drift):
     ev = _f64(events, 4).copy()
     _check(lib().sa_adjustEventsForDrift(ev.ctypes.data_as(_f64p), len(ev), drift), "adjustEventsForDrift")
     return ev
+
+
+# ------------------------------------------------------------------------------------------------
+# EM expectations (getExpectationsUsingAnchors, pairwiseAligner.c:1983-2003)
+# ------------------------------------------------------------------------------------------------
+def getExpectationsUsingAnchors(sm, reference, events, anchors, p, ragged_left=True, ragged_right=True, state=None,
+                                transition_pseudocount=0.001, emission_pseudocount=0.001):
+    """Expectations of one read on the plain FP64 form, accumulated into `state` (a previous result)
+    or into fresh accumulators with the given pseudocounts (hmmContinuous_getExpectationsHmm).
+    Returns dict(likelihood, transitions (3x3), event_expectations (n_kmers x 2), posteriors,
+    observed)."""
+    n = sm.n_kmers
+    if state is None:
+        state = dict(likelihood=0.0, transitions=np.full((3, 3), transition_pseudocount),
+                     event_expectations=np.zeros((n, 2)), posteriors=np.full(n, emission_pseudocount),
+                     observed=np.zeros(n, np.uint8))
+    ee = np.ascontiguousarray(state["event_expectations"], dtype=np.float64).copy()
+    po = np.ascontiguousarray(state["posteriors"], dtype=np.float64).copy()
+    ob = np.ascontiguousarray(state["observed"], dtype=np.uint8).copy()
+    ex = Expectations()
+    ex.likelihood = state["likelihood"]
+    for i, v in enumerate(np.asarray(state["transitions"], dtype=np.float64).reshape(-1)):
+        ex.transitions[i] = v
+    ex.event_expectations = ee.ctypes.data_as(_f64p)
+    ex.posteriors = po.ctypes.data_as(_f64p)
+    ex.observed = ob.ctypes.data_as(C.POINTER(C.c_uint8))
+    ev = _f64(events, 4)
+    a = _anchors(anchors)
+    ref = reference.encode()
+    _check(lib().sa_getExpectationsUsingAnchors(sm.handle, ref, len(ref), ev.ctypes.data_as(_f64p), len(ev),
+                                                a.ctypes.data_as(_i64p), len(a), C.byref(p), int(ragged_left),
+                                                int(ragged_right), C.byref(ex)), "getExpectationsUsingAnchors")
+    return dict(likelihood=ex.likelihood, transitions=np.array(list(ex.transitions)).reshape(3, 3),
+                event_expectations=ee, posteriors=po, observed=ob)

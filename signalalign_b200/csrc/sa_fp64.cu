@@ -57,6 +57,19 @@ struct SetOut {
     int64_t cap;
 };
 
+// Expectations mode (getExpectationsUsingAnchors, pairwiseAligner.c:1983-2003): one CTA walks the
+// read's regions in order and folds every transition posterior into a continuous pair HMM's
+// accumulators in the reference's order (their emission spreads depend on it).
+struct ExpectOut {
+    int32_t on, n_regions;
+    double *scratch;            // 8 transition posteriors per cell of the anti-diagonal at hand
+    int32_t *mask;              // per cell: lower / middle / upper neighbour present
+    double *acc;                // likelihood, then the 3 x 3 transition expectations
+    double *event_exp;          // per k-mer: weighted mean sum, weighted spread sum
+    double *posteriors;         // per k-mer: weight
+    unsigned char *observed;    // per k-mer
+};
+
 // the 3 states of path q in the cell of anti-diagonal d (q must belong to that cell's column)
 __device__ __forceinline__ double *slot(double *base, const Region64 &R, int32_t d, int32_t q) {
     return base + 3 * ((int64_t) (d % R.ring) * R.stride + (q - R.pfirst[(d + R.xl[d]) >> 1]));
@@ -217,11 +230,89 @@ __device__ double total_probability(const Model64 &M, const Region64 &R, int32_t
     return total;
 }
 
-__global__ void __launch_bounds__(128) region_kernel(const Model64 *models, const Region64 *regions, SetOut O) {
+// diagonalCalculation_Expectations (pairwiseAligner.c:1255-1275) on anti-diagonal d2 of a window
+// traced back to T: the cells of B[d2] against their forward neighbours (the reference has freed
+// F[T-1] by then, so the middle neighbours of d2 = T+1 are absent), each transition's posterior
+// exp(F[from] + B[to] + (e + t) - total) (cell_signal_updateExpectations, :763-793), computed in
+// parallel; then thread 0 adds them in stateMachine3_cellCalculate's order, cell by cell
+// (continuousPairHmm_addToEmissionExpectation, continuousHmm.c:160-169, for transitions into match).
+__device__ void expect_diagonal(const Model64 &M, const Region64 &R, const ExpectOut &X, int32_t d2, int32_t T,
+                                double total, double (&acc)[10]) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int32_t region = (int32_t) blockIdx.x;
-    const Region64 R = regions[region];
-    const Model64 M = models[R.model];
+    for (int32_t xmy = R.xl[d2] + 2 * tid; xmy <= R.xr[d2]; xmy += 2 * nt) {
+        const int32_t c = (xmy - R.xl[d2]) >> 1;
+        const int32_t x = (d2 + xmy) >> 1, y = (d2 - xmy) >> 1;
+        const int32_t r = R.pfirst[x], kid = R.pid[r];
+        const double *cur = slot(R.B, R, d2, r);
+        const bool lo = in_band(R, d2 - 1, xmy - 1), mi = d2 - 2 >= T && in_band(R, d2 - 2, xmy),
+                   up = in_band(R, d2 - 1, xmy + 1);
+        double *ps = X.scratch + 8 * (int64_t) c;
+        if (lo) {
+            const double *l = slot(R.F, R, d2 - 1, R.pfirst[x - 1]);
+            const double e = emit_gapx(M, kid);
+            ps[0] = exp(l[S_M] + cur[S_X] + (e + M.t[T_OX]) - total);
+            ps[1] = exp(l[S_X] + cur[S_X] + (e + M.t[T_EX]) - total);
+            ps[2] = exp(l[S_Y] + cur[S_X] + (e + M.t[T_SX]) - total);
+        }
+        if (mi) {
+            const double *m = slot(R.F, R, d2 - 2, R.pfirst[x - 1]);
+            const double2 ev = R.ev[y - 1];
+            const double e = emit_event(M, kid, ev.x, ev.y, true);
+            ps[3] = exp(m[S_M] + cur[S_M] + (e + M.t[T_MC]) - total);
+            ps[4] = exp(m[S_X] + cur[S_M] + (e + M.t[T_MFGX]) - total);
+            ps[5] = exp(m[S_Y] + cur[S_M] + (e + M.t[T_MFGY]) - total);
+        }
+        if (up) {
+            const double *u = slot(R.F, R, d2 - 1, r);
+            const double2 ev = R.ev[y - 1];
+            const double e = emit_event(M, kid, ev.x, ev.y, false);
+            ps[6] = exp(u[S_M] + cur[S_Y] + (e + M.t[T_OY]) - total);
+            ps[7] = exp(u[S_Y] + cur[S_Y] + (e + M.t[T_EY]) - total);
+        }
+        X.mask[c] = (lo ? 1 : 0) | (mi ? 2 : 0) | (up ? 4 : 0);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        acc[0] += total;   // hmmExpectations->likelihood += totalProbability, once per diagonal
+        const int32_t w = (R.xr[d2] - R.xl[d2]) / 2 + 1;
+        for (int32_t c = 0; c < w; ++c) {
+            const int32_t mk = X.mask[c];
+            const double *ps = X.scratch + 8 * (int64_t) c;
+            if (mk & 1) {   // lower: M, X, Y -> X
+                acc[1 + S_M * 3 + S_X] += ps[0];
+                acc[1 + S_X * 3 + S_X] += ps[1];
+                acc[1 + S_Y * 3 + S_X] += ps[2];
+            }
+            if (mk & 2) {   // middle: M, X, Y -> M, each also an emission expectation
+                const int32_t xmy = R.xl[d2] + 2 * c;
+                const int32_t x = (d2 + xmy) >> 1, y = (d2 - xmy) >> 1;
+                const int64_t kid = R.pid[R.pfirst[x]];
+                const double mu = M.match[kid * 5];
+                const double xe = (R.ev[y - 1].x + M.var * mu - M.scale * mu - M.shift) / M.var;
+                for (int j = 0; j < 3; ++j) {
+                    const double p = ps[3 + j];
+                    acc[1 + j * 3 + S_M] += p;
+                    X.event_exp[2 * kid] += p * xe;
+                    X.posteriors[kid] += p;
+                    const double uk = X.event_exp[2 * kid] / X.posteriors[kid];
+                    X.event_exp[2 * kid + 1] += p * (xe - uk) * (xe - uk);
+                    X.observed[kid] = 1;
+                }
+            }
+            if (mk & 4) {   // upper: M, Y -> Y
+                acc[1 + S_M * 3 + S_Y] += ps[6];
+                acc[1 + S_Y * 3 + S_Y] += ps[7];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// One region: forward sweep, windowed traceback, and per traceback window either the posterior
+// pairs or (expectations mode) the expectation updates.
+__device__ void run_region(const Model64 &M, const Region64 &R, int32_t region, const SetOut &O, const ExpectOut &X,
+                           double (&acc)[10]) {
+    const int tid = threadIdx.x, nt = blockDim.x;
     // startStateProb / raggedStartStateProb (stateMachine.c:1022-1032) on anti-diagonal 0
     if (tid == 0) {
         double *c = slot(R.F, R, 0, 0);
@@ -262,6 +353,13 @@ __global__ void __launch_bounds__(128) region_kernel(const Model64 *models, cons
             R.P[dr] = total_probability(M, R, dr, dr < W.D);
         }
         __syncthreads();
+        if (X.on) {
+            for (int32_t d2 = W.from; d2 > W.T; --d2)
+                expect_diagonal(M, R, X, d2, W.T, R.P[W.from - 10 * ((W.from - d2) / 10)], acc);
+            if (W.at_end) break;
+            W = R.win[++wi];
+            continue;
+        }
         // diagonalCalculationPosteriorMatchProbs (pairwiseAligner.c:1202-1253) on (T, from]
         for (int32_t d2 = W.from; d2 > W.T; --d2) {
             const double total = R.P[W.from - 10 * ((W.from - d2) / 10)];
@@ -295,6 +393,25 @@ __global__ void __launch_bounds__(128) region_kernel(const Model64 *models, cons
     }
     // the total probability of the last anti-diagonal is the region's log-likelihood
     if (tid == 0) *R.loglik = R.P[R.n];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(128) region_kernel(const Model64 *models, const Region64 *regions, SetOut O,
+                                                     ExpectOut X) {
+    double acc[10];
+    if (X.on) {
+        // the read's regions in order (the reference's split wrapper loops over them), one CTA
+        for (int i = 0; i < 10; ++i) acc[i] = X.acc[i];
+        for (int32_t r = 0; r < X.n_regions; ++r) {
+            const Region64 R = regions[r];
+            run_region(models[R.model], R, r, O, X, acc);
+        }
+        if (threadIdx.x == 0)
+            for (int i = 0; i < 10; ++i) X.acc[i] = acc[i];
+        return;
+    }
+    const Region64 R = regions[blockIdx.x];
+    run_region(models[R.model], R, (int32_t) blockIdx.x, O, X, acc);
 }
 
 }  // namespace
@@ -630,7 +747,9 @@ sa_status plain_run(PlainSet *s, cudaStream_t stream) {
     O.tag = s->d_tag;
     O.count = s->d_count;
     O.cap = s->cap;
-    region_kernel<<<(unsigned) s->regs.size(), 128, 0, stream>>>(s->d_models, s->d_regions, O);
+    ExpectOut X;
+    std::memset(&X, 0, sizeof(X));
+    region_kernel<<<(unsigned) s->regs.size(), 128, 0, stream>>>(s->d_models, s->d_regions, O, X);
     count_launch();
     return cudaGetLastError() == cudaSuccess ? SA_OK : SA_E_CUDA;
 }
@@ -783,4 +902,107 @@ extern "C" sa_status sa_getAlignedPairsUsingAnchors(const sa_state_machine *sm_c
     if (log_likelihood) *log_likelihood = plain_log_likelihood(s, 0);
     plain_destroy(s);
     return SA_OK;
+}
+
+extern "C" sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm_c, const char *reference,
+                                                    int64_t reference_length, const double *events, int64_t n_events,
+                                                    const int64_t *anchors, int64_t n_anchors, const sa_params *p,
+                                                    int32_t ragged_left, int32_t ragged_right, sa_expectations *ex) {
+    if (!sm_c || !p || !ex || !ex->event_expectations || !ex->posteriors || !ex->observed || reference_length < 0 ||
+        n_events < 0 || n_anchors < 0)
+        return SA_E_ARG;
+    if ((reference_length > 0 && !reference) || (n_events > 0 && !events) || (n_anchors > 0 && !anchors))
+        return SA_E_ARG;
+    auto *sm = const_cast<sa_state_machine *>(sm_c);
+    // the continuous pair HMM of the Gaussian machine (hmmContinuous_getExpectationsHmm,
+    // continuousHmm.c:842-857); the HDP machine collects assignments instead
+    if (sm->type != SA_THREE_STATE || sm->emission == SA_EMIT_HDP) return SA_E_UNSUPPORTED;
+    sa_status st = check_params(*p);
+    if (st) return st;
+    sa_read rd;
+    std::memset(&rd, 0, sizeof(rd));
+    rd.sm = sm;
+    rd.reference = reference;
+    rd.reference_length = reference_length;
+    rd.events = events;
+    rd.n_events = n_events;
+    rd.anchors = anchors;
+    rd.n_anchors = n_anchors;
+    rd.scale = sm->scale;
+    rd.shift = sm->shift;
+    rd.var = sm->var;
+    rd.ragged_left = ragged_left;
+    rd.ragged_right = ragged_right;
+    rd.degenerate = SA_CYTOSINE_METHYLATION3;
+    PlainSet *s = nullptr;
+    st = plain_create(&rd, 1, *p, kPlainMaxBytes, &s);
+    if (st) return st;
+    int32_t width = 1;
+    for (const PlainRegion &pr : s->regs) {
+        if (pr.max_paths > 1) st = SA_E_UNSUPPORTED;   // single-path cells only
+        width = std::max(width, pr.stride);
+    }
+    if (!st) st = (sa_status) s->read_status[0];
+    if (!st) st = ensure_device_model(sm);
+    int prev_dev = 0;
+    if (!st && cudaGetDevice(&prev_dev) != cudaSuccess) st = SA_E_CUDA;
+    if (!st && cudaSetDevice(s->device) != cudaSuccess) st = SA_E_CUDA;
+    if (st) {
+        plain_destroy(s);
+        return st;
+    }
+    const int64_t nk = sm->n_kmers;
+    // one device block: scratch, mask, accumulators, per-k-mer expectations
+    auto up = [](size_t v) { return (v + 255) & ~(size_t) 255; };
+    const size_t o_mask = up(sizeof(double) * 8 * (size_t) width), o_acc = o_mask + up(sizeof(int32_t) * width);
+    const size_t o_ee = o_acc + up(sizeof(double) * 10), o_po = o_ee + up(sizeof(double) * 2 * nk);
+    const size_t o_ob = o_po + up(sizeof(double) * nk), total = o_ob + up((size_t) nk);
+    MemBlock blk;
+    st = plain_upload(s, nullptr);
+    if (!st) st = mem_get(MemKind::Device, s->device, total, blk);
+    if (!st) {
+        auto *d = static_cast<unsigned char *>(blk.ptr);
+        double acc[10];
+        acc[0] = ex->likelihood;
+        for (int i = 0; i < 9; ++i) acc[i + 1] = ex->transitions[i];
+        if (cudaMemcpy(d + o_acc, acc, sizeof(acc), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d + o_ee, ex->event_expectations, sizeof(double) * 2 * nk, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d + o_po, ex->posteriors, sizeof(double) * nk, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d + o_ob, ex->observed, (size_t) nk, cudaMemcpyHostToDevice) != cudaSuccess)
+            st = SA_E_CUDA;
+        ExpectOut X;
+        X.on = 1;
+        X.n_regions = (int32_t) s->regs.size();
+        X.scratch = reinterpret_cast<double *>(d);
+        X.mask = reinterpret_cast<int32_t *>(d + o_mask);
+        X.acc = reinterpret_cast<double *>(d + o_acc);
+        X.event_exp = reinterpret_cast<double *>(d + o_ee);
+        X.posteriors = reinterpret_cast<double *>(d + o_po);
+        X.observed = d + o_ob;
+        SetOut O;
+        std::memset(&O, 0, sizeof(O));
+        auto *dev = static_cast<unsigned char *>(s->dev.ptr);
+        if (!st && (cudaMemsetAsync(dev + s->res_off, 0, s->res_bytes, nullptr) != cudaSuccess ||
+                    cudaMemsetAsync(s->d_P, 0, std::max<size_t>(s->p_bytes, 1), nullptr) != cudaSuccess))
+            st = SA_E_CUDA;
+        if (!st && !s->regs.empty()) {
+            region_kernel<<<1, 128>>>(s->d_models, s->d_regions, O, X);
+            count_launch();
+            if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = SA_E_CUDA;
+        }
+        if (!st) {
+            if (cudaMemcpy(acc, d + o_acc, sizeof(acc), cudaMemcpyDeviceToHost) != cudaSuccess ||
+                cudaMemcpy(ex->event_expectations, d + o_ee, sizeof(double) * 2 * nk, cudaMemcpyDeviceToHost) !=
+                    cudaSuccess ||
+                cudaMemcpy(ex->posteriors, d + o_po, sizeof(double) * nk, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                cudaMemcpy(ex->observed, d + o_ob, (size_t) nk, cudaMemcpyDeviceToHost) != cudaSuccess)
+                st = SA_E_CUDA;
+            ex->likelihood = acc[0];
+            for (int i = 0; i < 9; ++i) ex->transitions[i] = acc[i + 1];
+        }
+    }
+    mem_put(blk);
+    cudaSetDevice(prev_dev);
+    plain_destroy(s);
+    return st;
 }

@@ -1,0 +1,99 @@
+"""EM expectations (getExpectationsUsingAnchors with diagonalCalculation_Expectations,
+pairwiseAligner.c:1255-1275, 1983-2003) on the plain FP64 form against the FP64 oracle: likelihood,
+transition expectations and per-k-mer emission expectations.  The GPU evaluates the same terms in
+the same order (the per-k-mer spread depends on the order), so agreement is to rounding of exp():
+1e-9 relative."""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from signalalign_b200 import synth
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from signalalign_b200 import api as a
+    return a
+
+
+def _p(api, **kw):
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _op(p):
+    return orc.params(threshold=p.threshold, expansion=p.diagonal_expansion, min_diags=p.min_diags_between_traceback,
+                      traceback=p.traceback_diagonals, split=p.split_matrix_bigger_than_this)
+
+
+def _compare(got, want):
+    assert got["likelihood"] == pytest.approx(want["likelihood"], rel=1e-12)
+    np.testing.assert_allclose(got["transitions"], want["transitions"], rtol=RTOL)
+    assert np.array_equal(got["observed"], want["observed"])
+    obs = want["observed"] > 0
+    assert obs.sum() > 100
+    np.testing.assert_allclose(got["posteriors"], want["posteriors"], rtol=RTOL)
+    np.testing.assert_allclose(got["event_expectations"][obs], want["event_expectations"][obs], rtol=RTOL, atol=1e-9)
+
+
+@pytest.mark.parametrize("ragged", [(True, True), (False, False)])
+def test_expectations_config0(api, ragged):
+    cfg = synth.config0()
+    m = W.gaussian_model(cfg)
+    rd = cfg["reads"][0]
+    p = _p(api)
+    om = W.oracle_model(m, orc.EMIT_DESCALED, rd)
+    want = orc.expectations(om, rd["reference"], rd["events"], rd["anchors"], _op(p), *ragged)
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED, rd)
+    got = api.getExpectationsUsingAnchors(sm, rd["reference"], rd["events"], rd["anchors"], p, *ragged)
+    _compare(got, want)
+    # the transition expectations out of match sum to about the number of matches plus the gaps they open
+    assert got["transitions"].sum() > 0.5 * len(rd["events"])
+
+
+@pytest.mark.parametrize("split,min_diags", [(2000, 1000), (3000 * 3000, 150)])
+def test_expectations_split_regions_short_windows_and_accumulation(api, split, min_diags):
+    """forced split regions (processed in order in one CTA; 15-18 per read) or short traceback
+    windows (the forward diagonals the reference has freed at each window's start), accumulated over
+    two reads"""
+    cfg = synth.config1(seed=21, n_reads=2, span=(600, 1200))
+    m = W.gaussian_model(cfg)
+    p = _p(api, split_matrix_bigger_than_this=split, min_diags_between_traceback=min_diags)
+    got = want = None
+    for rd in cfg["reads"]:
+        om = W.oracle_model(m, orc.EMIT_DESCALED, rd)
+        want = orc.expectations(om, rd["reference"], rd["events"], rd["anchors"], _op(p), state=want)
+        sm = W.gpu_model(api, m, orc.EMIT_DESCALED, rd)
+        got = api.getExpectationsUsingAnchors(sm, rd["reference"], rd["events"], rd["anchors"], p, state=got)
+    _compare(got, want)
+
+
+def test_expectations_unsupported_inputs(api):
+    cfg = synth.config0()
+    m = W.gaussian_model(cfg)
+    rd = cfg["reads"][0]
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED, rd)
+    # an 'X' in an ACGT reference cannot be expanded (its options C/E/O are outside the alphabet)
+    ref = rd["reference"][:200] + "X" + rd["reference"][201:]
+    with pytest.raises(api.SAError) as ei:
+        api.getExpectationsUsingAnchors(sm, ref, rd["events"], rd["anchors"], _p(api))
+    assert ei.value.status == 2   # SA_E_ALPHABET
+    # the HDP machine's expectations are assignments for its sampler, not a continuous pair HMM
+    hc = W.small_hdp_config()
+    hdp = W.hdp_dict(hc["hdp"], len(hc["alphabet"]) ** hc["k"])
+    from oracle import formats
+    hm = formats.parse_model_lines(*synth.model_text(hc["alphabet"], hc["k"], hc["table"]).split("\n")[:3])
+    hrd = hc["reads"][0]
+    smh = W.gpu_model(api, hm, orc.EMIT_HDP, hrd, hdp)
+    with pytest.raises(api.SAError) as ei:
+        api.getExpectationsUsingAnchors(smh, hrd["reference"], hrd["events"], hrd["anchors"], _p(api))
+    assert ei.value.status == 7   # SA_E_UNSUPPORTED
