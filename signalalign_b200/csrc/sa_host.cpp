@@ -47,8 +47,10 @@ sa_status band_construct(const int64_t *anchors, int64_t n_anchors, int64_t lX, 
     int64_t box_x_lo = 0, box_y_hi = 0, box_x_hi = 0, box_y_lo = 0;
     for (int64_t xay = 0; xay <= last; ++xay) {
         int64_t lo = box_x_lo - box_y_hi, hi = box_x_hi - box_y_lo;
-        if ((xay + lo) % 2 != 0) lo += 1;
-        if ((xay + hi) % 2 != 0) hi += 1;
+        // band_avoidOffByOne: round up to the anti-diagonal's parity (branch-free: the parity
+        // alternates from one anti-diagonal to the next)
+        lo += (xay + lo) & 1;
+        hi += (xay + hi) & 1;
         int64_t v = col_x(xay, lo);
         if (v < box_x_lo) lo += 2 * (box_x_lo - v);
         v = row_y(xay, lo);
@@ -231,22 +233,34 @@ sa_status build_paths(const sa_state_machine *sm, const char *reference, int64_t
     const int k = sm->kmer_length;
     const char *opts = degenerate_options(degenerate);
     const int nopt = (int) std::strlen(opts);
+    // character -> digit over the sorted alphabet (-1 outside it); 'X' is expanded below
+    int8_t code[256];
+    std::memset(code, -1, sizeof(code));
+    for (size_t i = 0; i < sm->alphabet.size(); ++i) code[(unsigned char) sm->alphabet[i]] = (int8_t) i;
+    const int64_t a = (int64_t) sm->alphabet.size();
     pt.lX = lX;
     pt.multi = false;
     pt.first.assign(lX + 2, 0);
     pt.ids.clear();
-    pt.kmers.clear();
     pt.ids.reserve(lX + 1);
     pt.ids.push_back(-1);
-    pt.kmers.insert(pt.kmers.end(), k, 0);
     pt.first[0] = 0;
     char buf[kMaxK];
     for (int64_t x = 1; x <= lX; ++x) {
         pt.first[x] = (int32_t) pt.ids.size();
         const char *km = reference + (x - 1);
         int pos[kMaxK], nd = 0;
-        for (int i = 0; i < k; ++i)
+        int64_t id = 0;
+        for (int i = 0; i < k; ++i) {
             if (km[i] == 'X') pos[nd++] = i;
+            const int8_t c = code[(unsigned char) km[i]];
+            id = id * a + c;
+            if (c < 0 && km[i] != 'X') return SA_E_ALPHABET;
+        }
+        if (nd == 0) {   // one path: the k-mer as written
+            pt.ids.push_back((int32_t) id);
+            continue;
+        }
         int64_t np = 1;
         for (int i = 0; i < nd; ++i) np *= nopt;
         if (np > 1) pt.multi = true;
@@ -257,10 +271,9 @@ sa_status build_paths(const sa_state_machine *sm, const char *reference, int64_t
                 buf[pos[i]] = opts[rem % nopt];
                 rem /= nopt;
             }
-            int64_t id = kmer_id_of(buf, k, sm->alphabet);
-            if (id < 0) return SA_E_ALPHABET;
-            pt.ids.push_back((int32_t) id);
-            pt.kmers.insert(pt.kmers.end(), buf, buf + k);
+            const int64_t pid = kmer_id_of(buf, k, sm->alphabet);
+            if (pid < 0) return SA_E_ALPHABET;
+            pt.ids.push_back((int32_t) pid);
         }
     }
     pt.first[lX + 1] = (int32_t) pt.ids.size();

@@ -112,7 +112,6 @@ struct PathTable {
     bool multi = false;              // some column has more than one path
     std::vector<int32_t> first;      // lX + 1 entries; column x's paths are ids[first[x] .. first[x+1])
     std::vector<int32_t> ids;        // k-mer ids; column 0 holds the NULL path (-1)
-    std::vector<char> kmers;         // k chars per path (for the legality test)
 };
 
 const char *degenerate_options(int32_t degenerate);
