@@ -296,13 +296,21 @@ typedef struct {
     double *event_expectations;   /* n_kmers x 2: weighted descaled event means, weighted spread */
     double *posteriors;           /* n_kmers: weights */
     uint8_t *observed;            /* n_kmers */
+    /* HDP machine (hdpHmm_makeExpectationsHmm, continuousHmm.c:788-795): no emission expectations;
+     * for each match transition whose posterior reaches the parameters' threshold, the path k-mer id
+     * and the event's index in this read (cell_signal_updateExpectationsAndAssignments,
+     * pairwiseAligner.c:795-817), this call's only, in the reference's order, up to
+     * assignment_capacity (SA_E_OUTPUT beyond it; n_assignments is the count) */
+    int64_t *assignment_kmers;
+    int64_t *assignment_events;
+    int64_t assignment_capacity;
+    int64_t n_assignments;
 } sa_expectations;
 
 /* getExpectationsUsingAnchors with diagonalCalculation_Expectations (pairwiseAligner.c:1255-1275,
  * cell_signal_updateExpectations :763-793) on the plain FP64 form: the read's regions run in order in
  * one CTA; every transition posterior of the window's anti-diagonals is added in the reference's
- * order.  Gaussian machines (SA_THREE_STATE) and canonical references only (SA_E_UNSUPPORTED
- * otherwise). */
+ * order.  Canonical references only (SA_E_UNSUPPORTED for 'X'). */
 sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm, const char *reference, int64_t reference_length,
                                          const double *events, int64_t n_events, const int64_t *anchors,
                                          int64_t n_anchors, const sa_params *p, int32_t ragged_left,

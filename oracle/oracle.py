@@ -73,7 +73,7 @@ def lib():
         L.orc_expectations.restype = C.c_int
         L.orc_expectations.argtypes = [C.POINTER(_Model), C.c_char_p, C.c_int64, _f64p, C.c_int64, _i64p,
                                        C.c_int64, C.POINTER(_Params), C.c_int, C.c_int, _f64p, _f64p, _f64p, _f64p,
-                                       C.POINTER(C.c_uint8)]
+                                       C.POINTER(C.c_uint8), _i64p, _i64p, C.c_int64, _i64p]
         L.orc_emission.restype = C.c_double
         L.orc_emission.argtypes = [C.POINTER(_Model), C.c_int64, C.c_double, C.c_double, C.c_int]
         L.orc_log_gauss_pdf.restype = C.c_double
@@ -199,7 +199,9 @@ def expectations(om, ref, events, anchors, p, ragged_left=True, ragged_right=Tru
     """getExpectationsUsingAnchors (pairwiseAligner.c:1983-2003) with diagonalCalculation_Expectations
     into a continuous pair HMM (continuousPairHmm_construct's pseudocounts, continuousHmm.c:84-141).
     state: a previous result to accumulate into.  Returns dict(likelihood, transitions (3x3),
-    event_expectations (n_kmers x 2), posteriors (n_kmers), observed (n_kmers))."""
+    event_expectations (n_kmers x 2), posteriors (n_kmers), observed (n_kmers), assignments ((k-mer id,
+    event index) rows: the HDP machine's instead of the emission expectations,
+    cell_signal_updateExpectationsAndAssignments, pairwiseAligner.c:795-817))."""
     k = om.model["kmer_length"]
     n = om.model["n_kmers"]
     lX = max(len(ref) - (k - 1), 0) if len(ref) > 0 else 0
@@ -208,8 +210,14 @@ def expectations(om, ref, events, anchors, p, ragged_left=True, ragged_right=Tru
     if state is None:
         state = dict(likelihood=0.0, transitions=np.full((3, 3), transition_pseudocount),
                      event_expectations=np.zeros((n, 2)), posteriors=np.full(n, emission_pseudocount),
-                     observed=np.zeros(n, np.uint8))
+                     observed=np.zeros(n, np.uint8), assignments=np.zeros((0, 2), np.int64))
     st = {key: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for key, v in state.items()}
+    cap = len(st["assignments"]) + 4 * (lX + len(ev)) + 64
+    ak = np.zeros(cap, np.int64)
+    ae = np.zeros(cap, np.int64)
+    ak[:len(st["assignments"])] = st["assignments"][:, 0]
+    ae[:len(st["assignments"])] = st["assignments"][:, 1]
+    na = C.c_int64(len(st["assignments"]))
     ll = np.array([st["likelihood"]], np.float64)
     tr = np.ascontiguousarray(st["transitions"], dtype=np.float64)
     ee = np.ascontiguousarray(st["event_expectations"], dtype=np.float64)
@@ -218,10 +226,14 @@ def expectations(om, ref, events, anchors, p, ragged_left=True, ragged_right=Tru
     ps = _params_struct(p)
     rc = lib().orc_expectations(C.byref(om.s), ref.encode(), lX, _p(ev, C.c_double), len(ev), _p(a, C.c_int64), len(a),
                                 C.byref(ps), int(ragged_left), int(ragged_right), _p(ll, C.c_double),
-                                _p(tr, C.c_double), _p(ee, C.c_double), _p(po, C.c_double), _p(ob, C.c_uint8))
+                                _p(tr, C.c_double), _p(ee, C.c_double), _p(po, C.c_double), _p(ob, C.c_uint8),
+                                _p(ak, C.c_int64), _p(ae, C.c_int64), cap, C.byref(na))
     if rc:
         raise OracleError("orc_expectations rc=%d" % rc)
-    return dict(likelihood=float(ll[0]), transitions=tr, event_expectations=ee, posteriors=po, observed=ob)
+    if na.value > cap:
+        raise OracleError("orc_expectations: assignment capacity")
+    return dict(likelihood=float(ll[0]), transitions=tr, event_expectations=ee, posteriors=po, observed=ob,
+                assignments=np.column_stack([ak[:na.value], ae[:na.value]]))
 
 
 def full_matrix(om, ref, events, threshold, ragged_left=False, ragged_right=False, options="CEO", p_mode=0):

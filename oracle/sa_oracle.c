@@ -564,6 +564,11 @@ typedef struct {
     double *event_exp;          /* n_kmers x 2 */
     double *posteriors;         /* n_kmers */
     unsigned char *observed;    /* n_kmers */
+    /* HDP machine (hdpHmm_makeExpectationsHmm, continuousHmm.c:788-795): instead of the emission
+     * expectations, the (k-mer, event) of every match transition with posterior >= threshold */
+    int hdp;
+    double threshold;
+    int64_t *assign_kmer, *assign_event, assign_cap, n_assign;
 } orc_expect;
 
 /* cell_signal_updateExpectations (pairwiseAligner.c:763-793): one transition of the cell's
@@ -571,10 +576,19 @@ typedef struct {
  * emission expectation (continuousPairHmm_addToEmissionExpectation, continuousHmm.c:160-169: the
  * spread uses the running mean, so the order of the updates matters) */
 static void orc_expect_update(const orc_model *m, orc_expect *ex, double from_v, double to_v, int from, int to,
-                              double e, double t, double total, int64_t kmer, const double *ev) {
+                              double e, double t, double total, int64_t kmer, const double *ev, int64_t event) {
     double p = exp(from_v + to_v + (e + t) - total);
     ex->transitions[from * 3 + to] += p;
-    if (to == S_MATCH) {
+    if (to == S_MATCH && ex->hdp) {
+        /* cell_signal_updateExpectationsAndAssignments (pairwiseAligner.c:795-817) */
+        if (p >= ex->threshold) {
+            if (ex->n_assign < ex->assign_cap) {
+                ex->assign_kmer[ex->n_assign] = kmer;
+                ex->assign_event[ex->n_assign] = event;
+            }
+            ex->n_assign++;
+        }
+    } else if (to == S_MATCH) {
         double mu = m->match[kmer * 5];
         double x = (ev[0] + m->var * mu - m->scale * mu - m->shift) / m->var;
         ex->event_exp[2 * kmer] += p * x;
@@ -592,7 +606,8 @@ static void orc_expect_update(const orc_model *m, orc_expect *ex, double from_v,
  * posterior use (pairwiseAligner.c:1384-1387), so in a window traced back to T the middle
  * neighbours of xay = T+1 (F[T-1]) are gone and their transitions are skipped.  Single-path cells
  * only. */
-static void orc_expect_diag(orc_dp *dp, int64_t xay, double total, orc_expect *ex, int64_t traced_back_to) {
+static void orc_expect_diag(orc_dp *dp, int64_t xay, double total, orc_expect *ex, int64_t traced_back_to,
+                            int64_t oy) {
     const orc_model *m = dp->m;
     const orc_paths *P = dp->P;
     const double *t = m->t;
@@ -608,20 +623,20 @@ static void orc_expect_diag(orc_dp *dp, int64_t xay, double total, orc_expect *e
         const double *ev = orc_event(dp, y);
         if (lo) {
             double e = orc_emit_gapx(m, kid);
-            orc_expect_update(m, ex, lo[S_MATCH], cur[S_GAPX], S_MATCH, S_GAPX, e, t[T_GAP_OPEN_X], total, kid, ev);
-            orc_expect_update(m, ex, lo[S_GAPX], cur[S_GAPX], S_GAPX, S_GAPX, e, t[T_GAP_EXTEND_X], total, kid, ev);
-            orc_expect_update(m, ex, lo[S_GAPY], cur[S_GAPX], S_GAPY, S_GAPX, e, t[T_GAP_SWITCH_TO_X], total, kid, ev);
+            orc_expect_update(m, ex, lo[S_MATCH], cur[S_GAPX], S_MATCH, S_GAPX, e, t[T_GAP_OPEN_X], total, kid, ev, y - 1 + oy);
+            orc_expect_update(m, ex, lo[S_GAPX], cur[S_GAPX], S_GAPX, S_GAPX, e, t[T_GAP_EXTEND_X], total, kid, ev, y - 1 + oy);
+            orc_expect_update(m, ex, lo[S_GAPY], cur[S_GAPX], S_GAPY, S_GAPX, e, t[T_GAP_SWITCH_TO_X], total, kid, ev, y - 1 + oy);
         }
         if (mi) {
             double e = orc_emit_event(m, kid, ev, 1);
-            orc_expect_update(m, ex, mi[S_MATCH], cur[S_MATCH], S_MATCH, S_MATCH, e, t[T_MATCH_CONTINUE], total, kid, ev);
-            orc_expect_update(m, ex, mi[S_GAPX], cur[S_MATCH], S_GAPX, S_MATCH, e, t[T_MATCH_FROM_GAP_X], total, kid, ev);
-            orc_expect_update(m, ex, mi[S_GAPY], cur[S_MATCH], S_GAPY, S_MATCH, e, t[T_MATCH_FROM_GAP_Y], total, kid, ev);
+            orc_expect_update(m, ex, mi[S_MATCH], cur[S_MATCH], S_MATCH, S_MATCH, e, t[T_MATCH_CONTINUE], total, kid, ev, y - 1 + oy);
+            orc_expect_update(m, ex, mi[S_GAPX], cur[S_MATCH], S_GAPX, S_MATCH, e, t[T_MATCH_FROM_GAP_X], total, kid, ev, y - 1 + oy);
+            orc_expect_update(m, ex, mi[S_GAPY], cur[S_MATCH], S_GAPY, S_MATCH, e, t[T_MATCH_FROM_GAP_Y], total, kid, ev, y - 1 + oy);
         }
         if (up) {
             double e = orc_emit_event(m, kid, ev, 0);
-            orc_expect_update(m, ex, up[S_MATCH], cur[S_GAPY], S_MATCH, S_GAPY, e, t[T_GAP_OPEN_Y], total, kid, ev);
-            orc_expect_update(m, ex, up[S_GAPY], cur[S_GAPY], S_GAPY, S_GAPY, e, t[T_GAP_EXTEND_Y], total, kid, ev);
+            orc_expect_update(m, ex, up[S_MATCH], cur[S_GAPY], S_MATCH, S_GAPY, e, t[T_GAP_OPEN_Y], total, kid, ev, y - 1 + oy);
+            orc_expect_update(m, ex, up[S_GAPY], cur[S_GAPY], S_GAPY, S_GAPY, e, t[T_GAP_EXTEND_Y], total, kid, ev, y - 1 + oy);
         }
     }
 }
@@ -718,7 +733,7 @@ static int orc_banded_region(const orc_model *m, const char *seq, int64_t lX, co
                         (*n_tp)++;
                     }
                 }
-                if (ex) orc_expect_diag(&dp, d2, total, ex, traced_back_to);
+                if (ex) orc_expect_diag(&dp, d2, total, ex, traced_back_to, oy);
                 else rc = orc_posteriors(&dp, d2, total, p->threshold, out, n_out, max_out, ox, oy);
                 if (rc) goto done;
             }
@@ -759,8 +774,15 @@ int orc_aligned_pairs(const orc_model *m, const char *seq, int64_t lX, const dou
 int orc_expectations(const orc_model *m, const char *seq, int64_t lX, const double *events, int64_t lY,
                      const int64_t *anchors, int64_t n_anchors, const orc_params *p, int ragged_left,
                      int ragged_right, double *likelihood, double *transitions, double *event_exp,
-                     double *posteriors, unsigned char *observed) {
+                     double *posteriors, unsigned char *observed, int64_t *assign_kmer, int64_t *assign_event,
+                     int64_t assign_cap, int64_t *n_assign) {
     orc_expect ex;
+    ex.hdp = m->emission == ORC_EMIT_HDP;
+    ex.threshold = p->threshold;
+    ex.assign_kmer = assign_kmer;
+    ex.assign_event = assign_event;
+    ex.assign_cap = assign_cap;
+    ex.n_assign = *n_assign;
     ex.likelihood = *likelihood;
     for (int i = 0; i < 9; i++) ex.transitions[i] = transitions[i];
     ex.event_exp = event_exp;
@@ -771,6 +793,7 @@ int orc_expectations(const orc_model *m, const char *seq, int64_t lX, const doub
                            &n_out, NULL, 0, NULL, &ex);
     *likelihood = ex.likelihood;
     for (int i = 0; i < 9; i++) transitions[i] = ex.transitions[i];
+    *n_assign = ex.n_assign;
     return rc;
 }
 

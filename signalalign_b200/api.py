@@ -77,7 +77,9 @@ class ParamRead(C.Structure):
 class Expectations(C.Structure):
     _fields_ = [("likelihood", C.c_double), ("transitions", C.c_double * 9),
                 ("event_expectations", C.POINTER(C.c_double)), ("posteriors", C.POINTER(C.c_double)),
-                ("observed", C.POINTER(C.c_uint8))]
+                ("observed", C.POINTER(C.c_uint8)), ("assignment_kmers", C.POINTER(C.c_int64)),
+                ("assignment_events", C.POINTER(C.c_int64)), ("assignment_capacity", C.c_int64),
+                ("n_assignments", C.c_int64)]
 
 
 class OutputRead(C.Structure):
@@ -725,12 +727,12 @@ def getExpectationsUsingAnchors(sm, reference, events, anchors, p, ragged_left=T
     """Expectations of one read on the plain FP64 form, accumulated into `state` (a previous result)
     or into fresh accumulators with the given pseudocounts (hmmContinuous_getExpectationsHmm).
     Returns dict(likelihood, transitions (3x3), event_expectations (n_kmers x 2), posteriors,
-    observed)."""
+    observed, assignments ((k-mer id, event index) rows, the HDP machine's))."""
     n = sm.n_kmers
     if state is None:
         state = dict(likelihood=0.0, transitions=np.full((3, 3), transition_pseudocount),
                      event_expectations=np.zeros((n, 2)), posteriors=np.full(n, emission_pseudocount),
-                     observed=np.zeros(n, np.uint8))
+                     observed=np.zeros(n, np.uint8), assignments=np.zeros((0, 2), np.int64))
     ee = np.ascontiguousarray(state["event_expectations"], dtype=np.float64).copy()
     po = np.ascontiguousarray(state["posteriors"], dtype=np.float64).copy()
     ob = np.ascontiguousarray(state["observed"], dtype=np.uint8).copy()
@@ -741,11 +743,20 @@ def getExpectationsUsingAnchors(sm, reference, events, anchors, p, ragged_left=T
     ex.event_expectations = ee.ctypes.data_as(_f64p)
     ex.posteriors = po.ctypes.data_as(_f64p)
     ex.observed = ob.ctypes.data_as(C.POINTER(C.c_uint8))
+    cap = 4 * (len(reference) + len(events)) + 64
+    ak = np.zeros(cap, np.int64)
+    ae = np.zeros(cap, np.int64)
+    ex.assignment_kmers = ak.ctypes.data_as(_i64p)
+    ex.assignment_events = ae.ctypes.data_as(_i64p)
+    ex.assignment_capacity = cap
     ev = _f64(events, 4)
     a = _anchors(anchors)
     ref = reference.encode()
     _check(lib().sa_getExpectationsUsingAnchors(sm.handle, ref, len(ref), ev.ctypes.data_as(_f64p), len(ev),
                                                 a.ctypes.data_as(_i64p), len(a), C.byref(p), int(ragged_left),
                                                 int(ragged_right), C.byref(ex)), "getExpectationsUsingAnchors")
+    got = np.column_stack([ak[:ex.n_assignments], ae[:ex.n_assignments]])
     return dict(likelihood=ex.likelihood, transitions=np.array(list(ex.transitions)).reshape(3, 3),
-                event_expectations=ee, posteriors=po, observed=ob)
+                event_expectations=ee, posteriors=po, observed=ob,
+                assignments=np.concatenate([np.asarray(state.get("assignments", np.zeros((0, 2), np.int64)),
+                                                       dtype=np.int64).reshape(-1, 2), got]))

@@ -40,6 +40,7 @@ struct Region64 {
     int32_t lX, lY, n, n_windows;
     int32_t ragged_left, ragged_right;
     int32_t model, ring, stride, pad;
+    int64_t ev_base;              // the region's first event in the read (split regions start later)
     const int32_t *xl, *xr;
     const int32_t *pfirst, *pid, *ppre, *psuf;
     const double2 *ev;
@@ -68,6 +69,11 @@ struct ExpectOut {
     double *event_exp;          // per k-mer: weighted mean sum, weighted spread sum
     double *posteriors;         // per k-mer: weight
     unsigned char *observed;    // per k-mer
+    // HDP machine: (k-mer, event) of each match transition with posterior >= threshold instead
+    int32_t hdp, pad;
+    double threshold;
+    int64_t *assign_kmer, *assign_event, *n_assign;
+    int64_t assign_cap;
 };
 
 // the 3 states of path q in the cell of anti-diagonal d (q must belong to that cell's column)
@@ -292,6 +298,18 @@ __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const Expec
                 for (int j = 0; j < 3; ++j) {
                     const double p = ps[3 + j];
                     acc[1 + j * 3 + S_M] += p;
+                    if (X.hdp) {
+                        // cell_signal_updateExpectationsAndAssignments (pairwiseAligner.c:795-817)
+                        if (p >= X.threshold) {
+                            const int64_t at = *X.n_assign;
+                            if (at < X.assign_cap) {
+                                X.assign_kmer[at] = kid;
+                                X.assign_event[at] = R.ev_base + y - 1;
+                            }
+                            *X.n_assign = at + 1;
+                        }
+                        continue;
+                    }
                     X.event_exp[2 * kid] += p * xe;
                     X.posteriors[kid] += p;
                     const double uk = X.event_exp[2 * kid] / X.posteriors[kid];
@@ -557,6 +575,7 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
             r.ragged_left = pr.rg.ragged_left;
             r.ragged_right = pr.rg.ragged_right;
             r.model = pr.model;
+            r.ev_base = pr.rg.y1;
             r.threshold = s->threshold;
             r.ring = pr.ring;
             r.stride = pr.stride;
@@ -916,7 +935,9 @@ extern "C" sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm_c
     auto *sm = const_cast<sa_state_machine *>(sm_c);
     // the continuous pair HMM of the Gaussian machine (hmmContinuous_getExpectationsHmm,
     // continuousHmm.c:842-857); the HDP machine collects assignments instead
-    if (sm->type != SA_THREE_STATE || sm->emission == SA_EMIT_HDP) return SA_E_UNSUPPORTED;
+    const bool hdp = sm->emission == SA_EMIT_HDP;
+    if (hdp && (!sm->hdp.present || (ex->assignment_capacity > 0 && (!ex->assignment_kmers || !ex->assignment_events))))
+        return hdp && !sm->hdp.present ? SA_E_UNSUPPORTED : SA_E_ARG;
     sa_status st = check_params(*p);
     if (st) return st;
     sa_read rd;
@@ -956,7 +977,10 @@ extern "C" sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm_c
     auto up = [](size_t v) { return (v + 255) & ~(size_t) 255; };
     const size_t o_mask = up(sizeof(double) * 8 * (size_t) width), o_acc = o_mask + up(sizeof(int32_t) * width);
     const size_t o_ee = o_acc + up(sizeof(double) * 10), o_po = o_ee + up(sizeof(double) * 2 * nk);
-    const size_t o_ob = o_po + up(sizeof(double) * nk), total = o_ob + up((size_t) nk);
+    const int64_t acap = hdp ? std::max<int64_t>(ex->assignment_capacity, 0) : 0;
+    const size_t o_ob = o_po + up(sizeof(double) * nk), o_ak = o_ob + up((size_t) nk);
+    const size_t o_ae = o_ak + up(sizeof(int64_t) * std::max<int64_t>(acap, 1));
+    const size_t o_na = o_ae + up(sizeof(int64_t) * std::max<int64_t>(acap, 1)), total = o_na + up(sizeof(int64_t));
     MemBlock blk;
     st = plain_upload(s, nullptr);
     if (!st) st = mem_get(MemKind::Device, s->device, total, blk);
@@ -968,10 +992,18 @@ extern "C" sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm_c
         if (cudaMemcpy(d + o_acc, acc, sizeof(acc), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(d + o_ee, ex->event_expectations, sizeof(double) * 2 * nk, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(d + o_po, ex->posteriors, sizeof(double) * nk, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(d + o_ob, ex->observed, (size_t) nk, cudaMemcpyHostToDevice) != cudaSuccess)
+            cudaMemcpy(d + o_ob, ex->observed, (size_t) nk, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(d + o_na, 0, sizeof(int64_t)) != cudaSuccess)
             st = SA_E_CUDA;
         ExpectOut X;
+        std::memset(&X, 0, sizeof(X));
         X.on = 1;
+        X.hdp = hdp ? 1 : 0;
+        X.threshold = p->threshold;
+        X.assign_kmer = reinterpret_cast<int64_t *>(d + o_ak);
+        X.assign_event = reinterpret_cast<int64_t *>(d + o_ae);
+        X.n_assign = reinterpret_cast<int64_t *>(d + o_na);
+        X.assign_cap = acap;
         X.n_regions = (int32_t) s->regs.size();
         X.scratch = reinterpret_cast<double *>(d);
         X.mask = reinterpret_cast<int32_t *>(d + o_mask);
@@ -999,6 +1031,18 @@ extern "C" sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm_c
                 st = SA_E_CUDA;
             ex->likelihood = acc[0];
             for (int i = 0; i < 9; ++i) ex->transitions[i] = acc[i + 1];
+            int64_t na = 0;
+            if (cudaMemcpy(&na, d + o_na, sizeof(na), cudaMemcpyDeviceToHost) != cudaSuccess) st = SA_E_CUDA;
+            ex->n_assignments = na;
+            if (!st && hdp) {
+                const int64_t got = std::min(na, acap);
+                if (got > 0 && (cudaMemcpy(ex->assignment_kmers, d + o_ak, sizeof(int64_t) * got,
+                                           cudaMemcpyDeviceToHost) != cudaSuccess ||
+                                cudaMemcpy(ex->assignment_events, d + o_ae, sizeof(int64_t) * got,
+                                           cudaMemcpyDeviceToHost) != cudaSuccess))
+                    st = SA_E_CUDA;
+                if (!st && na > acap) st = SA_E_OUTPUT;
+            }
         }
     }
     mem_put(blk);

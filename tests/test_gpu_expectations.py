@@ -87,13 +87,27 @@ def test_expectations_unsupported_inputs(api):
     with pytest.raises(api.SAError) as ei:
         api.getExpectationsUsingAnchors(sm, ref, rd["events"], rd["anchors"], _p(api))
     assert ei.value.status == 2   # SA_E_ALPHABET
-    # the HDP machine's expectations are assignments for its sampler, not a continuous pair HMM
+
+
+
+@pytest.mark.parametrize("split", [3000 * 3000, 2000])
+def test_expectations_hdp_assignments(api, split):
+    """the HDP machine: transition expectations and, instead of emission expectations, the (k-mer,
+    event) assignments of match transitions at or above the threshold, in the reference's order
+    (cell_signal_updateExpectationsAndAssignments, pairwiseAligner.c:795-817); with split regions the
+    event indices stay read-level"""
+    from oracle import formats
     hc = W.small_hdp_config()
     hdp = W.hdp_dict(hc["hdp"], len(hc["alphabet"]) ** hc["k"])
-    from oracle import formats
     hm = formats.parse_model_lines(*synth.model_text(hc["alphabet"], hc["k"], hc["table"]).split("\n")[:3])
-    hrd = hc["reads"][0]
-    smh = W.gpu_model(api, hm, orc.EMIT_HDP, hrd, hdp)
-    with pytest.raises(api.SAError) as ei:
-        api.getExpectationsUsingAnchors(smh, hrd["reference"], hrd["events"], hrd["anchors"], _p(api))
-    assert ei.value.status == 7   # SA_E_UNSUPPORTED
+    p = _p(api, split_matrix_bigger_than_this=split)
+    got = want = None
+    for rd in hc["reads"][:2]:
+        om = W.oracle_model(hm, orc.EMIT_HDP, rd, hdp)
+        want = orc.expectations(om, rd["reference"], rd["events"], rd["anchors"], _op(p), state=want)
+        smh = W.gpu_model(api, hm, orc.EMIT_HDP, rd, hdp)
+        got = api.getExpectationsUsingAnchors(smh, rd["reference"], rd["events"], rd["anchors"], p, state=got)
+    assert got["likelihood"] == pytest.approx(want["likelihood"], rel=1e-12)
+    np.testing.assert_allclose(got["transitions"], want["transitions"], rtol=RTOL)
+    assert len(want["assignments"]) > 500
+    assert np.array_equal(got["assignments"], want["assignments"])
