@@ -429,35 +429,39 @@ def main():
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_seq_value = cells * world / (float(te.item()) / 1e3)
 
-    # e2e, pipelined: the same public calls on a stream of batches, as a pipeline uses them: batch k+1
-    # is planned on the host and uploaded on a copy stream while batch k's kernels run, batch k-1 is
-    # downloaded on the copy stream; events order the copies against the kernels.  Every batch's
-    # planning, H2D, kernels and D2H are inside the timed region.
-    copy_stream = torch.cuda.Stream()
-    cptr = copy_stream.cuda_stream
+    # e2e, pipelined: the same public calls on a stream of batches, as a pipeline uses them, three
+    # batches in flight: batch k is planned on the host and uploaded on an H2D stream while batch
+    # k-1's kernels run, and batch k-2 is downloaded on a D2H stream; events order the copies against
+    # the kernels.  Every batch's planning, H2D, kernels and D2H are inside the timed region.
+    h2d_stream, d2h_stream = torch.cuda.Stream(), torch.cuda.Stream()
+    hptr, dptr = h2d_stream.cuda_stream, d2h_stream.cuda_stream
 
     def pipeline(n):
-        prev = prev_done = None
+        inflight = []   # (batch, its kernels' completion event), oldest first
         for _ in range(n):
             cur = api.Batch(reads, p)
-            cur.upload(cptr)
+            cur.upload(hptr)
             uploaded = torch.cuda.Event()
-            uploaded.record(copy_stream)
+            uploaded.record(h2d_stream)
             stream.wait_event(uploaded)
             cur.run(sptr)
             done = torch.cuda.Event()
             done.record(stream)
-            if prev is not None:
-                copy_stream.wait_event(prev_done)
-                prev.download(cptr)
-                del prev
-            prev, prev_done = cur, done
-        copy_stream.wait_event(prev_done)
-        prev.download(cptr)
+            inflight.append((cur, done))
+            if len(inflight) > 2:
+                old, old_done = inflight.pop(0)
+                d2h_stream.wait_event(old_done)
+                old.download(dptr)
+                del old
+        while inflight:
+            old, old_done = inflight.pop(0)
+            d2h_stream.wait_event(old_done)
+            old.download(dptr)
+            del old
         torch.cuda.synchronize()
 
-    pipeline(2)   # untimed: the memory pools then hold the two batches' blocks a pipeline alternates
-    n_pipe = max(3, min(args.steps, 6))
+    pipeline(3)   # untimed: the memory pools then hold the blocks of the three batches in flight
+    n_pipe = 8   # a stream of 8 batches, pipeline fill and drain included
     barrier()
     t0 = time.perf_counter()
     pipeline(n_pipe)
@@ -518,9 +522,10 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": float(tp.item()),
                         "includes": "host planning (bands, windows, k-mer ids), H2D, launch, D2H of all pairs",
-                        "mode": "pipelined through sa_batch_create/upload/run/download: batch k+1 planned on the "
-                                "host and uploaded on a copy stream while batch k's kernels run, batch k-1 "
-                                "downloaded on the copy stream (events order copies and kernels)",
+                        "mode": "pipelined through sa_batch_create/upload/run/download, three batches in flight: "
+                                "batch k planned on the host and uploaded on an H2D stream while batch k-1's "
+                                "kernels run, batch k-2 downloaded on a D2H stream (events order copies and "
+                                "kernels)",
                         "sequential": {"value": e2e_seq_value, "ms_per_step": float(te.item()),
                                        "mode": "one synchronous sa_align_batch call per step"}},
                 "plain_fp64": {"value": plain_value, "unit": UNIT, "sample": "%d reads, one launch per read" % len(sample),
