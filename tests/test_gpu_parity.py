@@ -359,3 +359,25 @@ def test_batch_degenerate_reads_run_in_plain_form(api):
         else:
             assert W.max_posterior_error(want, b.pairs(i), p.threshold) <= FP32_TOL
     assert n_multi == len(deg)
+
+
+def test_batch_only_degenerate_reads_and_empty_batch(api):
+    """a batch whose every read has degenerate positions (no FP32 work: the plain form alone) gives
+    the single-read entry's pairs; an empty batch plans, runs and downloads nothing"""
+    cfg = synth.config3(seed=8, n_reads=1, span=(400, 600), grid_length=200, route="degenerate")
+    gm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["gauss_table"]).split("\n")[:3])
+    als = [a for a in cfg["alignments"] if a["model"] == "gauss"]
+    p = _p(api)
+    inputs = []
+    for a in als:
+        sm = W.gpu_model(api, gm, orc.EMIT_DESCALED, a)
+        inputs.append(api.ReadInput(sm=sm, reference=a["reference"], events=a["events"], anchors=a["anchors"],
+                                    scale=a["scale"], shift=a["shift"], degenerate=DEGENERATE["CE"]))
+    b = api.align_batch(inputs, p)
+    for i, a in enumerate(als):
+        assert b.status(i) == 0
+        alone = api.getAlignedPairsUsingAnchors(inputs[i].sm, a["reference"], a["events"], a["anchors"], p,
+                                                degenerate=DEGENERATE["CE"])
+        assert len(alone) > 50 and np.array_equal(alone, b.pairs(i))
+    empty = api.align_batch([], p)
+    assert empty.cells == 0

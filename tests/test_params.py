@@ -103,3 +103,18 @@ def test_estimate_params_batch_matches_oracle(api, model):
         assert p["scale"] == pytest.approx(tr["scale"], rel=0.02)
         assert p["shift"] == pytest.approx(tr["shift"], abs=1.5)
         assert p["drift"] == pytest.approx(tr["drift"], abs=0.2)
+
+
+@pytest.mark.gpu
+def test_estimate_params_read_without_assignments(api, model):
+    """a strand shorter than one k-mer has no assignments: the reference aborts, the batch marks that
+    read SA_E_ARG and still fits the others"""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    table = np.asarray(model["match"]).reshape(-1, 5)
+    sm = _sm(api, model)
+    read, em, ev = make_strand(30, table, length=2000)
+    got = api.estimateNanoporeParams([(sm, read[:4], em, ev, {}), (sm, read, em, ev, dict(var=1.0))])
+    assert got[0][0] == 1
+    assert got[1][0] == 0 and got[1][1]["scale"] == pytest.approx(1.03, rel=0.02)
