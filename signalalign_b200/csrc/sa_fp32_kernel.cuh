@@ -452,8 +452,11 @@ __device__ __forceinline__ void ring_init(float *base, int wmax) {
 // cell reads them from there; a chunk whose ranges exceed kEmitSpan reads global memory per cell.
 constexpr int kEmitWarps = 4;
 constexpr int kEmitSpan = 192;
+// The k-mer constants are staged as two float4 halves in separate arrays: lanes reading consecutive
+// columns then load 16-byte strides, which shared memory serves without bank conflicts (32-byte
+// records would put two lanes on every bank group).
 struct EmitStage {
-    KmerConst32 kc[kEmitSpan];
+    float4 kca[kEmitSpan], kcb[kEmitSpan];
     float4 ev[kEmitSpan];
     double mean[kEmitSpan];     // FP64 event means (HDP)
     int32_t kid[kEmitSpan];
@@ -533,7 +536,8 @@ __global__ void __launch_bounds__(32 * kEmitWarps) emission_kernel(const __grid_
                 const int32_t kid = ok ? __ldg(A.kmer + c.R.kmer_base + x - 1) : 0;
                 const float4 *kp = reinterpret_cast<const float4 *>(c.M->kc + kid);
                 const float4 ka = __ldg(kp), kb = __ldg(kp + 1);
-                st.kc[q] = KmerConst32{ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
+                st.kca[q] = ka;
+                st.kcb[q] = kb;
                 st.kid[q] = kid;
             }
             for (int q = lane; q <= yhi - ylo; q += 32) {
@@ -554,7 +558,9 @@ __global__ void __launch_bounds__(32 * kEmitWarps) emission_kernel(const __grid_
                 const bool ok = x >= 1 && x <= c.R.lX && y >= 1 && y <= c.R.lY;
                 float em, ey;
                 if (staged) {
-                    emit_cell(c, st.kc[x - xlo], st.kid[x - xlo], st.ev[y - ylo], c.hdp ? st.mean[y - ylo] : 0.0, ok,
+                    const float4 ka = st.kca[x - xlo], kb = st.kcb[x - xlo];
+                    const KmerConst32 kk{ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
+                    emit_cell(c, kk, st.kid[x - xlo], st.ev[y - ylo], c.hdp ? st.mean[y - ylo] : 0.0, ok,
                               em, ey);
                 } else {
                     const int32_t kid = ok ? __ldg(A.kmer + c.R.kmer_base + x - 1) : 0;
