@@ -490,8 +490,21 @@ def main():
             with open(mp) as fh:
                 hbm_peak, hbm_src = float(json.load(fh).get("hbm_gbs", hbm_peak)), "measured"
         em_gbs = EMISSION_BYTES_PER_CELL * cells / (em_ms / 1e3) / 1e9
-        # the sequential chain: the longest region's anti-diagonals bound the worker from below
-        longest = max(len(rd["reference"]) - 5 + len(rd["events"]) for rd in cfg["reads"])
+        # the sequential chain: the longest region's anti-diagonals bound the worker from below.  The
+        # bound is measured: the same read alone in a batch (its forward sweep alone on its SM, its
+        # windows served by two more CTAs) takes the worker's floor for this batch.
+        chain = [len(rd["reference"]) - 5 + len(rd["events"]) for rd in cfg["reads"]]
+        longest = max(chain)
+        lb = api.Batch([reads[int(np.argmax(chain))]], p)
+        lb.upload(sptr)
+        alone = []
+        for i in range(5):
+            lb.run(sptr)
+            torch.cuda.synchronize()
+            if i >= 2:
+                alone.append(lb.kernel_ms()[1])
+        alone_ms = min(alone)
+        del lb
         # plain FP64 form, one read per launch, on a sample of the batch
         order = np.argsort([len(rd["events"]) for rd in cfg["reads"]])
         sample = [int(i) for i in order[::max(1, len(order) // 8)][:8]]
@@ -543,7 +556,10 @@ def main():
                                       "note": "%.0f B written per band cell" % EMISSION_BYTES_PER_CELL},
                 "critical_path": {"longest_region_antidiagonals": longest,
                                   "worker_ns_per_antidiagonal": wk_ms * 1e6 / longest,
-                                  "note": "the forward sweep of one region is sequential over its anti-diagonals"},
+                                  "alone_worker_ms": alone_ms, "frac": alone_ms / wk_ms,
+                                  "note": "the forward sweep of one region is sequential over its anti-diagonals; "
+                                          "alone_worker_ms is the worker kernel on the longest read alone (the "
+                                          "batch's latency bound), frac = alone / batch worker time"},
                 "gpu_launches": launches, "clocks": clocks}
     if world > 1:
         dist.barrier()
