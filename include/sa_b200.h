@@ -316,6 +316,32 @@ sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm, const char 
                                          int64_t n_anchors, const sa_params *p, int32_t ragged_left,
                                          int32_t ragged_right, sa_expectations *ex);
 
+/* The EM maximisation step (continuousPairHmm_normalize, continuousHmm.c:283-306): the transitions
+ * divided by their row sums in place (hmmDiscrete_normalizeTransitions, discreteHmm.c:125-137); with
+ * an event model (n_kmers rows of 5, the machine's match table when the expectations were made, as
+ * continuousPairHmm_makeExpectationsHmm copies it, :201-212), each observed k-mer's level mean and
+ * sd become sum(p * e) / sum(p) and sqrt(spread / sum(p)), a zero keeping the previous value.
+ * event_model NULL: transitions only (the HDP machine's step). */
+sa_status sa_normalizeExpectations(sa_expectations *ex, int64_t n_kmers, double *event_model);
+
+/* continuousPairHmm_loadTransitionsIntoStateMachine (continuousHmm.c:321-339): the machine's nine
+ * transitions become the logs of the normalised ones (gap-X -> gap-Y stays LOG_ZERO; gap-Y -> gap-X
+ * becomes log(transitions[7])).  With an event model, continuousPairHmm_loadEmissionsIntoStateMachine
+ * (:341-352) too (Gaussian machines only): match table level means and sds, gap-Y sds x 1.75, and
+ * the gap-Y means at the index the reference writes them to (i + 5, not i * 5). */
+sa_status sa_stateMachine_loadExpectations(sa_state_machine *sm, const double transitions[9],
+                                           const double *event_model);
+
+/* hmmContinuous_writeToFile (continuousHmm.c:872-884): continuousPairHmm_writeToFile (:354-406) for
+ * the Gaussian machine, hdpHmm_writeToFile (:572-628) for the HDP machine (its assignments: the events'
+ * means from `events`, rows of 4, and the k-mers), byte for byte; empty when a transition is NaN.
+ * event_model NULL: the machine's match table.  The text is malloc'd (free with sa_free_text);
+ * sa_writeExpectations writes it to `path` (opened with "w"). */
+sa_status sa_formatExpectations(const sa_state_machine *sm, const sa_expectations *ex, const double *event_model,
+                                const double *events, int64_t n_events, char **text, int64_t *length);
+sa_status sa_writeExpectations(const char *path, const sa_state_machine *sm, const sa_expectations *ex,
+                               const double *event_model, const double *events, int64_t n_events);
+
 /* ---- before the path: anchor pairs from the guide alignment (signalMachine.c:615, :343-344) ---- */
 
 /* one cigar operation of the guide alignment (AlignmentOperation of sonLib's PairwiseAlignment) */

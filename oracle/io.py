@@ -15,10 +15,17 @@ imports this).  Plain-Python restatements of the reference, line for line:
   nanopore_compute_noise_scale_params (:783-848), nanopore_adjustEventsForDriftP (:535-540): the
   fits of signalUtils_estimateNanoporeParams (impl/signalMachineUtils.c:186-223), sums in the
   reference's sequential order.
+* continuousPairHmm_normalize / hmmDiscrete_normalizeTransitions, the two
+  continuousPairHmm_load*IntoStateMachine calls and the expectations file writers
+  (impl/continuousHmm.c:283-406, :572-628; impl/discreteHmm.c:125-137): the EM maximisation step.
 
 The reverse complement is sonLib's stString_reverseComplementString (sonLib is not vendored in the
 reference tree): A/C/G/T in either case complemented, other characters kept.
 """
+
+import math
+
+import numpy as np
 
 MATCH, INDEL_X, INDEL_Y = 0, 1, 2
 PAIR_PROB_1 = 10000000.0
@@ -210,3 +217,86 @@ def estimate_params(assignments, model):
 
 def adjust_events_for_drift(events, drift):
     return [[e[0] - e[3] * drift, e[1], e[2], e[3]] for e in events]
+
+
+# ------------------------------------------------------------------------------------------------
+# EM maximisation step and the expectations file (impl/continuousHmm.c, impl/discreteHmm.c)
+# ------------------------------------------------------------------------------------------------
+LOG_ZERO = float("-inf")
+# StateMachine3 transition fields, in the order of oracle models' "t" (inc/stateMachine.h:153-163)
+T_MC, T_MFGX, T_MFGY, T_OX, T_OY, T_EX, T_EY, T_SX, T_SY = range(9)
+
+
+def normalize_transitions(transitions):
+    """hmmDiscrete_normalizeTransitions (discreteHmm.c:125-137): each row divided by its sum"""
+    t = [[float(v) for v in row] for row in transitions]
+    for f in range(3):
+        total = 0.0
+        for to in range(3):
+            total += t[f][to]
+        for to in range(3):
+            t[f][to] = t[f][to] / total
+    return t
+
+
+def normalize_expectations(transitions, event_expectations, posteriors, observed, event_model):
+    """continuousPairHmm_normalize (continuousHmm.c:283-306): the normalised transitions and the
+    event model (n_kmers rows of 5, the machine's match table when the expectations were made) with
+    each observed k-mer's level mean and sd replaced by the weighted mean and the root of the
+    weighted spread (kept where either is exactly 0)."""
+    em = [[float(v) for v in row] for row in event_model]
+    for i in range(len(em)):
+        if not observed[i]:
+            continue
+        w = float(posteriors[i])
+        u = float(event_expectations[i][0]) / w
+        o = (float(event_expectations[i][1]) / w) ** 0.5
+        em[i][0] = em[i][0] if u == 0.0 else u
+        em[i][1] = em[i][1] if o == 0.0 else o
+    return normalize_transitions(transitions), em
+
+
+def _log(v):
+    return math.log(v) if v > 0.0 else LOG_ZERO
+
+
+def load_expectations(model_t, match, gapy, transitions, event_model=None):
+    """continuousPairHmm_loadTransitionsIntoStateMachine (continuousHmm.c:321-339) and, given an
+    event model, continuousPairHmm_loadEmissionsIntoStateMachine (:341-352), which writes each
+    k-mer's mean into the gap-Y table at [i + 5] (not [i * 5]) and its sd x 1.75 at [i * 5 + 1].
+    Returns (t, match, gapy): a list and two arrays shaped like the inputs."""
+    t = list(model_t)
+    T = transitions
+    t[T_MC], t[T_OX], t[T_OY] = _log(T[0][0]), _log(T[0][1]), _log(T[0][2])
+    t[T_MFGX], t[T_EX], t[T_SY] = _log(T[1][0]), _log(T[1][1]), LOG_ZERO
+    t[T_MFGY], t[T_EY], t[T_SX] = _log(T[2][0]), _log(T[2][2]), _log(T[2][1])
+    shape = np.shape(match)
+    match = np.array(match, dtype=np.float64).reshape(-1)
+    gapy = np.array(gapy, dtype=np.float64).reshape(-1)
+    if event_model is not None:
+        for i, row in enumerate(event_model):
+            match[i * 5] = row[0]
+            match[i * 5 + 1] = row[1]
+            gapy[i + 5] = row[0]
+            gapy[i * 5 + 1] = row[1] * 1.75
+    return t, match.reshape(shape), gapy.reshape(shape)
+
+
+def format_expectations(hdp, alphabet, k, transitions, likelihood, event_model, event_expectations=None,
+                        posteriors=None, observed=None, assignment_kmers=(), assignment_means=()):
+    """continuousPairHmm_writeToFile (continuousHmm.c:354-406) / hdpHmm_writeToFile (:572-628): the
+    text, or "" when a transition is NaN (hmmContinuous_checkTransitions, :12-22)."""
+    flat_t = [float(v) for row in transitions for v in row]
+    if any(v != v for v in flat_t):
+        return ""
+    out = ["3\t%d\t%s\t%d\t\n" % (len(alphabet), alphabet, k)]
+    out.append("".join("%f\t" % v for v in flat_t) + "%f\n" % likelihood)
+    out.append("".join("%f\t" % v for row in event_model for v in row) + "\n")
+    if hdp:
+        out.append("".join("%f\t" % v for v in assignment_means) + "\n")
+        out.append("".join("%s\t" % kmer_string(int(kid), alphabet, k) for kid in assignment_kmers) + "\n")
+    else:
+        out.append("".join("%f\t" % v for row in event_expectations for v in row) + "\n")
+        out.append("".join("%f\t" % v for v in posteriors) + "\n")
+        out.append("".join("%d\t" % int(v) for v in observed) + "\n")
+    return "".join(out)

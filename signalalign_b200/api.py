@@ -164,6 +164,11 @@ def _bind(L):
         "sa_getExpectationsUsingAnchors": (C.c_int, [vp, C.c_char_p, C.c_int64, _f64p, C.c_int64, _i64p, C.c_int64,
                                                      C.POINTER(Params), C.c_int32, C.c_int32,
                                                      C.POINTER(Expectations)]),
+        "sa_normalizeExpectations": (C.c_int, [C.POINTER(Expectations), C.c_int64, _f64p]),
+        "sa_stateMachine_loadExpectations": (C.c_int, [vp, _f64p, _f64p]),
+        "sa_formatExpectations": (C.c_int, [vp, C.POINTER(Expectations), _f64p, _f64p, C.c_int64,
+                                            C.POINTER(C.c_void_p), _i64p]),
+        "sa_writeExpectations": (C.c_int, [C.c_char_p, vp, C.POINTER(Expectations), _f64p, _f64p, C.c_int64]),
         "sa_status_string": (C.c_char_p, [C.c_int]),
         "sa_kernel_launch_count": (C.c_int64, []),
         "sa_measure_fp32_peak": (C.c_int, [C.c_int32, _f64p]),
@@ -728,21 +733,12 @@ def getExpectationsUsingAnchors(sm, reference, events, anchors, p, ragged_left=T
     or into fresh accumulators with the given pseudocounts (hmmContinuous_getExpectationsHmm).
     Returns dict(likelihood, transitions (3x3), event_expectations (n_kmers x 2), posteriors,
     observed, assignments ((k-mer id, event index) rows, the HDP machine's))."""
-    n = sm.n_kmers
     if state is None:
-        state = dict(likelihood=0.0, transitions=np.full((3, 3), transition_pseudocount),
-                     event_expectations=np.zeros((n, 2)), posteriors=np.full(n, emission_pseudocount),
-                     observed=np.zeros(n, np.uint8), assignments=np.zeros((0, 2), np.int64))
+        state = makeExpectationsHmm(sm, transition_pseudocount, emission_pseudocount)
     ee = np.ascontiguousarray(state["event_expectations"], dtype=np.float64).copy()
     po = np.ascontiguousarray(state["posteriors"], dtype=np.float64).copy()
     ob = np.ascontiguousarray(state["observed"], dtype=np.uint8).copy()
-    ex = Expectations()
-    ex.likelihood = state["likelihood"]
-    for i, v in enumerate(np.asarray(state["transitions"], dtype=np.float64).reshape(-1)):
-        ex.transitions[i] = v
-    ex.event_expectations = ee.ctypes.data_as(_f64p)
-    ex.posteriors = po.ctypes.data_as(_f64p)
-    ex.observed = ob.ctypes.data_as(C.POINTER(C.c_uint8))
+    ex, _ = _expectations_struct(dict(state, event_expectations=ee, posteriors=po, observed=ob, assignments=None))
     cap = 4 * (len(reference) + len(events)) + 64
     ak = np.zeros(cap, np.int64)
     ae = np.zeros(cap, np.int64)
@@ -759,4 +755,95 @@ def getExpectationsUsingAnchors(sm, reference, events, anchors, p, ragged_left=T
     return dict(likelihood=ex.likelihood, transitions=np.array(list(ex.transitions)).reshape(3, 3),
                 event_expectations=ee, posteriors=po, observed=ob,
                 assignments=np.concatenate([np.asarray(state.get("assignments", np.zeros((0, 2), np.int64)),
-                                                       dtype=np.int64).reshape(-1, 2), got]))
+                                                       dtype=np.int64).reshape(-1, 2), got]),
+                event_model=state.get("event_model"))
+
+
+def makeExpectationsHmm(sm, transition_pseudocount=0.001, emission_pseudocount=0.001):
+    """continuousPairHmm_makeExpectationsHmm / hdpHmm_makeExpectationsHmm (continuousHmm.c:201-212,
+    :788-795): empty accumulators with the pseudocounts, and the machine's match table as the event
+    model."""
+    n = sm.n_kmers
+    return dict(likelihood=0.0, transitions=np.full((3, 3), float(transition_pseudocount)),
+                event_expectations=np.zeros((n, 2)), posteriors=np.full(n, float(emission_pseudocount)),
+                observed=np.zeros(n, np.uint8), assignments=np.zeros((0, 2), np.int64),
+                event_model=sm.tables()["match"])
+
+
+def _expectations_struct(hmm):
+    """sa_expectations over the arrays of an expectations dict; returns (struct, arrays to keep alive)"""
+    ex = Expectations()
+    ex.likelihood = hmm["likelihood"]
+    for i, v in enumerate(np.asarray(hmm["transitions"], dtype=np.float64).reshape(-1)):
+        ex.transitions[i] = v
+    keep = []
+    for name, field, dt, ct in (("event_expectations", "event_expectations", np.float64, C.c_double),
+                                ("posteriors", "posteriors", np.float64, C.c_double),
+                                ("observed", "observed", np.uint8, C.c_uint8)):
+        if hmm.get(name) is not None:
+            a = np.ascontiguousarray(hmm[name], dtype=dt)
+            keep.append(a)
+            setattr(ex, field, a.ctypes.data_as(C.POINTER(ct)))
+    if hmm.get("assignments") is not None:
+        asg = np.asarray(hmm["assignments"], dtype=np.int64).reshape(-1, 2)
+        ak, ae = np.ascontiguousarray(asg[:, 0]), np.ascontiguousarray(asg[:, 1])
+        keep += [ak, ae]
+        ex.assignment_kmers, ex.assignment_events = ak.ctypes.data_as(_i64p), ae.ctypes.data_as(_i64p)
+        ex.assignment_capacity = ex.n_assignments = len(asg)
+    return ex, keep
+
+
+def normalizeExpectations(hmm, transitions_only=False):
+    """continuousPairHmm_normalize (continuousHmm.c:283-306), or hmmDiscrete_normalizeTransitions alone
+    (discreteHmm.c:125-137, the HDP machine's step) with transitions_only: a new dict with normalised
+    transitions and, for the Gaussian machine, the re-estimated event model."""
+    out = dict(hmm)
+    em = None if transitions_only else np.array(hmm["event_model"], dtype=np.float64).reshape(-1, 5)
+    ex, keep = _expectations_struct(hmm)
+    n = len(em) if em is not None else 0
+    _check(lib().sa_normalizeExpectations(C.byref(ex), n, em.ctypes.data_as(_f64p) if em is not None else None),
+           "normalizeExpectations")
+    out["transitions"] = np.array(list(ex.transitions)).reshape(3, 3)
+    if em is not None:
+        out["event_model"] = em
+    return out
+
+
+def loadExpectationsIntoStateMachine(sm, hmm, emissions=True):
+    """continuousPairHmm_loadTransitionsIntoStateMachine and, with emissions,
+    continuousPairHmm_loadEmissionsIntoStateMachine (continuousHmm.c:321-352) from a normalised
+    expectations dict."""
+    t = np.ascontiguousarray(hmm["transitions"], dtype=np.float64).reshape(-1)
+    em = np.ascontiguousarray(hmm["event_model"], dtype=np.float64).reshape(-1) if emissions else None
+    _check(lib().sa_stateMachine_loadExpectations(sm.handle, t.ctypes.data_as(_f64p),
+                                                  em.ctypes.data_as(_f64p) if em is not None else None),
+           "loadExpectationsIntoStateMachine")
+
+
+def formatExpectations(sm, hmm, events=None):
+    """The text hmmContinuous_writeToFile (continuousHmm.c:872-884) writes for an expectations dict;
+    events (rows of 4) give the HDP machine's assigned event means."""
+    ex, keep = _expectations_struct(hmm)
+    em = hmm.get("event_model")
+    em = np.ascontiguousarray(em, dtype=np.float64) if em is not None else None
+    ev = _f64(events, 4) if events is not None else np.zeros((0, 4))
+    text = C.c_void_p()
+    n = C.c_int64(0)
+    _check(lib().sa_formatExpectations(sm.handle, C.byref(ex), em.ctypes.data_as(_f64p) if em is not None else None,
+                                       ev.ctypes.data_as(_f64p), len(ev), C.byref(text), C.byref(n)),
+           "formatExpectations")
+    try:
+        return C.string_at(text, n.value).decode() if n.value else ""
+    finally:
+        lib().sa_free_text(text)
+
+
+def writeExpectations(path, sm, hmm, events=None):
+    """hmmContinuous_writeToFile: the expectations file at `path` (replaced)."""
+    ex, keep = _expectations_struct(hmm)
+    em = hmm.get("event_model")
+    em = np.ascontiguousarray(em, dtype=np.float64) if em is not None else None
+    ev = _f64(events, 4) if events is not None else np.zeros((0, 4))
+    _check(lib().sa_writeExpectations(str(path).encode(), sm.handle, C.byref(ex),
+                                      em.ctypes.data_as(_f64p) if em is not None else None,
+                                      ev.ctypes.data_as(_f64p), len(ev)), "writeExpectations")

@@ -18,6 +18,7 @@ SOURCES = [
     ("sa_memory.cpp", []),
     ("sa_server.cpp", []),
     ("sa_io.cpp", []),
+    ("sa_em.cpp", []),
     ("sa_params.cu", ["-fmad=false"]),
     ("sa_fp64.cu", ["-fmad=false"]),
     ("sa_fp32.cu", []),

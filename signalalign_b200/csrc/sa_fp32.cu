@@ -140,7 +140,8 @@ struct sa_batch {
     // device timing of the last run's kernels (batches that own their device memory only)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timed = false;
-    // reads whose references have degenerate positions (multi-path cells) run in the plain FP64 form
+    // reads whose references have degenerate positions (multi-path cells), or whose machine's gap-Y
+    // table does not follow its match table, run in the plain FP64 form
     std::vector<int64_t> plain_of;          // per read: its index in `plain`, or -1
     std::vector<sa_read> plain_reads;
     PlainSet *plain = nullptr;
@@ -241,7 +242,8 @@ int planning_threads() {
 // one read's plan before packing
 struct ReadPlan {
     sa_status status = SA_OK;
-    bool multi = false;         // degenerate positions: aligned by the plain form
+    bool plain = false;         // degenerate positions, or a machine whose gap-Y table has its own
+                                // level mean or noise: aligned by the plain FP64 form
     int32_t model = -1;
     int64_t lX = 0;
     std::vector<int32_t> kid;   // k-mer id per column 1..lX
@@ -300,6 +302,8 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         scale64[r] = ReadScale64{sm->emission == SA_EMIT_PLAIN ? 1.0 : rd.scale, sm->emission == SA_EMIT_PLAIN ? 0.0 : rd.shift,
                                  var, 0.0};
     }
+    std::vector<char> fp32_tables(b->models.size());
+    for (size_t i = 0; i < b->models.size(); ++i) fp32_tables[i] = gapy_follows_match(b->models[i]);
     const int threads = planning_threads();
     // k-mer ids, regions and windows of each read
     parallel_for(n_reads, threads, [&](int64_t r) {
@@ -308,8 +312,8 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         const sa_read &rd = reads[r];
         PathTable pt;
         sa_status st = build_paths(rd.sm, rd.reference, rp.lX, rd.degenerate, pt);
-        if (!st && pt.multi) {
-            rp.multi = true;
+        if (!st && (pt.multi || !fp32_tables[rp.model])) {
+            rp.plain = true;
             return;
         }
         if (!st)
@@ -343,7 +347,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         b->read_n_regions[r] = (int64_t) rp.regs.size();
         nreg += (int64_t) rp.regs.size(); ndiag += rp.diags; ncell += rp.cells; nwin += rp.windows;
         nchunk += rp.chunks; nout += rp.out;
-        if (!rp.status && !rp.multi) {
+        if (!rp.status && !rp.plain) {
             nkmer += rp.lX;
             nevent += reads[r].n_events;
         }
@@ -351,7 +355,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     }
     b->plain_of.assign(n_reads, -1);
     for (int64_t r = 0; r < n_reads; ++r)
-        if (plan[r].multi && !plan[r].status) {
+        if (plan[r].plain && !plan[r].status) {
             b->plain_of[r] = (int64_t) b->plain_reads.size();
             b->plain_reads.push_back(reads[r]);
         }
@@ -374,7 +378,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     // the packed inputs, read by read
     parallel_for(n_reads, threads, [&](int64_t r) {
         const ReadPlan &rp = plan[r];
-        if (rp.status || rp.multi) return;
+        if (rp.status || rp.plain) return;
         const sa_read &rd = reads[r];
         const sa_state_machine *sm = rd.sm;
         for (int64_t x = 0; x < rp.lX; ++x) {

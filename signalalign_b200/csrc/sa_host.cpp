@@ -553,6 +553,15 @@ static sa_status upload(T **dst, const T *src, size_t n) {
     return SA_OK;
 }
 
+bool gapy_follows_match(const sa_state_machine *sm) {
+    if (sm->emission == SA_EMIT_HDP) return true;   // the HDP density serves both states
+    for (int64_t i = 0; i < sm->n_kmers; ++i) {
+        const double *m = &sm->match[5 * i], *y = &sm->gapy[5 * i];
+        if (!(y[0] == m[0] && y[2] == m[2] && y[4] == m[4])) return false;
+    }
+    return true;
+}
+
 static std::mutex g_model_mutex;
 
 sa_status ensure_device_model(sa_state_machine *sm) {

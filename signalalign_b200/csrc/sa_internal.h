@@ -120,6 +120,12 @@ sa_status build_paths(const sa_state_machine *sm, const char *reference, int64_t
 
 // device model upload (both kernel forms)
 sa_status ensure_device_model(sa_state_machine *sm);
+
+// The batched FP32 form takes the extra-event (gap-Y) emission's level mean, noise mean and noise
+// lambda from the match table and only the level sd from the gap-Y table.  True when the machine's
+// tables agree on those three fields for every k-mer (tables read from a .model file, and scaled by
+// scaleModel / scaleNoise, always do); reads of other machines run in the plain FP64 form.
+bool gapy_follows_match(const sa_state_machine *sm);
 void free_device_model(sa_state_machine *sm);
 
 void count_launch(int64_t n = 1);

@@ -111,3 +111,59 @@ def test_expectations_hdp_assignments(api, split):
     np.testing.assert_allclose(got["transitions"], want["transitions"], rtol=RTOL)
     assert len(want["assignments"]) > 500
     assert np.array_equal(got["assignments"], want["assignments"])
+
+
+def test_em_rounds_match_oracle_and_batches_follow(api):
+    """Three EM rounds on the device (expectations, continuousPairHmm_normalize, both loads into the
+    machine, as test_continuousPairHmm_em runs them, stateMachineTests.c:1210-1260) against the same
+    rounds on the oracle.  Re-estimated sds of k-mers seen once shrink by tens of orders of magnitude
+    a round, so rounding differences grow: the oracle perturbed by 1e-9 moves 6e-8 after three
+    rounds; rtol 1e-6.  Then a batch on the re-estimated machine, whose gap-Y table no longer follows
+    its match table: its reads run in the plain FP64 form, identical to the single-read entry."""
+    cfg = synth.config0()
+    m = W.gaussian_model(cfg)
+    rd = cfg["reads"][0]
+    p = _p(api)
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED, rd)
+    model = dict(m)
+    for _ in range(3):
+        want = orc.expectations(W.oracle_model(model, orc.EMIT_DESCALED, rd), rd["reference"], rd["events"],
+                                rd["anchors"], _op(p), False, False)
+        got = api.getExpectationsUsingAnchors(sm, rd["reference"], rd["events"], rd["anchors"], p, False, False)
+        assert got["likelihood"] == pytest.approx(want["likelihood"], rel=1e-6)
+        np.testing.assert_allclose(got["transitions"], want["transitions"], rtol=1e-6)
+        api.loadExpectationsIntoStateMachine(sm, api.normalizeExpectations(got))
+        model, _ = W.oracle_em_step(model, want, True)
+    np.testing.assert_allclose(sm.tables()["t"], model["t"], rtol=1e-6)
+    b = api.align_batch([api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                                       scale=rd["scale"], shift=rd["shift"])], p)
+    assert b.status(0) == 0
+    alone = api.getAlignedPairsUsingAnchors(sm, rd["reference"], rd["events"], rd["anchors"], p)
+    assert len(alone) > 100 and np.array_equal(alone, b.pairs(0))
+
+
+def test_hdp_em_transition_rounds_match_oracle(api):
+    """test_hdpHmm_emTransitions (stateMachineTests.c:1262-1305) on the device: the HDP machine,
+    transition pseudocount 0, transitions normalised and loaded each round, against the oracle"""
+    from oracle import formats
+    hc = W.small_hdp_config()
+    hdp = W.hdp_dict(hc["hdp"], len(hc["alphabet"]) ** hc["k"])
+    hm = formats.parse_model_lines(*synth.model_text(hc["alphabet"], hc["k"], hc["table"]).split("\n")[:3])
+    rd = hc["reads"][0]
+    p = _p(api)
+    smh = W.gpu_model(api, hm, orc.EMIT_HDP, rd, hdp)
+    model = dict(hm)
+    lik = []
+    for _ in range(4):
+        want = orc.expectations(W.oracle_model(model, orc.EMIT_HDP, rd, hdp), rd["reference"], rd["events"],
+                                rd["anchors"], _op(p), False, False, transition_pseudocount=0.0)
+        got = api.getExpectationsUsingAnchors(smh, rd["reference"], rd["events"], rd["anchors"], p, False, False,
+                                              transition_pseudocount=0.0)
+        assert got["likelihood"] == pytest.approx(want["likelihood"], rel=1e-9)
+        np.testing.assert_allclose(got["transitions"], want["transitions"], rtol=1e-8, atol=1e-12)
+        assert np.array_equal(got["assignments"], want["assignments"])
+        api.loadExpectationsIntoStateMachine(smh, api.normalizeExpectations(got, transitions_only=True),
+                                             emissions=False)
+        model, _ = W.oracle_em_step(model, want, False)
+        lik.append(got["likelihood"])
+    assert all(b >= a * (1 + 1e-7) for a, b in zip(lik, lik[1:]))   # negative: not lower, to 1e-7

@@ -2,6 +2,7 @@
 import numpy as np
 
 from oracle import formats
+from oracle import io as oio
 from oracle import oracle as orc
 from signalalign_b200 import synth
 
@@ -75,3 +76,16 @@ def max_posterior_error(a, b, threshold):
             present = pa if key in ma else pb
             err = max(err, present - threshold)
     return err
+
+
+def oracle_em_step(model, ex, emissions):
+    """The oracle's maximisation step on a model dict: continuousPairHmm_normalize and both loads
+    (emissions) or the transitions alone.  Returns (model, normalised transitions)."""
+    em0 = np.asarray(model["match"], dtype=np.float64).reshape(-1, 5)
+    if emissions:
+        T, em = oio.normalize_expectations(ex["transitions"], ex["event_expectations"], ex["posteriors"],
+                                           ex["observed"], em0)
+    else:
+        T, em = oio.normalize_transitions(ex["transitions"]), None
+    t, match, gapy = oio.load_expectations(model["t"], model["match"], model["gapy"], T, em)
+    return dict(model, t=t, match=match, gapy=gapy), T
