@@ -316,6 +316,16 @@ sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm, const char 
                                          int64_t n_anchors, const sa_params *p, int32_t ragged_left,
                                          int32_t ragged_right, sa_expectations *ex);
 
+/* Many reads' expectations in one launch (no signalAlign counterpart: signalMachine computes one
+ * read's expectations per process, signalMachine.c:620-690, and the training script sums the
+ * files).  One CTA walks read i's regions in order into ex[i], exactly as
+ * sa_getExpectationsUsingAnchors does for one read (identical results); each read uses its own
+ * scale / shift / var, ragged flags and machine.  read_status[i] is read i's status (ex[i] is
+ * written only for SA_OK, and for SA_E_OUTPUT when its assignments overflowed); the call returns
+ * SA_OK unless an argument, the parameters or a device step failed. */
+sa_status sa_getExpectationsBatch(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_expectations *ex,
+                                  int32_t *read_status);
+
 /* The EM maximisation step (continuousPairHmm_normalize, continuousHmm.c:283-306): the transitions
  * divided by their row sums in place (hmmDiscrete_normalizeTransitions, discreteHmm.c:125-137); with
  * an event model (n_kmers rows of 5, the machine's match table when the expectations were made, as

@@ -164,6 +164,8 @@ def _bind(L):
         "sa_getExpectationsUsingAnchors": (C.c_int, [vp, C.c_char_p, C.c_int64, _f64p, C.c_int64, _i64p, C.c_int64,
                                                      C.POINTER(Params), C.c_int32, C.c_int32,
                                                      C.POINTER(Expectations)]),
+        "sa_getExpectationsBatch": (C.c_int, [C.POINTER(Read), C.c_int64, C.POINTER(Params), C.POINTER(Expectations),
+                                              C.POINTER(C.c_int32)]),
         "sa_normalizeExpectations": (C.c_int, [C.POINTER(Expectations), C.c_int64, _f64p]),
         "sa_stateMachine_loadExpectations": (C.c_int, [vp, _f64p, _f64p]),
         "sa_formatExpectations": (C.c_int, [vp, C.POINTER(Expectations), _f64p, _f64p, C.c_int64,
@@ -757,6 +759,44 @@ def getExpectationsUsingAnchors(sm, reference, events, anchors, p, ragged_left=T
                 assignments=np.concatenate([np.asarray(state.get("assignments", np.zeros((0, 2), np.int64)),
                                                        dtype=np.int64).reshape(-1, 2), got]),
                 event_model=state.get("event_model"))
+
+
+def getExpectationsBatch(reads, p, states=None, transition_pseudocount=0.001, emission_pseudocount=0.001):
+    """Expectations of many reads (ReadInputs) in one launch (sa_getExpectationsBatch), each read into
+    its own accumulators (states[i], or fresh ones).  Returns (list of result dicts as
+    getExpectationsUsingAnchors returns, list of per-read statuses)."""
+    n = len(reads)
+    if states is None:
+        states = [makeExpectationsHmm(r.sm, transition_pseudocount, emission_pseudocount) for r in reads]
+    keep = []
+    arr = _read_array(reads, keep)
+    exs = (Expectations * max(n, 1))()
+    bufs = []
+    for i, (r, st) in enumerate(zip(reads, states)):
+        ee = np.ascontiguousarray(st["event_expectations"], dtype=np.float64).copy()
+        po = np.ascontiguousarray(st["posteriors"], dtype=np.float64).copy()
+        ob = np.ascontiguousarray(st["observed"], dtype=np.uint8).copy()
+        ex, _ = _expectations_struct(dict(st, event_expectations=ee, posteriors=po, observed=ob, assignments=None))
+        cap = 4 * (len(r.reference) + len(r.events)) + 64
+        ak, ae = np.zeros(cap, np.int64), np.zeros(cap, np.int64)
+        ex.assignment_kmers, ex.assignment_events = ak.ctypes.data_as(_i64p), ae.ctypes.data_as(_i64p)
+        ex.assignment_capacity = cap
+        exs[i] = ex
+        bufs.append((ee, po, ob, ak, ae))
+    status = np.zeros(max(n, 1), np.int32)
+    _check(lib().sa_getExpectationsBatch(arr, n, C.byref(p), exs, status.ctypes.data_as(C.POINTER(C.c_int32))),
+           "getExpectationsBatch")
+    out = []
+    for i, st in enumerate(states):
+        ee, po, ob, ak, ae = bufs[i]
+        ex = exs[i]
+        got = np.column_stack([ak[:min(ex.n_assignments, len(ak))], ae[:min(ex.n_assignments, len(ae))]])
+        out.append(dict(likelihood=ex.likelihood, transitions=np.array(list(ex.transitions)).reshape(3, 3),
+                        event_expectations=ee, posteriors=po, observed=ob,
+                        assignments=np.concatenate([np.asarray(st.get("assignments", np.zeros((0, 2), np.int64)),
+                                                               dtype=np.int64).reshape(-1, 2), got]),
+                        event_model=st.get("event_model")))
+    return out, [int(v) for v in status[:n]]
 
 
 def makeExpectationsHmm(sm, transition_pseudocount=0.001, emission_pseudocount=0.001):

@@ -63,6 +63,7 @@ struct SetOut {
 // accumulators in the reference's order (their emission spreads depend on it).
 struct ExpectOut {
     int32_t on, n_regions;
+    int32_t first_region, pad0;   // the read's regions: first_region .. first_region + n_regions - 1
     double *scratch;            // 8 transition posteriors per cell of the anti-diagonal at hand
     int32_t *mask;              // per cell: lower / middle / upper neighbour present
     double *acc;                // likelihood, then the 3 x 3 transition expectations
@@ -414,13 +415,15 @@ __device__ void run_region(const Model64 &M, const Region64 &R, int32_t region, 
     __syncthreads();
 }
 
+// Expectations mode (XS: one ExpectOut per read): CTA b walks read b's regions in order.
 __global__ void __launch_bounds__(128) region_kernel(const Model64 *models, const Region64 *regions, SetOut O,
-                                                     ExpectOut X) {
+                                                     const ExpectOut *XS) {
     double acc[10];
-    if (X.on) {
+    if (XS) {
         // the read's regions in order (the reference's split wrapper loops over them), one CTA
+        const ExpectOut X = XS[blockIdx.x];
         for (int i = 0; i < 10; ++i) acc[i] = X.acc[i];
-        for (int32_t r = 0; r < X.n_regions; ++r) {
+        for (int32_t r = X.first_region; r < X.first_region + X.n_regions; ++r) {
             const Region64 R = regions[r];
             run_region(models[R.model], R, r, O, X, acc);
         }
@@ -428,6 +431,7 @@ __global__ void __launch_bounds__(128) region_kernel(const Model64 *models, cons
             for (int i = 0; i < 10; ++i) X.acc[i] = acc[i];
         return;
     }
+    const ExpectOut X{};
     const Region64 R = regions[blockIdx.x];
     run_region(models[R.model], R, (int32_t) blockIdx.x, O, X, acc);
 }
@@ -766,9 +770,7 @@ sa_status plain_run(PlainSet *s, cudaStream_t stream) {
     O.tag = s->d_tag;
     O.count = s->d_count;
     O.cap = s->cap;
-    ExpectOut X;
-    std::memset(&X, 0, sizeof(X));
-    region_kernel<<<(unsigned) s->regs.size(), 128, 0, stream>>>(s->d_models, s->d_regions, O, X);
+    region_kernel<<<(unsigned) s->regs.size(), 128, 0, stream>>>(s->d_models, s->d_regions, O, nullptr);
     count_launch();
     return cudaGetLastError() == cudaSuccess ? SA_OK : SA_E_CUDA;
 }
@@ -853,6 +855,7 @@ using namespace sa;
 // Device memory bound of one plain call (the forward and backward rings of a 20 kb read take tens
 // of MB; a pathological band of many-path cells is refused rather than allowed to take the GPU).
 static constexpr size_t kPlainMaxBytes = (size_t) 32 << 30;
+static constexpr size_t kExpectMaxBytes = (size_t) 64 << 30;
 
 extern "C" sa_status sa_getAlignedPairsUsingAnchors(const sa_state_machine *sm_c, const char *reference,
                                                     int64_t reference_length, sa_degenerate degenerate,
@@ -923,6 +926,151 @@ extern "C" sa_status sa_getAlignedPairsUsingAnchors(const sa_state_machine *sm_c
     return SA_OK;
 }
 
+// Expectations of many reads in one launch: CTA i walks read i's regions in order into ex[i]'s
+// accumulators (the single-read call is this with one read).  Per read on the device: the
+// anti-diagonal scratch and cell masks, the accumulators, and (HDP machines) the assignment lists.
+static sa_status expectations_batch(const sa_read *reads, int64_t n, const sa_params &p, sa_expectations *ex,
+                                    int32_t *read_status) {
+    for (int64_t i = 0; i < n; ++i) {
+        read_status[i] = SA_OK;
+        const sa_state_machine *sm = reads[i].sm;
+        if (!sm || !ex[i].event_expectations || !ex[i].posteriors || !ex[i].observed) {
+            read_status[i] = SA_E_ARG;
+        } else if (sm->emission == SA_EMIT_HDP) {
+            // the HDP machine collects assignments instead (hdpHmm_makeExpectationsHmm)
+            if (!sm->hdp.present) read_status[i] = SA_E_UNSUPPORTED;
+            else if (ex[i].assignment_capacity > 0 && (!ex[i].assignment_kmers || !ex[i].assignment_events))
+                read_status[i] = SA_E_ARG;
+        }
+    }
+    PlainSet *s = nullptr;
+    sa_status st = plain_create(reads, n, p, kExpectMaxBytes, &s);
+    if (st) return st;
+    std::vector<int32_t> width(n, 1);
+    for (int64_t i = 0; i < n; ++i) {
+        if (!read_status[i]) read_status[i] = s->read_status[i];
+        for (int64_t r = s->read_first[i]; r < s->read_first[i] + s->read_count[i]; ++r) {
+            if (s->regs[r].max_paths > 1 && !read_status[i]) read_status[i] = SA_E_UNSUPPORTED;   // single-path cells only
+            width[i] = std::max(width[i], s->regs[r].stride);
+        }
+    }
+    std::vector<int64_t> run;   // reads that run, in order
+    for (int64_t i = 0; i < n; ++i)
+        if (!read_status[i] && s->read_count[i] > 0) run.push_back(i);
+    for (int64_t i : run)
+        if (!st) st = ensure_device_model(const_cast<sa_state_machine *>(reads[i].sm));
+    int prev_dev = 0;
+    if (!st && cudaGetDevice(&prev_dev) != cudaSuccess) st = SA_E_CUDA;
+    if (!st && cudaSetDevice(s->device) != cudaSuccess) st = SA_E_CUDA;
+    if (st || run.empty()) {
+        if (!st)
+            for (int64_t i = 0; i < n; ++i)
+                if (!read_status[i]) ex[i].n_assignments = 0;
+        plain_destroy(s);
+        return st;
+    }
+    // one device block: per running read its buffers, then the ExpectOut array
+    struct Off { size_t scratch, mask, acc, ee, po, ob, ak, ae, na; int64_t nk, cap; bool hdp; };
+    auto up = [](size_t v) { return (v + 255) & ~(size_t) 255; };
+    std::vector<Off> off(run.size());
+    size_t total = 0;
+    for (size_t j = 0; j < run.size(); ++j) {
+        const int64_t i = run[j];
+        const sa_state_machine *sm = reads[i].sm;
+        Off &o = off[j];
+        o.nk = sm->n_kmers;
+        o.hdp = sm->emission == SA_EMIT_HDP;
+        o.cap = o.hdp ? std::max<int64_t>(ex[i].assignment_capacity, 0) : 0;
+        o.scratch = total; total += up(sizeof(double) * 8 * (size_t) width[i]);
+        o.mask = total; total += up(sizeof(int32_t) * (size_t) width[i]);
+        o.acc = total; total += up(sizeof(double) * 10);
+        o.ee = total; total += up(sizeof(double) * 2 * (size_t) o.nk);
+        o.po = total; total += up(sizeof(double) * (size_t) o.nk);
+        o.ob = total; total += up((size_t) o.nk);
+        o.ak = total; total += up(sizeof(int64_t) * (size_t) std::max<int64_t>(o.cap, 1));
+        o.ae = total; total += up(sizeof(int64_t) * (size_t) std::max<int64_t>(o.cap, 1));
+        o.na = total; total += up(sizeof(int64_t));
+    }
+    const size_t o_xs = total;
+    total += up(sizeof(ExpectOut) * run.size());
+    std::vector<unsigned char> host(total, 0);
+    MemBlock blk;
+    st = plain_upload(s, nullptr);
+    if (!st) st = mem_get(MemKind::Device, s->device, total, blk);
+    if (!st) {
+        auto *d = static_cast<unsigned char *>(blk.ptr);
+        auto *xs = reinterpret_cast<ExpectOut *>(host.data() + o_xs);
+        for (size_t j = 0; j < run.size(); ++j) {
+            const int64_t i = run[j];
+            const Off &o = off[j];
+            auto *acc = reinterpret_cast<double *>(host.data() + o.acc);
+            acc[0] = ex[i].likelihood;
+            for (int k = 0; k < 9; ++k) acc[k + 1] = ex[i].transitions[k];
+            std::memcpy(host.data() + o.ee, ex[i].event_expectations, sizeof(double) * 2 * (size_t) o.nk);
+            std::memcpy(host.data() + o.po, ex[i].posteriors, sizeof(double) * (size_t) o.nk);
+            std::memcpy(host.data() + o.ob, ex[i].observed, (size_t) o.nk);
+            ExpectOut &X = xs[j];
+            X.on = 1;
+            X.first_region = (int32_t) s->read_first[i];
+            X.n_regions = (int32_t) s->read_count[i];
+            X.hdp = o.hdp ? 1 : 0;
+            X.threshold = p.threshold;
+            X.scratch = reinterpret_cast<double *>(d + o.scratch);
+            X.mask = reinterpret_cast<int32_t *>(d + o.mask);
+            X.acc = reinterpret_cast<double *>(d + o.acc);
+            X.event_exp = reinterpret_cast<double *>(d + o.ee);
+            X.posteriors = reinterpret_cast<double *>(d + o.po);
+            X.observed = d + o.ob;
+            X.assign_kmer = reinterpret_cast<int64_t *>(d + o.ak);
+            X.assign_event = reinterpret_cast<int64_t *>(d + o.ae);
+            X.n_assign = reinterpret_cast<int64_t *>(d + o.na);
+            X.assign_cap = o.cap;
+        }
+        SetOut O;
+        std::memset(&O, 0, sizeof(O));
+        auto *dev = static_cast<unsigned char *>(s->dev.ptr);
+        if (cudaMemcpy(d, host.data(), total, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemsetAsync(dev + s->res_off, 0, s->res_bytes, nullptr) != cudaSuccess ||
+            cudaMemsetAsync(s->d_P, 0, std::max<size_t>(s->p_bytes, 1), nullptr) != cudaSuccess)
+            st = SA_E_CUDA;
+        if (!st) {
+            region_kernel<<<(unsigned) run.size(), 128>>>(s->d_models, s->d_regions, O,
+                                                        reinterpret_cast<const ExpectOut *>(d + o_xs));
+            count_launch();
+            if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = SA_E_CUDA;
+        }
+        if (!st && cudaMemcpy(host.data(), d, o_xs, cudaMemcpyDeviceToHost) != cudaSuccess) st = SA_E_CUDA;
+        if (!st) {
+            for (size_t j = 0; j < run.size(); ++j) {
+                const int64_t i = run[j];
+                const Off &o = off[j];
+                const auto *acc = reinterpret_cast<const double *>(host.data() + o.acc);
+                ex[i].likelihood = acc[0];
+                for (int k = 0; k < 9; ++k) ex[i].transitions[k] = acc[k + 1];
+                std::memcpy(ex[i].event_expectations, host.data() + o.ee, sizeof(double) * 2 * (size_t) o.nk);
+                std::memcpy(ex[i].posteriors, host.data() + o.po, sizeof(double) * (size_t) o.nk);
+                std::memcpy(ex[i].observed, host.data() + o.ob, (size_t) o.nk);
+                const int64_t na = *reinterpret_cast<const int64_t *>(host.data() + o.na);
+                ex[i].n_assignments = na;
+                if (o.hdp) {
+                    const int64_t got = std::min(na, o.cap);
+                    if (got > 0) {
+                        std::memcpy(ex[i].assignment_kmers, host.data() + o.ak, sizeof(int64_t) * (size_t) got);
+                        std::memcpy(ex[i].assignment_events, host.data() + o.ae, sizeof(int64_t) * (size_t) got);
+                    }
+                    if (na > o.cap) read_status[i] = SA_E_OUTPUT;
+                }
+            }
+            for (int64_t i = 0; i < n; ++i)
+                if (!read_status[i] && s->read_count[i] == 0) ex[i].n_assignments = 0;
+        }
+    }
+    mem_put(blk);
+    cudaSetDevice(prev_dev);
+    plain_destroy(s);
+    return st;
+}
+
 extern "C" sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm_c, const char *reference,
                                                     int64_t reference_length, const double *events, int64_t n_events,
                                                     const int64_t *anchors, int64_t n_anchors, const sa_params *p,
@@ -932,121 +1080,33 @@ extern "C" sa_status sa_getExpectationsUsingAnchors(const sa_state_machine *sm_c
         return SA_E_ARG;
     if ((reference_length > 0 && !reference) || (n_events > 0 && !events) || (n_anchors > 0 && !anchors))
         return SA_E_ARG;
-    auto *sm = const_cast<sa_state_machine *>(sm_c);
-    // the continuous pair HMM of the Gaussian machine (hmmContinuous_getExpectationsHmm,
-    // continuousHmm.c:842-857); the HDP machine collects assignments instead
-    const bool hdp = sm->emission == SA_EMIT_HDP;
-    if (hdp && (!sm->hdp.present || (ex->assignment_capacity > 0 && (!ex->assignment_kmers || !ex->assignment_events))))
-        return hdp && !sm->hdp.present ? SA_E_UNSUPPORTED : SA_E_ARG;
     sa_status st = check_params(*p);
     if (st) return st;
     sa_read rd;
     std::memset(&rd, 0, sizeof(rd));
-    rd.sm = sm;
+    rd.sm = sm_c;
     rd.reference = reference;
     rd.reference_length = reference_length;
     rd.events = events;
     rd.n_events = n_events;
     rd.anchors = anchors;
     rd.n_anchors = n_anchors;
-    rd.scale = sm->scale;
-    rd.shift = sm->shift;
-    rd.var = sm->var;
+    rd.scale = sm_c->scale;
+    rd.shift = sm_c->shift;
+    rd.var = sm_c->var;
     rd.ragged_left = ragged_left;
     rd.ragged_right = ragged_right;
     rd.degenerate = SA_CYTOSINE_METHYLATION3;
-    PlainSet *s = nullptr;
-    st = plain_create(&rd, 1, *p, kPlainMaxBytes, &s);
+    int32_t rs = SA_OK;
+    st = expectations_batch(&rd, 1, *p, ex, &rs);
+    return st ? st : (sa_status) rs;
+}
+
+extern "C" sa_status sa_getExpectationsBatch(const sa_read *reads, int64_t n_reads, const sa_params *p,
+                                             sa_expectations *ex, int32_t *read_status) {
+    if (n_reads < 0 || !p || (n_reads > 0 && (!reads || !ex || !read_status))) return SA_E_ARG;
+    sa_status st = check_params(*p);
     if (st) return st;
-    int32_t width = 1;
-    for (const PlainRegion &pr : s->regs) {
-        if (pr.max_paths > 1) st = SA_E_UNSUPPORTED;   // single-path cells only
-        width = std::max(width, pr.stride);
-    }
-    if (!st) st = (sa_status) s->read_status[0];
-    if (!st) st = ensure_device_model(sm);
-    int prev_dev = 0;
-    if (!st && cudaGetDevice(&prev_dev) != cudaSuccess) st = SA_E_CUDA;
-    if (!st && cudaSetDevice(s->device) != cudaSuccess) st = SA_E_CUDA;
-    if (st) {
-        plain_destroy(s);
-        return st;
-    }
-    const int64_t nk = sm->n_kmers;
-    // one device block: scratch, mask, accumulators, per-k-mer expectations
-    auto up = [](size_t v) { return (v + 255) & ~(size_t) 255; };
-    const size_t o_mask = up(sizeof(double) * 8 * (size_t) width), o_acc = o_mask + up(sizeof(int32_t) * width);
-    const size_t o_ee = o_acc + up(sizeof(double) * 10), o_po = o_ee + up(sizeof(double) * 2 * nk);
-    const int64_t acap = hdp ? std::max<int64_t>(ex->assignment_capacity, 0) : 0;
-    const size_t o_ob = o_po + up(sizeof(double) * nk), o_ak = o_ob + up((size_t) nk);
-    const size_t o_ae = o_ak + up(sizeof(int64_t) * std::max<int64_t>(acap, 1));
-    const size_t o_na = o_ae + up(sizeof(int64_t) * std::max<int64_t>(acap, 1)), total = o_na + up(sizeof(int64_t));
-    MemBlock blk;
-    st = plain_upload(s, nullptr);
-    if (!st) st = mem_get(MemKind::Device, s->device, total, blk);
-    if (!st) {
-        auto *d = static_cast<unsigned char *>(blk.ptr);
-        double acc[10];
-        acc[0] = ex->likelihood;
-        for (int i = 0; i < 9; ++i) acc[i + 1] = ex->transitions[i];
-        if (cudaMemcpy(d + o_acc, acc, sizeof(acc), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(d + o_ee, ex->event_expectations, sizeof(double) * 2 * nk, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(d + o_po, ex->posteriors, sizeof(double) * nk, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(d + o_ob, ex->observed, (size_t) nk, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemset(d + o_na, 0, sizeof(int64_t)) != cudaSuccess)
-            st = SA_E_CUDA;
-        ExpectOut X;
-        std::memset(&X, 0, sizeof(X));
-        X.on = 1;
-        X.hdp = hdp ? 1 : 0;
-        X.threshold = p->threshold;
-        X.assign_kmer = reinterpret_cast<int64_t *>(d + o_ak);
-        X.assign_event = reinterpret_cast<int64_t *>(d + o_ae);
-        X.n_assign = reinterpret_cast<int64_t *>(d + o_na);
-        X.assign_cap = acap;
-        X.n_regions = (int32_t) s->regs.size();
-        X.scratch = reinterpret_cast<double *>(d);
-        X.mask = reinterpret_cast<int32_t *>(d + o_mask);
-        X.acc = reinterpret_cast<double *>(d + o_acc);
-        X.event_exp = reinterpret_cast<double *>(d + o_ee);
-        X.posteriors = reinterpret_cast<double *>(d + o_po);
-        X.observed = d + o_ob;
-        SetOut O;
-        std::memset(&O, 0, sizeof(O));
-        auto *dev = static_cast<unsigned char *>(s->dev.ptr);
-        if (!st && (cudaMemsetAsync(dev + s->res_off, 0, s->res_bytes, nullptr) != cudaSuccess ||
-                    cudaMemsetAsync(s->d_P, 0, std::max<size_t>(s->p_bytes, 1), nullptr) != cudaSuccess))
-            st = SA_E_CUDA;
-        if (!st && !s->regs.empty()) {
-            region_kernel<<<1, 128>>>(s->d_models, s->d_regions, O, X);
-            count_launch();
-            if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) st = SA_E_CUDA;
-        }
-        if (!st) {
-            if (cudaMemcpy(acc, d + o_acc, sizeof(acc), cudaMemcpyDeviceToHost) != cudaSuccess ||
-                cudaMemcpy(ex->event_expectations, d + o_ee, sizeof(double) * 2 * nk, cudaMemcpyDeviceToHost) !=
-                    cudaSuccess ||
-                cudaMemcpy(ex->posteriors, d + o_po, sizeof(double) * nk, cudaMemcpyDeviceToHost) != cudaSuccess ||
-                cudaMemcpy(ex->observed, d + o_ob, (size_t) nk, cudaMemcpyDeviceToHost) != cudaSuccess)
-                st = SA_E_CUDA;
-            ex->likelihood = acc[0];
-            for (int i = 0; i < 9; ++i) ex->transitions[i] = acc[i + 1];
-            int64_t na = 0;
-            if (cudaMemcpy(&na, d + o_na, sizeof(na), cudaMemcpyDeviceToHost) != cudaSuccess) st = SA_E_CUDA;
-            ex->n_assignments = na;
-            if (!st && hdp) {
-                const int64_t got = std::min(na, acap);
-                if (got > 0 && (cudaMemcpy(ex->assignment_kmers, d + o_ak, sizeof(int64_t) * got,
-                                           cudaMemcpyDeviceToHost) != cudaSuccess ||
-                                cudaMemcpy(ex->assignment_events, d + o_ae, sizeof(int64_t) * got,
-                                           cudaMemcpyDeviceToHost) != cudaSuccess))
-                    st = SA_E_CUDA;
-                if (!st && na > acap) st = SA_E_OUTPUT;
-            }
-        }
-    }
-    mem_put(blk);
-    cudaSetDevice(prev_dev);
-    plain_destroy(s);
-    return st;
+    if (n_reads == 0) return SA_OK;
+    return expectations_batch(reads, n_reads, *p, ex, read_status);
 }

@@ -167,3 +167,45 @@ def test_hdp_em_transition_rounds_match_oracle(api):
         model, _ = W.oracle_em_step(model, want, False)
         lik.append(got["likelihood"])
     assert all(b >= a * (1 + 1e-7) for a, b in zip(lik, lik[1:]))   # negative: not lower, to 1e-7
+
+
+def test_expectations_batch_matches_single_reads(api):
+    """sa_getExpectationsBatch: Gaussian reads with split regions, HDP reads, a read whose 'X' the ACGT
+    alphabet cannot expand and one with an empty reference, in one launch.  Each read's result is
+    identical to its single-read call (one CTA walks its regions in the same order), the failing
+    read gets its own status and the others are unaffected."""
+    from oracle import formats
+    cfg = synth.config1(seed=21, n_reads=4, span=(600, 1200))
+    m = W.gaussian_model(cfg)
+    p = _p(api, split_matrix_bigger_than_this=2000)
+    hc = W.small_hdp_config()
+    hdp = W.hdp_dict(hc["hdp"], len(hc["alphabet"]) ** hc["k"])
+    hm = formats.parse_model_lines(*synth.model_text(hc["alphabet"], hc["k"], hc["table"]).split("\n")[:3])
+    cases = [(rd, W.gpu_model(api, m, orc.EMIT_DESCALED, rd)) for rd in cfg["reads"]]
+    cases += [(rd, W.gpu_model(api, hm, orc.EMIT_HDP, rd, hdp)) for rd in hc["reads"][:2]]
+    reads, singles = [], []
+    for rd, sm in cases:
+        reads.append(api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                                   scale=rd["scale"], shift=rd["shift"], var=rd.get("var", 1.0)))
+        singles.append(api.getExpectationsUsingAnchors(sm, rd["reference"], rd["events"], rd["anchors"], p))
+    bad = cfg["reads"][0]
+    reads.insert(2, api.ReadInput(sm=cases[0][1], reference=bad["reference"][:200] + "X" + bad["reference"][201:],
+                                  events=bad["events"], anchors=bad["anchors"], scale=bad["scale"], shift=bad["shift"]))
+    singles.insert(2, None)
+    reads.append(api.ReadInput(sm=cases[0][1], reference="", events=bad["events"][:5], anchors=np.zeros((0, 2))))
+    singles.append(api.getExpectationsUsingAnchors(cases[0][1], "", bad["events"][:5], np.zeros((0, 2)), p))
+    got, status = api.getExpectationsBatch(reads, p)
+    assert status[2] == 2                      # SA_E_ALPHABET, as the single call reports it
+    for g, want, st in zip(got, singles, status):
+        if want is None:
+            continue
+        assert st == 0
+        for key in ("likelihood", "transitions", "event_expectations", "posteriors", "observed", "assignments"):
+            np.testing.assert_array_equal(g[key], want[key])   # bit for bit (NaN where the single call has NaN)
+    assert len(got[-2]["assignments"]) > 100   # the HDP reads' assignment lists
+    rd = cfg["reads"][1]
+    want = orc.expectations(W.oracle_model(m, orc.EMIT_DESCALED, rd), rd["reference"], rd["events"], rd["anchors"],
+                            _op(p))
+    _compare(got[1], want)
+    empty, st = api.getExpectationsBatch([], p)
+    assert empty == [] and st == []
