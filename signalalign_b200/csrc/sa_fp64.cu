@@ -61,11 +61,14 @@ struct SetOut {
 // Expectations mode (getExpectationsUsingAnchors, pairwiseAligner.c:1983-2003): one CTA walks the
 // read's regions in order and folds every transition posterior into a continuous pair HMM's
 // accumulators in the reference's order (their emission spreads depend on it).
+constexpr int kExpectScratch = 9;   // doubles of expectations scratch per cell
+
 struct ExpectOut {
     int32_t on, n_regions;
     int32_t first_region, pad0;   // the read's regions: first_region .. first_region + n_regions - 1
-    double *scratch;            // 8 transition posteriors per cell of the anti-diagonal at hand
-    int32_t *mask;              // per cell: lower / middle / upper neighbour present
+    double *scratch;            // per cell of the anti-diagonal at hand: 8 transition posteriors and
+                                // the descaled event mean
+    int32_t *mask;              // per cell: lower / middle / upper neighbour present, k-mer id + 1
     double *acc;                // likelihood, then the 3 x 3 transition expectations
     double *event_exp;          // per k-mer: weighted mean sum, weighted spread sum
     double *posteriors;         // per k-mer: weight
@@ -241,11 +244,18 @@ __device__ double total_probability(const Model64 &M, const Region64 &R, int32_t
 // traced back to T: the cells of B[d2] against their forward neighbours (the reference has freed
 // F[T-1] by then, so the middle neighbours of d2 = T+1 are absent), each transition's posterior
 // exp(F[from] + B[to] + (e + t) - total) (cell_signal_updateExpectations, :763-793), computed in
-// parallel; then thread 0 adds them in stateMachine3_cellCalculate's order, cell by cell
-// (continuousPairHmm_addToEmissionExpectation, continuousHmm.c:160-169, for transitions into match).
+// parallel.  Then thread 0 adds the transition posteriors in stateMachine3_cellCalculate's order, cell
+// by cell (and, for the HDP machine, appends the assignments in that order), while the other threads
+// fold the match posteriors into the per-k-mer emission expectations
+// (continuousPairHmm_addToEmissionExpectation, continuousHmm.c:160-169): k-mers are independent, and
+// one k-mer's updates (a running mean, so order matters) are made by one thread in cell order.  The
+// cells of an anti-diagonal lie in distinct columns, so a k-mer recurs on it only where the reference
+// repeats it within the band; the first such cell's thread makes the updates of all of them.
 __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const ExpectOut &X, int32_t d2, int32_t T,
                                 double total, double (&acc)[10]) {
     const int tid = threadIdx.x, nt = blockDim.x;
+    double *const scratch = X.scratch;
+    int32_t *const mask = X.mask;
     for (int32_t xmy = R.xl[d2] + 2 * tid; xmy <= R.xr[d2]; xmy += 2 * nt) {
         const int32_t c = (xmy - R.xl[d2]) >> 1;
         const int32_t x = (d2 + xmy) >> 1, y = (d2 - xmy) >> 1;
@@ -253,7 +263,7 @@ __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const Expec
         const double *cur = slot(R.B, R, d2, r);
         const bool lo = in_band(R, d2 - 1, xmy - 1), mi = d2 - 2 >= T && in_band(R, d2 - 2, xmy),
                    up = in_band(R, d2 - 1, xmy + 1);
-        double *ps = X.scratch + 8 * (int64_t) c;
+        double *ps = scratch + kExpectScratch * (int64_t) c;
         if (lo) {
             const double *l = slot(R.F, R, d2 - 1, R.pfirst[x - 1]);
             const double e = emit_gapx(M, kid);
@@ -268,6 +278,10 @@ __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const Expec
             ps[3] = exp(m[S_M] + cur[S_M] + (e + M.t[T_MC]) - total);
             ps[4] = exp(m[S_X] + cur[S_M] + (e + M.t[T_MFGX]) - total);
             ps[5] = exp(m[S_Y] + cur[S_M] + (e + M.t[T_MFGY]) - total);
+            // the descaled event mean (emissions_signal_descaleEventMean_JordanStyle) with the
+            // k-mer's level mean from the machine's match table
+            const double mu = M.match[(int64_t) kid * 5];
+            ps[8] = (ev.x + M.var * mu - M.scale * mu - M.shift) / M.var;
         }
         if (up) {
             const double *u = slot(R.F, R, d2 - 1, r);
@@ -276,52 +290,74 @@ __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const Expec
             ps[6] = exp(u[S_M] + cur[S_Y] + (e + M.t[T_OY]) - total);
             ps[7] = exp(u[S_Y] + cur[S_Y] + (e + M.t[T_EY]) - total);
         }
-        X.mask[c] = (lo ? 1 : 0) | (mi ? 2 : 0) | (up ? 4 : 0);
+        // neighbour flags in the low 3 bits, k-mer id + 1 above them (ids are below 2^27)
+        mask[c] = (lo ? 1 : 0) | (mi ? 2 : 0) | (up ? 4 : 0) | ((kid + 1) << 3);
     }
     __syncthreads();
+    const int32_t w = (R.xr[d2] - R.xl[d2]) / 2 + 1;
     if (tid == 0) {
         acc[0] += total;   // hmmExpectations->likelihood += totalProbability, once per diagonal
-        const int32_t w = (R.xr[d2] - R.xl[d2]) / 2 + 1;
         for (int32_t c = 0; c < w; ++c) {
-            const int32_t mk = X.mask[c];
-            const double *ps = X.scratch + 8 * (int64_t) c;
+            const int32_t mk = mask[c];
+            const double *ps = scratch + kExpectScratch * (int64_t) c;
             if (mk & 1) {   // lower: M, X, Y -> X
                 acc[1 + S_M * 3 + S_X] += ps[0];
                 acc[1 + S_X * 3 + S_X] += ps[1];
                 acc[1 + S_Y * 3 + S_X] += ps[2];
             }
-            if (mk & 2) {   // middle: M, X, Y -> M, each also an emission expectation
+            if (mk & 2) {   // middle: M, X, Y -> M
                 const int32_t xmy = R.xl[d2] + 2 * c;
-                const int32_t x = (d2 + xmy) >> 1, y = (d2 - xmy) >> 1;
-                const int64_t kid = R.pid[R.pfirst[x]];
-                const double mu = M.match[kid * 5];
-                const double xe = (R.ev[y - 1].x + M.var * mu - M.scale * mu - M.shift) / M.var;
+                const int32_t y = (d2 - xmy) >> 1;
+                const int64_t kid = (mk >> 3) - 1;
                 for (int j = 0; j < 3; ++j) {
                     const double p = ps[3 + j];
                     acc[1 + j * 3 + S_M] += p;
-                    if (X.hdp) {
-                        // cell_signal_updateExpectationsAndAssignments (pairwiseAligner.c:795-817)
-                        if (p >= X.threshold) {
-                            const int64_t at = *X.n_assign;
-                            if (at < X.assign_cap) {
-                                X.assign_kmer[at] = kid;
-                                X.assign_event[at] = R.ev_base + y - 1;
-                            }
-                            *X.n_assign = at + 1;
+                    // cell_signal_updateExpectationsAndAssignments (pairwiseAligner.c:795-817)
+                    if (X.hdp && p >= X.threshold) {
+                        const int64_t at = *X.n_assign;
+                        if (at < X.assign_cap) {
+                            X.assign_kmer[at] = kid;
+                            X.assign_event[at] = R.ev_base + y - 1;
                         }
-                        continue;
+                        *X.n_assign = at + 1;
                     }
-                    X.event_exp[2 * kid] += p * xe;
-                    X.posteriors[kid] += p;
-                    const double uk = X.event_exp[2 * kid] / X.posteriors[kid];
-                    X.event_exp[2 * kid + 1] += p * (xe - uk) * (xe - uk);
-                    X.observed[kid] = 1;
                 }
             }
             if (mk & 4) {   // upper: M, Y -> Y
                 acc[1 + S_M * 3 + S_Y] += ps[6];
                 acc[1 + S_Y * 3 + S_Y] += ps[7];
             }
+        }
+    } else if (!X.hdp) {
+        for (int32_t c = tid - 1; c < w; c += nt - 1) {
+            const int32_t mk = mask[c];
+            if (!(mk & 2)) continue;
+            const int32_t key = mk >> 3;
+            bool first = true;
+            for (int32_t c2 = 0; c2 < c && first; ++c2) {
+                const int32_t m2 = mask[c2];
+                first = !((m2 & 2) && (m2 >> 3) == key);
+            }
+            if (!first) continue;
+            const int64_t kid = key - 1;
+            double e0 = X.event_exp[2 * kid], e1 = X.event_exp[2 * kid + 1], po = X.posteriors[kid];
+            for (int32_t c2 = c; c2 < w; ++c2) {
+                const int32_t m2 = mask[c2];
+                if (!((m2 & 2) && (m2 >> 3) == key)) continue;
+                const double *ps = scratch + kExpectScratch * (int64_t) c2;
+                const double xe = ps[8];
+                for (int j = 0; j < 3; ++j) {
+                    const double p = ps[3 + j];
+                    e0 += p * xe;
+                    po += p;
+                    const double uk = e0 / po;
+                    e1 += p * (xe - uk) * (xe - uk);
+                }
+            }
+            X.event_exp[2 * kid] = e0;
+            X.event_exp[2 * kid + 1] = e1;
+            X.posteriors[kid] = po;
+            X.observed[kid] = 1;
         }
     }
     __syncthreads();
@@ -981,7 +1017,7 @@ static sa_status expectations_batch(const sa_read *reads, int64_t n, const sa_pa
         o.nk = sm->n_kmers;
         o.hdp = sm->emission == SA_EMIT_HDP;
         o.cap = o.hdp ? std::max<int64_t>(ex[i].assignment_capacity, 0) : 0;
-        o.scratch = total; total += up(sizeof(double) * 8 * (size_t) width[i]);
+        o.scratch = total; total += up(sizeof(double) * kExpectScratch * (size_t) width[i]);
         o.mask = total; total += up(sizeof(int32_t) * (size_t) width[i]);
         o.acc = total; total += up(sizeof(double) * 10);
         o.ee = total; total += up(sizeof(double) * 2 * (size_t) o.nk);
