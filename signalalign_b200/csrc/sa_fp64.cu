@@ -296,24 +296,46 @@ __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const Expec
     __syncthreads();
     const int32_t w = (R.xr[d2] - R.xl[d2]) / 2 + 1;
     if (tid == 0) {
+        // the accumulators in registers for the pass; a cell's posteriors are loaded whether or not
+        // its neighbours exist (unused values are never added), so loads of later cells need not
+        // wait for earlier cells' branches
+        double t[9];
+        for (int i = 0; i < 9; ++i) t[i] = acc[1 + i];
         acc[0] += total;   // hmmExpectations->likelihood += totalProbability, once per diagonal
+#pragma unroll 4
         for (int32_t c = 0; c < w; ++c) {
             const int32_t mk = mask[c];
             const double *ps = scratch + kExpectScratch * (int64_t) c;
+            const double p0 = ps[0], p1 = ps[1], p2 = ps[2], p3 = ps[3], p4 = ps[4], p5 = ps[5], p6 = ps[6],
+                         p7 = ps[7];
             if (mk & 1) {   // lower: M, X, Y -> X
-                acc[1 + S_M * 3 + S_X] += ps[0];
-                acc[1 + S_X * 3 + S_X] += ps[1];
-                acc[1 + S_Y * 3 + S_X] += ps[2];
+                t[S_M * 3 + S_X] += p0;
+                t[S_X * 3 + S_X] += p1;
+                t[S_Y * 3 + S_X] += p2;
             }
             if (mk & 2) {   // middle: M, X, Y -> M
+                t[S_M * 3 + S_M] += p3;
+                t[S_X * 3 + S_M] += p4;
+                t[S_Y * 3 + S_M] += p5;
+            }
+            if (mk & 4) {   // upper: M, Y -> Y
+                t[S_M * 3 + S_Y] += p6;
+                t[S_Y * 3 + S_Y] += p7;
+            }
+        }
+        for (int i = 0; i < 9; ++i) acc[1 + i] = t[i];
+        // cell_signal_updateExpectationsAndAssignments (pairwiseAligner.c:795-817): the HDP
+        // machine's assignments, in cell order and, within a cell, from match, gap-X, gap-Y
+        if (X.hdp) {
+            for (int32_t c = 0; c < w; ++c) {
+                const int32_t mk = mask[c];
+                if (!(mk & 2)) continue;
+                const double *ps = scratch + kExpectScratch * (int64_t) c;
                 const int32_t xmy = R.xl[d2] + 2 * c;
                 const int32_t y = (d2 - xmy) >> 1;
                 const int64_t kid = (mk >> 3) - 1;
                 for (int j = 0; j < 3; ++j) {
-                    const double p = ps[3 + j];
-                    acc[1 + j * 3 + S_M] += p;
-                    // cell_signal_updateExpectationsAndAssignments (pairwiseAligner.c:795-817)
-                    if (X.hdp && p >= X.threshold) {
+                    if (ps[3 + j] >= X.threshold) {
                         const int64_t at = *X.n_assign;
                         if (at < X.assign_cap) {
                             X.assign_kmer[at] = kid;
@@ -323,22 +345,21 @@ __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const Expec
                     }
                 }
             }
-            if (mk & 4) {   // upper: M, Y -> Y
-                acc[1 + S_M * 3 + S_Y] += ps[6];
-                acc[1 + S_Y * 3 + S_Y] += ps[7];
-            }
         }
     } else if (!X.hdp) {
         for (int32_t c = tid - 1; c < w; c += nt - 1) {
             const int32_t mk = mask[c];
             if (!(mk & 2)) continue;
             const int32_t key = mk >> 3;
-            bool first = true;
-            for (int32_t c2 = 0; c2 < c && first; ++c2) {
+            // an earlier cell of the anti-diagonal with the same k-mer makes this cell's updates
+            // (no early exit: the loads do not wait on one another)
+            bool dup = false;
+#pragma unroll 4
+            for (int32_t c2 = 0; c2 < c; ++c2) {
                 const int32_t m2 = mask[c2];
-                first = !((m2 & 2) && (m2 >> 3) == key);
+                dup |= (m2 & 2) != 0 && (m2 >> 3) == key;
             }
-            if (!first) continue;
+            if (dup) continue;
             const int64_t kid = key - 1;
             double e0 = X.event_exp[2 * kid], e1 = X.event_exp[2 * kid + 1], po = X.posteriors[kid];
             for (int32_t c2 = c; c2 < w; ++c2) {
