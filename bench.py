@@ -51,6 +51,9 @@ def parse_args():
     ap.add_argument("--config", type=int, default=1, choices=[1, 2, 3],
                     help="1: the 256-read Gaussian batch (default); 2: 128 HDP reads (6-mer ACEGT, 2000-point "
                          "grid); 3: 512 2D reads x {C, E} hypotheses, Gaussian and HDP mixed")
+    ap.add_argument("--expectations", action="store_true",
+                    help="EM expectations run instead: the reads' expectations in one batched call, against the CPU "
+                         "oracle on a bounded sample")
     ap.add_argument("--serve", action="store_true",
                     help="serving run instead: Poisson arrivals at --load of the measured capacity, p50/p99 latency")
     ap.add_argument("--serve-requests", type=int, default=400)
@@ -341,8 +344,73 @@ def run_config(args):
     print(json.dumps(line), flush=True)
 
 
+def run_expectations(args):
+    """EM expectations on the 256-read workload: every read's expectations (transitions, per-k-mer
+    emission expectations, likelihood) in one sa_getExpectationsBatch call (the plain FP64 form, one
+    CTA per read walking its regions in order), timed end to end from host buffers (planning, H2D,
+    kernel, D2H); the CPU oracle's expectations on a bounded sample, one read per host thread."""
+    import torch
+    from oracle import oracle as orc
+    from signalalign_b200 import api
+    torch.cuda.set_device(0)
+    cfg, m = model_and_reads(args.reads, args.seed)
+    sm = api.StateMachine.from_tables("ACGT", 6, m["t"], m["match"], m["gapy"], m["gapx"], emission=api.EMIT_DESCALED)
+    p = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=50, threshold=0.01)
+    reads = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                           scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
+    cells = []
+    for rd in cfg["reads"]:
+        L, R = orc.band(rd["anchors"], len(rd["reference"]) - 5, len(rd["events"]), 50)
+        cells.append(int(np.sum((R - L) // 2 + 1)))
+    for _ in range(max(1, args.warmup)):
+        api.getExpectationsBatch(reads[:4], p)
+    sampler = ClockSampler(0)
+    sampler.start()
+    launches0 = api.kernel_launch_count()
+    times, errors = [], 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, status = api.getExpectationsBatch(reads, p)
+        times.append(time.perf_counter() - t0)
+        errors += sum(1 for v in status if v)
+    launches = api.kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    value = sum(cells) * args.steps / sum(times)
+    # CPU: the oracle's expectations, smallest reads first, about 10 s of work over the host threads
+    threads = os.cpu_count() or 1
+    oms = [orc.OracleModel(m, orc.EMIT_DESCALED, rd["scale"], rd["shift"], 1.0) for rd in cfg["reads"]]
+    op = orc.params(threshold=0.01, expansion=50)
+    chosen, tot = [], 0
+    for i in np.argsort(cells):
+        if tot + cells[i] > 1.0e6 * 10.0 * threads and chosen:
+            break
+        chosen.append(int(i))
+        tot += cells[i]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda i: orc.expectations(oms[i], cfg["reads"][i]["reference"], cfg["reads"][i]["events"],
+                                               cfg["reads"][i]["anchors"], op), chosen))
+    cpu_dt = time.perf_counter() - t0
+    line = {"metric": "em_expectation_cells_per_sec", "value": value, "unit": "cells/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": 1e3 * statistics.mean(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD + ", expectations (pseudocounts 0.001)", "global_batch": len(reads),
+                       "cells_per_step": int(sum(cells))},
+            "e2e": {"value": value, "unit": "cells/s", "mode": "one sa_getExpectationsBatch call per step from host "
+                    "buffers: planning, H2D, kernel, D2H of every read's accumulators"},
+            "gpu_launches": launches, "errors": errors, "clocks": clocks,
+            "cpu_baseline": {"value": tot / cpu_dt, "unit": "cells/s", "cores": threads, "kind": "port",
+                             "sample": "%d reads (%d cells, smallest bands first), one read per thread, %.1f s"
+                                       % (len(chosen), tot, cpu_dt)}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.expectations:
+        run_expectations(args)
+        return
     if args.serve:
         run_serve(args)
         return
