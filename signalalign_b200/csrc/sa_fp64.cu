@@ -46,6 +46,8 @@ struct Region64 {
     const double2 *ev;
     const Window *win;
     double *F, *B, *P;
+    double *E;                    // ring like F: per path slot the match and extra-event emissions
+                                  // the forward sweep computed (the backward sweep reuses them)
     double threshold;
     double *loglik;
     int32_t *status;
@@ -85,6 +87,12 @@ __device__ __forceinline__ double *slot(double *base, const Region64 &R, int32_t
     return base + 3 * ((int64_t) (d % R.ring) * R.stride + (q - R.pfirst[(d + R.xl[d]) >> 1]));
 }
 
+// the match and extra-event emissions of path q's cell on anti-diagonal d, as the forward sweep
+// computed them (only where it needed them: a middle or an upper neighbour present)
+__device__ __forceinline__ double *eslot(const Region64 &R, int32_t d, int32_t q) {
+    return R.E + 2 * ((int64_t) (d % R.ring) * R.stride + (q - R.pfirst[(d + R.xl[d]) >> 1]));
+}
+
 __device__ __forceinline__ bool in_band(const Region64 &R, int32_t d, int32_t xmy) {
     return d >= 0 && d <= R.n && xmy >= R.xl[d] && xmy <= R.xr[d];
 }
@@ -116,9 +124,11 @@ __device__ void forward_cell(const Model64 &M, const Region64 &R, int32_t d, int
                 vX = log_add(vX, l[S_Y] + (e + M.t[T_SX]));
             }
         }
+        double *es = eslot(R, d, r);
         if (mi) {
             const double2 ev = R.ev[y - 1];
             const double e = emit_event(M, kid, ev.x, ev.y, true);
+            es[0] = e;
             for (int32_t q = q0; q < q1; ++q) {
                 if (!legal(R, q, r)) continue;
                 const double *m = slot(R.F, R, d - 2, q);
@@ -131,6 +141,7 @@ __device__ void forward_cell(const Model64 &M, const Region64 &R, int32_t d, int
             const double *u = slot(R.F, R, d - 1, r);
             const double2 ev = R.ev[y - 1];
             const double e = emit_event(M, kid, ev.x, ev.y, false);
+            es[1] = e;
             vY = log_add(vY, u[S_M] + (e + M.t[T_OY]));
             vY = log_add(vY, u[S_Y] + (e + M.t[T_EY]));
         }
@@ -148,7 +159,7 @@ __device__ void forward_cell(const Model64 &M, const Region64 &R, int32_t d, int
 // Path r of the cell receives from every path p of the pushing cell that r may precede, in
 // ascending p, each with p's emission.
 __device__ void backward_cell(const Model64 &M, const Region64 &R, int32_t d, int32_t xmy, int32_t top) {
-    const int32_t x = (d + xmy) >> 1, y = (d - xmy) >> 1;
+    const int32_t x = (d + xmy) >> 1;
     const bool mi = d + 2 <= top && in_band(R, d + 2, xmy), up = in_band(R, d + 1, xmy - 1),
                lo = in_band(R, d + 1, xmy + 1);
     // column x+1 exists whenever a cell of it is in the band
@@ -156,11 +167,10 @@ __device__ void backward_cell(const Model64 &M, const Region64 &R, int32_t d, in
     for (int32_t r = R.pfirst[x]; r < R.pfirst[x + 1]; ++r) {
         double vM = kNegInf, vX = kNegInf, vY = kNegInf;
         if (mi) {
-            const double2 ev = R.ev[y];
             for (int32_t p = p0; p < p1; ++p) {
                 if (!legal(R, r, p)) continue;
                 const double *m = slot(R.B, R, d + 2, p);
-                const double e = emit_event(M, R.pid[p], ev.x, ev.y, true);
+                const double e = eslot(R, d + 2, p)[0];   // the forward sweep's match emission of p
                 vM = log_add(vM, m[S_M] + (e + M.t[T_MC]));
                 vX = log_add(vX, m[S_M] + (e + M.t[T_MFGX]));
                 vY = log_add(vY, m[S_M] + (e + M.t[T_MFGY]));
@@ -168,8 +178,7 @@ __device__ void backward_cell(const Model64 &M, const Region64 &R, int32_t d, in
         }
         if (up) {
             const double *u = slot(R.B, R, d + 1, r);
-            const double2 ev = R.ev[y];
-            const double e = emit_event(M, R.pid[r], ev.x, ev.y, false);
+            const double e = eslot(R, d + 1, r)[1];   // its extra-event emission
             vM = log_add(vM, u[S_Y] + (e + M.t[T_OY]));
             vY = log_add(vY, u[S_Y] + (e + M.t[T_EY]));
         }
@@ -211,14 +220,13 @@ __device__ double total_probability(const Model64 &M, const Region64 &R, int32_t
         const int32_t dn = d + 1;
         double through = kNegInf;
         for (int32_t xmy = R.xl[dn]; xmy <= R.xr[dn]; xmy += 2) {
-            const int32_t x = (dn + xmy) >> 1, y = (dn - xmy) >> 1;
+            const int32_t x = (dn + xmy) >> 1;
             const bool mi = in_band(R, d - 1, xmy);
             double cell_total = kNegInf;
             for (int32_t r = R.pfirst[x]; r < R.pfirst[x + 1]; ++r) {
                 double m = kNegInf;
                 if (mi) {
-                    const double2 ev = R.ev[y - 1];
-                    const double e = emit_event(M, R.pid[r], ev.x, ev.y, true);
+                    const double e = eslot(R, dn, r)[0];   // the forward sweep's match emission
                     for (int32_t q = R.pfirst[x - 1]; q < R.pfirst[x]; ++q) {
                         if (!legal(R, q, r)) continue;
                         const double *f = slot(R.F, R, d - 1, q);
@@ -274,7 +282,7 @@ __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const Expec
         if (mi) {
             const double *m = slot(R.F, R, d2 - 2, R.pfirst[x - 1]);
             const double2 ev = R.ev[y - 1];
-            const double e = emit_event(M, kid, ev.x, ev.y, true);
+            const double e = eslot(R, d2, r)[0];   // the forward sweep's emissions of the cell
             ps[3] = exp(m[S_M] + cur[S_M] + (e + M.t[T_MC]) - total);
             ps[4] = exp(m[S_X] + cur[S_M] + (e + M.t[T_MFGX]) - total);
             ps[5] = exp(m[S_Y] + cur[S_M] + (e + M.t[T_MFGY]) - total);
@@ -285,8 +293,7 @@ __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const Expec
         }
         if (up) {
             const double *u = slot(R.F, R, d2 - 1, r);
-            const double2 ev = R.ev[y - 1];
-            const double e = emit_event(M, kid, ev.x, ev.y, false);
+            const double e = eslot(R, d2, r)[1];
             ps[6] = exp(u[S_M] + cur[S_Y] + (e + M.t[T_OY]) - total);
             ps[7] = exp(u[S_Y] + cur[S_Y] + (e + M.t[T_EY]) - total);
         }
@@ -594,11 +601,12 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
     for (const PlainRegion &pr : s->regs) p_total += (size_t) (pr.rg.lX + pr.rg.lY + 1);
     const size_t o_P = take(p_total * sizeof(double));
     s->p_bytes = p_total * sizeof(double);
-    std::vector<size_t> o_F(nreg), o_B(nreg);
+    std::vector<size_t> o_F(nreg), o_B(nreg), o_E(nreg);
     for (size_t i = 0; i < nreg; ++i) {
         const size_t ring_bytes = 3 * sizeof(double) * (size_t) s->regs[i].ring * (size_t) s->regs[i].stride;
         o_F[i] = take(ring_bytes);
         o_B[i] = take(ring_bytes);
+        o_E[i] = take(ring_bytes / 3 * 2);
     }
     const size_t o_out = take((size_t) s->cap * sizeof(sa_aligned_pair));
     const size_t o_tag = take((size_t) s->cap * sizeof(int32_t));
@@ -650,6 +658,7 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
             r.win = reinterpret_cast<const Window *>(dev + off[i].win);
             r.F = reinterpret_cast<double *>(dev + o_F[i]);
             r.B = reinterpret_cast<double *>(dev + o_B[i]);
+            r.E = reinterpret_cast<double *>(dev + o_E[i]);
             r.P = s->d_P + p_at;
             p_at += (size_t) r.n + 1;
             r.loglik = s->d_loglik + i;
