@@ -1023,15 +1023,18 @@ static sa_status expectations_batch(const sa_read *reads, int64_t n, const sa_pa
     std::vector<int64_t> run;   // reads that run, in order
     for (int64_t i = 0; i < n; ++i)
         if (!read_status[i] && s->read_count[i] > 0) run.push_back(i);
+    if (run.empty()) {   // nothing for the device: no device call at all
+        for (int64_t i = 0; i < n; ++i)
+            if (!read_status[i]) ex[i].n_assignments = 0;
+        plain_destroy(s);
+        return SA_OK;
+    }
     for (int64_t i : run)
         if (!st) st = ensure_device_model(const_cast<sa_state_machine *>(reads[i].sm));
     int prev_dev = 0;
     if (!st && cudaGetDevice(&prev_dev) != cudaSuccess) st = SA_E_CUDA;
     if (!st && cudaSetDevice(s->device) != cudaSuccess) st = SA_E_CUDA;
-    if (st || run.empty()) {
-        if (!st)
-            for (int64_t i = 0; i < n; ++i)
-                if (!read_status[i]) ex[i].n_assignments = 0;
+    if (st) {
         plain_destroy(s);
         return st;
     }

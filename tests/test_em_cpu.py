@@ -159,3 +159,30 @@ def test_expectations_file_hdp_bytes(api):
     with pytest.raises(api.SAError) as ei:      # emissions are loaded into Gaussian machines only
         api.loadExpectationsIntoStateMachine(sm, dict(hmm, event_model=sm.tables()["match"]))
     assert ei.value.status == 7
+
+
+def test_expectations_batch_statuses_without_device_work(api):
+    """sa_getExpectationsBatch: argument and parameter errors fail the call; reads that cannot run get
+    their own status (an HDP machine without its tables, an 'X' the ACGT alphabet cannot expand) and,
+    when no read runs, nothing touches the device"""
+    import ctypes as C
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    assert api.getExpectationsBatch([], p) == ([], [])
+    assert api.lib().sa_getExpectationsBatch(None, -1, C.byref(p), None, None) == 1
+    assert api.lib().sa_getExpectationsBatch(None, 2, C.byref(p), None, None) == 1
+    cfg = synth.config0()
+    m = W.gaussian_model(cfg)
+    rd = cfg["reads"][0]
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED, rd)
+    bad = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=51)   # must be even
+    with pytest.raises(api.SAError) as ei:
+        api.getExpectationsBatch([api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"],
+                                                anchors=rd["anchors"])], bad)
+    assert ei.value.status == 1
+    hdp_sm = api.StateMachine.from_tables("ACGT", 6, m["t"], m["match"], m["gapy"], m["gapx"], emission=api.EMIT_HDP)
+    x_ref = rd["reference"][:100] + "X" + rd["reference"][101:]
+    reads = [api.ReadInput(sm=hdp_sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"]),
+             api.ReadInput(sm=sm, reference=x_ref, events=rd["events"], anchors=rd["anchors"])]
+    got, status = api.getExpectationsBatch(reads, p)
+    assert status == [7, 2]
+    assert got[1]["likelihood"] == 0.0 and got[1]["transitions"][0, 0] == 0.001   # untouched accumulators
