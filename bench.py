@@ -59,6 +59,7 @@ def parse_args():
     ap.add_argument("--serve-requests", type=int, default=400)
     ap.add_argument("--load", type=float, default=0.8)
     ap.add_argument("--serve-budget", type=int, default=200_000_000, help="band cells in flight")
+    ap.add_argument("--serve-streams", type=int, default=8, help="micro-batches in flight")
     return ap.parse_args()
 
 
@@ -209,7 +210,7 @@ def run_serve(args):
         reqs.append((api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
                                    scale=rd["scale"], shift=rd["shift"]), int(L), int(np.sum((hi - lo) // 2 + 1))))
     p = api.pairwiseAlignmentBandingParameters_construct()
-    srv = api.Server(device=0, max_inflight_cells=args.serve_budget, max_batches=8)
+    srv = api.Server(device=0, max_inflight_cells=args.serve_budget, max_batches=args.serve_streams)
     try:
         for q, _, _ in reqs[:8]:                       # warm-up: tables resident, pools filled
             t = srv.submit(q, p)
@@ -253,7 +254,7 @@ def run_serve(args):
             "config": {"workload": "%d requests, log-normal spans (median 8 kb, sigma 0.6, clipped 500 bp-100 kb), "
                                    "6-mer ACGT / ACEGT Gaussian tables per request, Poisson arrivals at %.0f%% of "
                                    "measured capacity" % (n, 100 * args.load),
-                       "band_cell_budget": args.serve_budget, "streams": 8},
+                       "band_cell_budget": args.serve_budget, "streams": args.serve_streams},
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "p50_ms_8to12kb": float(np.percentile(ten, 50)) if len(ten) else None,
             "p99_ms_8to12kb": float(np.percentile(ten, 99)) if len(ten) else None,
