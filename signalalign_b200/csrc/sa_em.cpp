@@ -114,6 +114,7 @@ sa_status sa_stateMachine_loadExpectations(sa_state_machine *sm, const double tr
                                            const double *event_model) {
     if (!sm || !transitions) return SA_E_ARG;
     if (event_model && sm->type != SA_THREE_STATE) return SA_E_UNSUPPORTED;
+    if (event_model && sm->n_kmers < 2) return SA_E_ARG;   // the gap-Y index i + 5 needs two k-mers
     const double *T = transitions;
     // continuousPairHmm_loadTransitionsIntoStateMachine (continuousHmm.c:321-339); log(0) = -inf is
     // the reference's LOG_ZERO
@@ -131,7 +132,6 @@ sa_status sa_stateMachine_loadExpectations(sa_state_machine *sm, const double tr
     // each k-mer's level mean and sd; the gap-Y table takes the sd x 1.75 at [i * 5 + 1] and the mean
     // at [i + 5], the index the reference writes (so later k-mers' means overwrite rows 1 onwards)
     const int64_t n = sm->n_kmers;
-    if (n < 2) return SA_E_ARG;
     for (int64_t i = 0; i < n; ++i) {
         const double mean = event_model[5 * i], sd = event_model[5 * i + 1];
         sm->match[5 * i] = mean;
