@@ -45,9 +45,9 @@ def test_em_transitions_only_never_lowers_the_likelihood():
 
 
 def test_continuousPairHmm_em_property():
-    """test_continuousPairHmm_em (tests/stateMachineTests.c:1210-1260): ten rounds of expectations
+    """test_continuousPairHmm_em (tests/stateMachineTests.c:1210-1260): ten iterations of expectations
     (pseudocounts 0.001, not ragged), continuousPairHmm_normalize and both loads into the machine
-    (the gap-Y means at the reference's i + 5 included); from the third round on the previous
+    (the gap-Y means at the reference's i + 5 included); from the third iteration on the previous
     likelihood is at most 0.85 x the current one."""
     cfg = synth.config0()
     lik, _ = _oracle_em(W.gaussian_model(cfg), cfg["reads"][0], orc.EMIT_DESCALED, 10, True, 0.001)
@@ -57,7 +57,7 @@ def test_continuousPairHmm_em_property():
 
 def test_hdpHmm_emTransitions_property():
     """test_hdpHmm_emTransitions (tests/stateMachineTests.c:1262-1305): the HDP machine, transition
-    pseudocount 0, only the transitions normalised and loaded; every round's previous likelihood is
+    pseudocount 0, only the transitions normalised and loaded; every iteration's previous likelihood is
     at most 0.95 x the current one."""
     hc = W.small_hdp_config()
     hdp = W.hdp_dict(hc["hdp"], len(hc["alphabet"]) ** hc["k"])

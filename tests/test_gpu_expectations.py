@@ -113,12 +113,12 @@ def test_expectations_hdp_assignments(api, split):
     assert np.array_equal(got["assignments"], want["assignments"])
 
 
-def test_em_rounds_match_oracle_and_batches_follow(api):
-    """Three EM rounds on the device (expectations, continuousPairHmm_normalize, both loads into the
+def test_em_iterations_match_oracle_and_batches_follow(api):
+    """Three EM iterations on the device (expectations, continuousPairHmm_normalize, both loads into the
     machine, as test_continuousPairHmm_em runs them, stateMachineTests.c:1210-1260) against the same
-    rounds on the oracle.  Re-estimated sds of k-mers seen once shrink by tens of orders of magnitude
-    a round, so rounding differences grow: the oracle perturbed by 1e-9 moves 6e-8 after three
-    rounds; rtol 1e-6.  Then a batch on the re-estimated machine, whose gap-Y table no longer follows
+    iterations on the oracle.  Re-estimated sds of k-mers seen once shrink by tens of orders of magnitude
+    an iteration, so rounding differences grow: the oracle perturbed by 1e-9 moves 6e-8 after three
+    iterations; rtol 1e-6.  Then a batch on the re-estimated machine, whose gap-Y table no longer follows
     its match table: its reads run in the plain FP64 form, identical to the single-read entry."""
     cfg = synth.config0()
     m = W.gaussian_model(cfg)
@@ -142,9 +142,9 @@ def test_em_rounds_match_oracle_and_batches_follow(api):
     assert len(alone) > 100 and np.array_equal(alone, b.pairs(0))
 
 
-def test_hdp_em_transition_rounds_match_oracle(api):
+def test_hdp_em_transition_iterations_match_oracle(api):
     """test_hdpHmm_emTransitions (stateMachineTests.c:1262-1305) on the device: the HDP machine,
-    transition pseudocount 0, transitions normalised and loaded each round, against the oracle"""
+    transition pseudocount 0, transitions normalised and loaded each iteration, against the oracle"""
     from oracle import formats
     hc = W.small_hdp_config()
     hdp = W.hdp_dict(hc["hdp"], len(hc["alphabet"]) ** hc["k"])
