@@ -186,3 +186,23 @@ def test_expectations_batch_statuses_without_device_work(api):
     got, status = api.getExpectationsBatch(reads, p)
     assert status == [7, 2]
     assert got[1]["likelihood"] == 0.0 and got[1]["transitions"][0, 0] == 0.001   # untouched accumulators
+
+
+def test_expectations_file_loads_as_a_model(api, gauss_case, tmp_path):
+    """The first three lines of an expectations file are a .model (stateMachine3_loadFromFile,
+    stateMachine.c:1328-1426): the normalised transitions and the re-estimated event model written by
+    sa_writeExpectations come back through the model reader at the file's six decimals (with the
+    reader's own rules: gap-Y sd x 1.75, gap-Y -> gap-X into SWITCH_TO_Y)"""
+    m, rd, ex = gauss_case
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED, rd)
+    hmm = api.normalizeExpectations(_hmm(api, sm, ex))
+    path = tmp_path / "trained.hmm"
+    api.writeExpectations(path, sm, hmm)
+    back = api.StateMachine.load(str(path)).tables()
+    T = np.asarray(hmm["transitions"])
+    want_p = [T[0][0], T[1][0], T[2][0], T[0][1], T[0][2], T[1][1], T[2][2], 0.0, T[2][1]]
+    np.testing.assert_allclose(np.exp(back["t"]), want_p, rtol=0, atol=5e-7)   # "%f": six decimals
+    assert back["t"][7] == -np.inf
+    em = np.asarray(hmm["event_model"]).reshape(-1, 5)
+    np.testing.assert_allclose(back["match"], em, rtol=0, atol=5e-7)
+    np.testing.assert_allclose(back["gapy"][:, 1], 1.75 * back["match"][:, 1], rtol=1e-15)
