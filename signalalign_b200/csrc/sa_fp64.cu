@@ -43,6 +43,7 @@ struct Region64 {
     int64_t ev_base;              // the region's first event in the read (split regions start later)
     const int32_t *xl, *xr;
     const int32_t *pfirst, *pid, *ppre, *psuf;
+    const int32_t *row;           // per anti-diagonal d: (d mod ring) * stride - its first path slot
     const double2 *ev;
     const Window *win;
     double *F, *B, *P;
@@ -84,13 +85,13 @@ struct ExpectOut {
 
 // the 3 states of path q in the cell of anti-diagonal d (q must belong to that cell's column)
 __device__ __forceinline__ double *slot(double *base, const Region64 &R, int32_t d, int32_t q) {
-    return base + 3 * ((int64_t) (d % R.ring) * R.stride + (q - R.pfirst[(d + R.xl[d]) >> 1]));
+    return base + 3 * ((int64_t) R.row[d] + q);
 }
 
 // the match and extra-event emissions of path q's cell on anti-diagonal d, as the forward sweep
 // computed them (only where it needed them: a middle or an upper neighbour present)
 __device__ __forceinline__ double *eslot(const Region64 &R, int32_t d, int32_t q) {
-    return R.E + 2 * ((int64_t) (d % R.ring) * R.stride + (q - R.pfirst[(d + R.xl[d]) >> 1]));
+    return R.E + 2 * ((int64_t) R.row[d] + q);
 }
 
 __device__ __forceinline__ bool in_band(const Region64 &R, int32_t d, int32_t xmy) {
@@ -511,7 +512,7 @@ namespace {
 struct PlainRegion {
     int32_t read = 0, model = 0;
     Region rg;
-    std::vector<int32_t> xl, xr, pfirst, pid, ppre, psuf;
+    std::vector<int32_t> xl, xr, pfirst, pid, ppre, psuf, row;
     int32_t ring = 3, stride = 1, max_paths = 1;
     size_t ev_off = 0;   // first event of the region in the set's event array
 };
@@ -574,7 +575,7 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
     const size_t o_regions = take(nreg * sizeof(Region64));
     const size_t o_models = take(s->models.size() * sizeof(Model64));
     std::vector<Region64> R(nreg);
-    struct Off { size_t xl, xr, pfirst, pid, ppre, psuf, win; };
+    struct Off { size_t xl, xr, pfirst, pid, ppre, psuf, row, win; };
     std::vector<Off> off(nreg);
     for (size_t i = 0; i < nreg; ++i) {
         const PlainRegion &pr = s->regs[i];
@@ -584,6 +585,7 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
         off[i].pid = take(pr.pid.size() * sizeof(int32_t));
         off[i].ppre = take(pr.ppre.size() * sizeof(int32_t));
         off[i].psuf = take(pr.psuf.size() * sizeof(int32_t));
+        off[i].row = take(pr.row.size() * sizeof(int32_t));
         off[i].win = take(pr.rg.windows.size() * sizeof(Window));
     }
     const size_t o_events = take(s->events.size() * sizeof(double2));
@@ -634,6 +636,7 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
             put(off[i].pid, pr.pid.data(), pr.pid.size() * sizeof(int32_t));
             put(off[i].ppre, pr.ppre.data(), pr.ppre.size() * sizeof(int32_t));
             put(off[i].psuf, pr.psuf.data(), pr.psuf.size() * sizeof(int32_t));
+            put(off[i].row, pr.row.data(), pr.row.size() * sizeof(int32_t));
             put(off[i].win, pr.rg.windows.data(), pr.rg.windows.size() * sizeof(Window));
             Region64 &r = R[i];
             std::memset(&r, 0, sizeof(r));
@@ -654,6 +657,7 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
             r.pid = reinterpret_cast<const int32_t *>(dev + off[i].pid);
             r.ppre = reinterpret_cast<const int32_t *>(dev + off[i].ppre);
             r.psuf = reinterpret_cast<const int32_t *>(dev + off[i].psuf);
+            r.row = reinterpret_cast<const int32_t *>(dev + off[i].row);
             r.ev = reinterpret_cast<const double2 *>(dev + o_events) + pr.ev_off;
             r.win = reinterpret_cast<const Window *>(dev + off[i].win);
             r.F = reinterpret_cast<double *>(dev + o_F[i]);
@@ -732,6 +736,11 @@ void plan_region(const PathTable &pt, int32_t asz, int64_t kpow, PlainRegion &pr
     int32_t span = 0;
     for (const Window &w : rg.windows) span = std::max(span, w.D - w.T + 1);
     pr.ring = std::max(3, span) + 1;
+    // ring row of each anti-diagonal, so a slot lookup is one load instead of a modulo and two
+    // dependent loads
+    pr.row.resize((size_t) n + 1);
+    for (int32_t d = 0; d <= n; ++d)
+        pr.row[d] = (int32_t) ((int64_t) (d % pr.ring) * pr.stride - pr.pfirst[(d + rg.xmy_l[d]) / 2]);
 }
 
 }  // namespace
