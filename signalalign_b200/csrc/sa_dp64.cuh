@@ -16,6 +16,8 @@ struct Model64 {
     int32_t pad;
     double t[9];                 // transitions, StateMachine3 order
     const double *match, *gapy, *gapx;
+    const double *klog;          // per k-mer: log sd and log lambda of the match and gap-Y rows
+                                 // (the device's own log of the table values, computed once)
     double scale, shift, var;
     int64_t grid_length;
     const double *grid, *density, *slope;
@@ -39,21 +41,7 @@ __device__ __forceinline__ double log_add(double x, double y) {
     return (y == kNegInf || x - y >= 7.5) ? x : lookup(x - y) + y;
 }
 
-// emissions_signal_logGaussPdf / logInvGaussPdf / descaleEventMean_JordanStyle (stateMachine.c:226-289)
-__device__ __forceinline__ double log_gauss(double x, double mu, double sigma) {
-    if (sigma == 0.0) return kNegInf;
-    double ls = log(sigma);
-    double a = (x - mu) / sigma;
-    return -0.91893853320467267 - ls + (-0.5 * a * a);
-}
-
-__device__ __forceinline__ double log_inv_gauss(double n, double mu, double lambda) {
-    double ln = log(n);
-    double a = (n - mu) / mu;
-    double ll = log(lambda);
-    return (ll - 1.8378770664093453 - 3 * ln - lambda * a * a / n) / 2;
-}
-
+// emissions_signal_descaleEventMean_JordanStyle (stateMachine.c:285-289)
 __device__ __forceinline__ double descale(double e, double mu, double scale, double shift, double var) {
     return (e + var * mu - scale * mu - shift) / var;
 }
@@ -90,10 +78,20 @@ __device__ __forceinline__ double emit_event(const Model64 &M, int32_t kid, doub
         return log((1 / M.var) * d);
     }
     const double *tab = (match ? M.match : M.gapy) + (int64_t) kid * 5;
+    const double *lg = M.klog + 4 * (int64_t) kid;
     double mu = tab[0], sd = tab[1];
     double m = M.emission == 1 ? descale(mean, mu, M.scale, M.shift, M.var) : mean;
-    double lm = log_gauss(m, mu, sd);
-    double ln = log_inv_gauss(noise, tab[2], tab[4]);
+    // emissions_signal_logGaussPdf and logInvGaussPdf (stateMachine.c:226-247), the logs of the
+    // table's sd and lambda looked up
+    double lm = kNegInf;
+    if (sd != 0.0) {
+        double a = (m - mu) / sd;
+        lm = -0.91893853320467267 - lg[match ? 0 : 1] + (-0.5 * a * a);
+    }
+    const double nmu = tab[2], lambda = tab[4];
+    double ln_n = log(noise);
+    double b = (noise - nmu) / nmu;
+    double ln = (lg[match ? 2 : 3] - 1.8378770664093453 - 3 * ln_n - lambda * b * b / noise) / 2;
     return lm + ln;
 }
 

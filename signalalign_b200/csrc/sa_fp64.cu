@@ -501,7 +501,36 @@ __global__ void __launch_bounds__(128) region_kernel(const Model64 *models, cons
     run_region(models[R.model], R, (int32_t) blockIdx.x, O, X, acc);
 }
 
+// the per-k-mer logs the FP64 emissions use, with the same device log as an inline call
+__global__ void kmer_logs_kernel(const double *match, const double *gapy, int64_t n, double *out) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+        out[4 * i + 0] = log(match[5 * i + 1]);
+        out[4 * i + 1] = log(gapy[5 * i + 1]);
+        out[4 * i + 2] = log(match[5 * i + 4]);
+        out[4 * i + 3] = log(gapy[5 * i + 4]);
+    }
+}
+
 }  // namespace
+
+// Called with the machine's device current and its tables resident; synchronous, so the table is
+// ready for launches on any stream.
+sa_status compute_kmer_logs(sa_state_machine *sm) {
+    const int64_t n = sm->n_kmers;
+    DeviceModel &d = sm->dev;
+    if (cudaMalloc(reinterpret_cast<void **>(&d.klog), sizeof(double) * 4 * (size_t) std::max<int64_t>(n, 1)) !=
+        cudaSuccess) {
+        d.klog = nullptr;
+        return SA_E_NOMEM;
+    }
+    if (n > 0) {
+        const int64_t blocks = std::min<int64_t>((n + 255) / 256, 4096);
+        kmer_logs_kernel<<<(unsigned) blocks, 256>>>(d.match, d.gapy, n, d.klog);
+        count_launch();
+    }
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return SA_E_CUDA;
+    return SA_OK;
+}
 
 // ------------------------------------------------------------------------------------------------
 // plain sets: host side
@@ -678,6 +707,7 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
             M.match = sm->dev.match;
             M.gapy = sm->dev.gapy;
             M.gapx = sm->dev.gapx;
+            M.klog = sm->dev.klog;
             M.scale = s->models[m].scale;
             M.shift = s->models[m].shift;
             M.var = s->models[m].var;

@@ -536,7 +536,7 @@ void free_device_model(sa_state_machine *sm) {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(d.device);
-    cudaFree(d.match); cudaFree(d.gapy); cudaFree(d.gapx);
+    cudaFree(d.match); cudaFree(d.gapy); cudaFree(d.gapx); cudaFree(d.klog);
     cudaFree(d.hdp_grid); cudaFree(d.hdp_density); cudaFree(d.hdp_slope); cudaFree(d.hdp_kmer_row);
     cudaFree(d.kc32); cudaFree(d.gapx32);
     int dev = d.device;
@@ -602,6 +602,7 @@ sa_status ensure_device_model(sa_state_machine *sm) {
         if (!st) st = upload(&d.hdp_slope, h.slope.data(), h.slope.size());
         if (!st) st = upload(&d.hdp_kmer_row, h.kmer_row.data(), h.kmer_row.size());
     }
+    if (!st) st = compute_kmer_logs(sm);
     cudaSetDevice(prev);
     if (st) {
         free_device_model(sm);

@@ -45,6 +45,7 @@ struct DeviceModel {
     int device = 0;
     // FP64 tables (reference layout)
     double *match = nullptr, *gapy = nullptr, *gapx = nullptr;
+    double *klog = nullptr;   // per k-mer: log sd (match, gap-Y), log lambda (match, gap-Y)
     double *hdp_grid = nullptr, *hdp_density = nullptr, *hdp_slope = nullptr;
     int64_t *hdp_kmer_row = nullptr;
     // FP32 tables
@@ -120,6 +121,9 @@ sa_status build_paths(const sa_state_machine *sm, const char *reference, int64_t
 
 // device model upload (both kernel forms)
 sa_status ensure_device_model(sa_state_machine *sm);
+
+// the plain FP64 form's per-k-mer logs (DeviceModel::klog) from the resident tables, on the device
+sa_status compute_kmer_logs(sa_state_machine *sm);
 
 // The batched FP32 form takes the extra-event (gap-Y) emission's level mean, noise mean and noise
 // lambda from the match table and only the level sd from the gap-Y table.  True when the machine's
