@@ -243,7 +243,9 @@ class StateMachine:
                                                 nhdp_file.encode() if nhdp_file else None,
                                                 int(set_hdp_expected_values), device, C.byref(h))
         _check(st, "stateMachine3_loadFromFile(%s)" % model_file)
-        return cls(h.value)
+        sm = cls(h.value)
+        sm.emission = emission
+        return sm
 
     @classmethod
     def from_tables(cls, alphabet, kmer_length, transitions, match, gap_y, gap_x, emission=EMIT_DESCALED,
@@ -256,7 +258,9 @@ class StateMachine:
                                               t.ctypes.data_as(_f64p), m.ctypes.data_as(_f64p),
                                               y.ctypes.data_as(_f64p), x.ctypes.data_as(_f64p), device, C.byref(h))
         _check(st, "stateMachine_fromTables")
-        return cls(h.value)
+        sm = cls(h.value)
+        sm.emission = emission
+        return sm
 
     def set_hdp(self, grid_start, grid_stop, grid_length, density, slope, kmer_row):
         d, s = _f64(density, grid_length), _f64(slope, grid_length)
@@ -777,8 +781,9 @@ def getExpectationsBatch(reads, p, states=None, transition_pseudocount=0.001, em
         po = np.ascontiguousarray(st["posteriors"], dtype=np.float64).copy()
         ob = np.ascontiguousarray(st["observed"], dtype=np.uint8).copy()
         ex, _ = _expectations_struct(dict(st, event_expectations=ee, posteriors=po, observed=ob, assignments=None))
-        cap = 4 * (len(r.reference) + len(r.events)) + 64
-        ak, ae = np.zeros(cap, np.int64), np.zeros(cap, np.int64)
+        # assignment lists: the HDP machine's only
+        cap = 4 * (len(r.reference) + len(r.events)) + 64 if getattr(r.sm, "emission", EMIT_HDP) == EMIT_HDP else 0
+        ak, ae = np.zeros(max(cap, 1), np.int64), np.zeros(max(cap, 1), np.int64)
         ex.assignment_kmers, ex.assignment_events = ak.ctypes.data_as(_i64p), ae.ctypes.data_as(_i64p)
         ex.assignment_capacity = cap
         exs[i] = ex
