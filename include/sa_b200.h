@@ -246,6 +246,9 @@ void sa_batch_destroy(sa_batch *b);
  *     sa_batch_create, sa_getAlignedPairsUsingAnchors); otherwise SA_E_ARG.
  *   - A batch that needs more than SA_NOALLOC_SCRATCH_BYTES is rejected with SA_E_CAPACITY before
  *     any device work; *scratch_bytes (optional) receives the bytes the batch needs in every case.
+ *   - Reads only the plain FP64 form runs (references with 'X' positions; machines whose gap-Y
+ *     table has its own level means or noise, as after sa_stateMachine_loadExpectations with an
+ *     event model) get read status SA_E_UNSUPPORTED; the others are aligned.
  *   - What must be zero when the kernel starts (the region queue counter, per-read status words and
  *     per-region pair counts) is cleared by the call itself on `stream` before every launch; every
  *     other byte the kernel reads is written earlier in the same call.
