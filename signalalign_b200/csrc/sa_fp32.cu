@@ -663,7 +663,8 @@ sa_status sa_batch_download(sa_batch *b, void *stream) {
     b->read_ll.assign(b->n_reads, 0.0);
     for (int64_t r = 0; r < b->n_reads && !st; ++r) {
         if (b->plain_of[r] >= 0) {
-            b->read_ll[r] = plain_log_likelihood(b->plain, b->plain_of[r]);
+            // the no-allocation entry makes no plain set: its reads report SA_E_UNSUPPORTED
+            if (b->plain) b->read_ll[r] = plain_log_likelihood(b->plain, b->plain_of[r]);
             continue;
         }
         for (int64_t i = 0; i < b->read_n_regions[r]; ++i) b->read_ll[r] += b->loglik[b->read_first_region[r] + i];

@@ -99,3 +99,33 @@ def test_noalloc_matches_align_batch_twice():
             assert err <= FP32_TOL, (call, i, err)
             ll_w, ll_g = ref.log_likelihood(i), got.log_likelihood(i)
             assert abs(ll_g - ll_w) <= 1e-3 * abs(ll_w), (call, i, ll_w, ll_g)
+
+
+def test_noalloc_leaves_plain_form_reads_unsupported():
+    """Reads only the plain FP64 form runs get SA_E_UNSUPPORTED from the no-allocation entry (it
+    allocates nothing for that form): a reference with an 'X' position, and a read of a machine
+    whose gap-Y table no longer follows its match table (after the EM emission load).  The other
+    reads of the call are aligned as sa_align_batch aligns them."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    cfg = synth.config1(seed=13, n_reads=3, span=(300, 900))
+    m = W.gaussian_model(cfg)
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED)
+    em_sm = W.gpu_model(api, m, orc.EMIT_DESCALED)
+    table = em_sm.tables()
+    api.loadExpectationsIntoStateMachine(em_sm, dict(transitions=np.full((3, 3), 1.0 / 3.0),
+                                                     event_model=table["match"]))
+    reads = _inputs(sm, cfg["reads"])
+    rd = cfg["reads"][1]
+    reads[1] = api.ReadInput(sm=sm, reference=rd["reference"][:50] + "X" + rd["reference"][51:], events=rd["events"],
+                             anchors=rd["anchors"], scale=rd["scale"], shift=rd["shift"],
+                             degenerate=api.CANONICAL_VARIANTS)   # X -> A, C, G, T: four paths
+    reads[2] = _inputs(em_sm, [cfg["reads"][2]])[0]
+    p = _params()
+    ref = api.align_batch(reads, p)          # allocating: every read runs; tables resident
+    got = api.align_batch_noalloc(reads, p)
+    assert [got.status(i) for i in range(3)] == [0, 7, 7]
+    assert ref.status(1) == 0 and ref.status(2) == 0 and len(ref.pairs(2)) > 0
+    err = W.max_posterior_error(ref.pairs(0), got.pairs(0), p.threshold)
+    assert err <= FP32_TOL
