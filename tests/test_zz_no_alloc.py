@@ -77,6 +77,7 @@ def test_requires_resident_device_tables():
 
 
 @pytest.mark.gpu
+@pytest.mark.gpu
 def test_noalloc_matches_align_batch_twice():
     import torch
     if not torch.cuda.is_available():
@@ -101,6 +102,7 @@ def test_noalloc_matches_align_batch_twice():
             assert abs(ll_g - ll_w) <= 1e-3 * abs(ll_w), (call, i, ll_w, ll_g)
 
 
+@pytest.mark.gpu
 def test_noalloc_leaves_plain_form_reads_unsupported():
     """Reads only the plain FP64 form runs get SA_E_UNSUPPORTED from the no-allocation entry (it
     allocates nothing for that form): a reference with an 'X' position, and a read of a machine
