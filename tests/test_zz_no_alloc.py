@@ -77,7 +77,6 @@ def test_requires_resident_device_tables():
 
 
 @pytest.mark.gpu
-@pytest.mark.gpu
 def test_noalloc_matches_align_batch_twice():
     import torch
     if not torch.cuda.is_available():
