@@ -1,4 +1,4 @@
-// Plain FP64 form: one region (read, or split sub-region) per kernel launch, one CTA sweeping the
+// Plain FP64 form: one region (read, or split sub-region) per CTA, sweeping the
 // band anti-diagonal by anti-diagonal in log space with the reference's logAdd, windowed traceback
 // and every-10th-anti-diagonal total-probability refresh (getPosteriorProbsWithBanding,
 // pairwiseAligner.c:1282-1420).  It is the parity anchor of the engine: results agree with
@@ -18,6 +18,11 @@
 //                    on T .. D only, and ring > D - T for every window (the reference also keeps only
 //                    the current window's forward diagonals, pairwiseAligner.c:1390-1410).  The
 //                    paths of one anti-diagonal are consecutive (x rises by one from cell to cell).
+//   row[d]           (d mod ring) * stride - first path of anti-diagonal d: slot of path q on d is
+//                    row[d] + q
+//   E                2 doubles per slot (match and extra-event emissions), a ring like F, written by
+//                    the forward sweep where it needs them and read back by the backward sweep, the
+//                    refresh totals and the expectations
 //   P                refresh total probabilities, indexed by anti-diagonal
 //   out, tag         the set's pairs (shared, appended by atomics) and each pair's region
 #include <algorithm>
