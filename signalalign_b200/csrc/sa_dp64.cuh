@@ -26,19 +26,25 @@ struct Model64 {
 
 // lookup + logAdd (pairwiseAligner.c:237-254): log(e^x + e^y) by a 4-piece cubic in the difference,
 // exact max once the difference reaches 7.5; float literals evaluated in double as in the reference.
+// The piece's coefficients are selected, not branched to, and the cubic is evaluated in the
+// reference's order, so results are the reference's bit for bit.
 __device__ __forceinline__ double lookup(double d) {
-    if (d <= 1.00f)
-        return ((-0.009350833524763f * d + 0.130659527668286f) * d + 0.498799810682272f) * d + 0.693203116424741f;
-    if (d <= 2.50f)
-        return ((-0.014532321752540f * d + 0.139942324101744f) * d + 0.495635523139337f) * d + 0.692140569840976f;
-    if (d <= 4.50f)
-        return ((-0.004605031767994f * d + 0.063427417320019f) * d + 0.695956496475118f) * d + 0.514272634594009f;
-    return ((-0.000458661602210f * d + 0.009695946122598f) * d + 0.930734667215156f) * d + 0.168037164329057f;
+    const bool p0 = d <= 1.00f, p1 = d <= 2.50f, p2 = d <= 4.50f;
+    const double a = p0 ? (double) -0.009350833524763f : p1 ? (double) -0.014532321752540f
+                   : p2 ? (double) -0.004605031767994f : (double) -0.000458661602210f;
+    const double b = p0 ? (double) 0.130659527668286f : p1 ? (double) 0.139942324101744f
+                   : p2 ? (double) 0.063427417320019f : (double) 0.009695946122598f;
+    const double c = p0 ? (double) 0.498799810682272f : p1 ? (double) 0.495635523139337f
+                   : p2 ? (double) 0.695956496475118f : (double) 0.930734667215156f;
+    const double e = p0 ? (double) 0.693203116424741f : p1 ? (double) 0.692140569840976f
+                   : p2 ? (double) 0.514272634594009f : (double) 0.168037164329057f;
+    return ((a * d + b) * d + c) * d + e;
 }
 
 __device__ __forceinline__ double log_add(double x, double y) {
-    if (x < y) return (x == kNegInf || y - x >= 7.5) ? y : lookup(y - x) + x;
-    return (y == kNegInf || x - y >= 7.5) ? x : lookup(x - y) + y;
+    const bool lt = x < y;
+    const double hi = lt ? y : x, lo = lt ? x : y;
+    return (lo == kNegInf || hi - lo >= 7.5) ? hi : lookup(hi - lo) + lo;
 }
 
 // emissions_signal_descaleEventMean_JordanStyle (stateMachine.c:285-289)
