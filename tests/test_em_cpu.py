@@ -206,3 +206,13 @@ def test_expectations_file_loads_as_a_model(api, gauss_case, tmp_path):
     em = np.asarray(hmm["event_model"]).reshape(-1, 5)
     np.testing.assert_allclose(back["match"], em, rtol=0, atol=5e-7)
     np.testing.assert_allclose(back["gapy"][:, 1], 1.75 * back["match"][:, 1], rtol=1e-15)
+
+
+def test_expectations_file_defaults_to_the_machines_match_table(api, gauss_case):
+    """sa_formatExpectations with no event model writes the machine's match table (what
+    continuousPairHmm_makeExpectationsHmm copies), so signalMachine's raw file needs only the machine"""
+    m, rd, ex = gauss_case
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED, rd)
+    with_model = api.formatExpectations(sm, _hmm(api, sm, ex))
+    without = api.formatExpectations(sm, dict(ex, event_model=None))
+    assert without == with_model and len(without) > 0
