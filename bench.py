@@ -71,12 +71,72 @@ def dist_env():
 
 
 def model_and_reads(n_reads, seed):
-    from oracle import formats
+    """The synthetic reads and their .model text (6-mer ACGT Gaussian table, nanopore transitions)."""
     from signalalign_b200 import synth
     cfg = synth.config1(seed=seed, n_reads=n_reads)
-    text = synth.model_text(cfg["alphabet"], cfg["k"], cfg["table"])
-    m = formats.parse_model_lines(*text.split("\n")[:3])
-    return cfg, m
+    return cfg, synth.model_text(cfg["alphabet"], cfg["k"], cfg["table"])
+
+
+def oracle_model_dict(text):
+    """The checker's own reading of the .model text (the oracle's restated loader)."""
+    from oracle import formats
+    return formats.parse_model_lines(*text.split("\n")[:3])
+
+
+def load_product_model(text, device=0):
+    """The product's loader on the .model file (stateMachine3_loadFromFile + getStateMachine3_descaled)."""
+    import tempfile
+    from signalalign_b200 import api
+    with tempfile.NamedTemporaryFile("w", suffix=".model", delete=False) as fh:
+        fh.write(text)
+        path = fh.name
+    try:
+        return api.StateMachine.load(path, api.THREE_STATE, api.EMIT_DESCALED, device=device)
+    finally:
+        os.unlink(path)
+
+
+def accuracy_vs_oracle(m, reads, got_pairs, got_ll, threshold, threads, emission=None, hdp=None):
+    """Every read's pairs and log-likelihood against the FP64 oracle, one read per host thread.
+    Returns the largest posterior error over the union of each read's pairs (a pair on one side only
+    counts as its posterior minus the threshold), the largest |log-likelihood| error (absolute and
+    relative to |log-likelihood|), and the pairs present on one side only with a posterior more than
+    the FP32 bound (1e-4) above the threshold."""
+    from oracle import oracle as orc
+    emission = orc.EMIT_DESCALED if emission is None else emission
+    p = orc.params(threshold=threshold, expansion=50)
+
+    def one(i):
+        rd = reads[i]
+        om = orc.OracleModel(m if not isinstance(m, list) else m[i], emission, rd["scale"], rd["shift"],
+                             rd.get("var", 1.0), hdp=hdp)
+        want, tps = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], p, with_total_probs=True)
+        got = got_pairs(i)
+        ma = {(int(r["x"]), int(r["y"])): r["score"] / 1e7 for r in want}
+        mg = {(int(r["x"]), int(r["y"])): r["score"] / 1e7 for r in got}
+        err, outside = 0.0, 0
+        for key in set(ma) | set(mg):
+            if key in ma and key in mg:
+                err = max(err, abs(ma[key] - mg[key]))
+            else:
+                present = ma.get(key) or mg.get(key)
+                err = max(err, present - threshold)
+                outside += present - threshold > 1e-4
+        k = 6
+        top = [v for d, v in tps if d == len(rd["reference"]) - (k - 1) + len(rd["events"])]
+        ll_abs = abs(got_ll(i) - top[0]) if top else 0.0
+        ll_rel = ll_abs / max(1.0, abs(top[0])) if top else 0.0
+        return err, ll_abs, ll_rel, outside, len(want)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        res = list(ex.map(one, range(len(reads))))
+    return {"max_posterior_err": max(r[0] for r in res), "max_loglik_abs_err": max(r[1] for r in res),
+            "max_loglik_rel_err": max(r[2] for r in res),
+            "pairs_outside_threshold_tolerance": int(sum(r[3] for r in res)),
+            "oracle_pairs": int(sum(r[4] for r in res)), "reads": len(reads),
+            "longest_read_antidiagonals": int(max(len(rd["reference"]) - 5 + len(rd["events"]) for rd in reads)),
+            "oracle_seconds": time.perf_counter() - t0, "vs": "FP64 CPU oracle, every read of the batch"}
 
 
 class ClockSampler:
@@ -164,7 +224,8 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    cfg, m = model_and_reads(args.reads, args.seed)
+    cfg, text = model_and_reads(args.reads, args.seed)
+    m = oracle_model_dict(text)
     threads = os.cpu_count() or 1
     vals = []
     for s in range(args.warmup + args.steps):
@@ -188,16 +249,13 @@ def run_serve(args):
     (all requests of a saturation set submitted at once); the timed run offers --load of it.  Latency
     is submission to completion as the server records it (planning, upload, kernels, download)."""
     import torch
-    from oracle import formats
     from signalalign_b200 import api, synth
     torch.cuda.set_device(0)
     r = np.random.Generator(np.random.PCG64(args.seed + 404))
     models = []
     for alphabet in ("ACGT", "ACEGT"):
         table = synth.gaussian_table(alphabet, 6, 1000 + len(alphabet))
-        m = formats.parse_model_lines(*synth.model_text(alphabet, 6, table).split("\n")[:3])
-        sm = api.StateMachine.from_tables(alphabet, 6, m["t"], m["match"], m["gapy"], m["gapx"],
-                                          emission=api.EMIT_DESCALED)
+        sm = load_product_model(synth.model_text(alphabet, 6, table))
         models.append((alphabet, table, sm))
     n = args.serve_requests
     spans = np.clip(np.exp(np.log(8000.0) + 0.6 * r.standard_normal(n)), 500, 100000).astype(int)
@@ -291,7 +349,8 @@ def run_config(args):
         hdp = W.hdp_dict(cfg["hdp"], 5 ** 6)
         gm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["gauss_table"]).split("\n")[:3])
         hm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["hdp_table"]).split("\n")[:3])
-        models = {"gauss": (W.gpu_model(api, gm, orc.EMIT_DESCALED), gm, orc.EMIT_DESCALED, None),
+        models = {"gauss": (load_product_model(synth.model_text("ACEGT", 6, cfg["gauss_table"])), gm,
+                            orc.EMIT_DESCALED, None),
                   "hdp": (W.gpu_model(api, hm, orc.EMIT_HDP, None, hdp), hm, orc.EMIT_HDP, hdp)}
         als = cfg["alignments"]
         workload = ("512 reads x U(1kb,30kb) x {template, complement} x {all-C, all-E} at CCWGG sites = 2048 "
@@ -325,22 +384,34 @@ def run_config(args):
         torch.cuda.synchronize()
         e2e_ms += (time.perf_counter() - t0) * 1e3
         del bb
-    # accuracy on the 4 shortest alignments
-    order = np.argsort([len(a["events"]) for a in als])[:4]
-    bb = api.align_batch([inputs[i] for i in order], p, sptr)
-    errs = []
-    for k, i in enumerate(order):
-        a = als[i]
-        _, mm, emis, hh = models[a["model"]]
-        om = W.oracle_model(mm, emis, a, hh)
-        want = orc.aligned_pairs(om, a["reference"], a["events"], a["anchors"], orc.params(threshold=0.01, expansion=50))
-        errs.append(W.max_posterior_error(want, bb.pairs(k), 0.01))
+    # accuracy against the FP64 oracle: every alignment of config 2; for config 3 the longest
+    # alignment of each model and a spread of the others (about 20 s of host work)
+    n_al = len(als)
+    if args.config == 2:
+        chosen = list(range(n_al))
+    else:
+        order = [int(i) for i in np.argsort([len(a["events"]) for a in als])]
+        chosen = sorted(set(order[::max(1, n_al // 48)]) |
+                        {max((i for i in range(n_al) if als[i]["model"] == mk), key=lambda i: len(als[i]["events"]))
+                         for mk in models})
+    bb = api.align_batch([inputs[i] for i in chosen], p, sptr)
+    sub_reads = [als[i] for i in chosen]
+    ms = [models[a["model"]][1] for a in sub_reads]
+    acc = {}
+    for mk, (_, mm, emis, hh) in models.items():
+        idx = [j for j, a in enumerate(sub_reads) if a["model"] == mk]
+        if not idx:
+            continue
+        a_k = accuracy_vs_oracle(mm, [sub_reads[j] for j in idx], lambda q: bb.pairs(idx[q]),
+                                 lambda q: bb.log_likelihood(idx[q]), 0.01, os.cpu_count() or 1, emission=emis, hdp=hh)
+        acc[mk] = a_k
+    del ms
     line = {"metric": METRIC, "value": cells / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload, "alignments": len(als), "cells": cells, "sub_batches": len(groups)},
             "e2e": {"value": cells / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms},
-            "accuracy": {"max_posterior_err": max(errs), "alignments": len(errs), "vs": "FP64 CPU oracle"},
+            "accuracy": acc,
             "gpu_launches": api.kernel_launch_count() - launches0}
     print(json.dumps(line), flush=True)
 
@@ -354,8 +425,9 @@ def run_expectations(args):
     from oracle import oracle as orc
     from signalalign_b200 import api
     torch.cuda.set_device(0)
-    cfg, m = model_and_reads(args.reads, args.seed)
-    sm = api.StateMachine.from_tables("ACGT", 6, m["t"], m["match"], m["gapy"], m["gapx"], emission=api.EMIT_DESCALED)
+    cfg, text = model_and_reads(args.reads, args.seed)
+    m = oracle_model_dict(text)
+    sm = load_product_model(text)
     p = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=50, threshold=0.01)
     reads = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
                            scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
@@ -431,9 +503,9 @@ def main():
                                 device_id=torch.device("cuda", local))
     from signalalign_b200 import api
 
-    cfg, m = model_and_reads(args.reads, args.seed + 1000 * rank)
-    sm = api.StateMachine.from_tables("ACGT", 6, m["t"], m["match"], m["gapy"], m["gapx"], emission=api.EMIT_DESCALED,
-                                      device=local)
+    cfg, text = model_and_reads(args.reads, args.seed + 1000 * rank)
+    m = oracle_model_dict(text)
+    sm = load_product_model(text, device=local)
     p = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=50, threshold=0.01)
     reads = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
                            scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
@@ -582,8 +654,7 @@ def main():
             rd = cfg["reads"][i]
             L, R = api.band_construct(rd["anchors"], len(rd["reference"]) - 5, len(rd["events"]), 50)
             sample_cells += int(np.sum((R - L) // 2 + 1))
-        sm64 = api.StateMachine.from_tables("ACGT", 6, m["t"], m["match"], m["gapy"], m["gapx"],
-                                            emission=api.EMIT_DESCALED, device=local)
+        sm64 = load_product_model(text, device=local)
         api.getAlignedPairsUsingAnchors(sm64, cfg["reads"][sample[0]]["reference"][:300],
                                         cfg["reads"][sample[0]]["events"][:400], [], p)
         torch.cuda.synchronize()
@@ -638,28 +709,9 @@ def main():
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": "%d reads (%d cells, smallest bands first), one read per thread, %.1f s"
                                           % (nr, ccells, dt)}
-        # accuracy of the batched FP32 form against the FP64 oracle on 4 reads
-        from oracle import oracle as orc
+        # accuracy of the batched FP32 form against the FP64 oracle on every read of the batch
         bb = api.align_batch(reads, p, sptr)
-        errs, llerr = [], []
-        for i in [int(j) for j in np.argsort([len(rd["events"]) for rd in cfg["reads"]])[:4]]:
-            rd = cfg["reads"][i]
-            om = orc.OracleModel(m, orc.EMIT_DESCALED, rd["scale"], rd["shift"], 1.0)
-            want, tps = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"],
-                                          orc.params(threshold=0.01, expansion=50), with_total_probs=True)
-            got = bb.pairs(i)
-            ma = {(int(r["x"]), int(r["y"])): r["score"] / 1e7 for r in want}
-            mg = {(int(r["x"]), int(r["y"])): r["score"] / 1e7 for r in got}
-            e = 0.0
-            for k in set(ma) | set(mg):
-                e = max(e, abs(ma.get(k, 0.0) - mg.get(k, 0.0)) if (k in ma and k in mg)
-                        else (ma.get(k) or mg.get(k)) - 0.01)
-            errs.append(e)
-            top = [v2 for d, v2 in tps if d == len(rd["reference"]) - 5 + len(rd["events"])]
-            if top:
-                llerr.append(abs(bb.log_likelihood(i) - top[0]))
-        line["accuracy"] = {"max_posterior_err": max(errs), "max_loglik_abs_err": max(llerr) if llerr else None,
-                            "reads": 4, "vs": "FP64 CPU oracle"}
+        line["accuracy"] = accuracy_vs_oracle(m, cfg["reads"], bb.pairs, bb.log_likelihood, 0.01, threads)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -224,6 +224,12 @@ int64_t sa_batch_regions(const sa_batch *b);
  * forward / traceback-window worker, the pair gather.  Waits for them.  SA_E_ARG if the batch has
  * not run (no counterpart in signalAlign: a diagnostic of this engine) */
 sa_status sa_batch_kernel_ms(const sa_batch *b, double *emission_ms, double *worker_ms, double *gather_ms);
+/* Bound, in SM clock cycles, of every device-side wait of the batch's worker kernel (a warp waiting
+ * for a traceback window to be published).  Default 2e10 (about 10 s), far beyond any forward sweep.
+ * A wait that runs out sets the batch's error flag: every other waiter leaves, the kernel ends
+ * normally, and every read of the batch reports SA_E_TIMEOUT.  No counterpart in signalAlign (its
+ * CPU code never waits); a diagnostic of this engine's bounded waits. */
+sa_status sa_batch_set_wait_limit(sa_batch *b, int64_t cycles);
 void sa_batch_destroy(sa_batch *b);
 
 /* ---- batched FP32 form without device allocation (no counterpart in signalAlign) ---- */
@@ -254,7 +260,9 @@ void sa_batch_destroy(sa_batch *b);
  *     other byte the kernel reads is written earlier in the same call.
  *   - The first call on a device looks the array's address up (cudaGetSymbolAddress, which can load
  *     the library's device code on that device): make one call on each device during set-up, before
- *     any stream capture begins.
+ *     any stream capture begins.  With lazy module loading that first call is also when the device
+ *     reserves the array's SA_NOALLOC_SCRATCH_BYTES, so make it before the host framework reserves
+ *     its own memory pool; if the device has no room left by then the call returns SA_E_CUDA.
  *   - All calls on a device share the array, so two calls whose device work overlapped would
  *     overwrite each other's data.  The call is synchronous (it returns after `stream` drained) and
  *     holds a per-device lock for its whole duration, so calls from several host threads run one
@@ -483,6 +491,10 @@ void sa_free_text(char *text);
 const char *sa_status_string(sa_status s);
 /* number of kernel launches this process has made through the library (all entry points) */
 int64_t sa_kernel_launch_count(void);
+/* number of device and pinned-host allocations (cudaMalloc, cudaHostAlloc) the library has made in
+ * this process (no counterpart in signalAlign: a diagnostic; memory pools reuse blocks, so a warm
+ * steady state adds none) */
+int64_t sa_allocation_count(void);
 /* FP32 FMA issue rate of `device` in TFLOP/s, measured by a short probe kernel (the denominator of
  * the engine's compute roofline; no counterpart in signalAlign) */
 sa_status sa_measure_fp32_peak(int32_t device, double *tflops);

@@ -135,6 +135,7 @@ def _bind(L):
         "sa_batch_regions": (C.c_int64, [vp]),
         "sa_batch_kernel_ms": (C.c_int, [vp, _f64p, _f64p, _f64p]),
         "sa_batch_transfer_bytes": (C.c_int, [vp, _i64p, _i64p]),
+        "sa_batch_set_wait_limit": (C.c_int, [vp, C.c_int64]),
         "sa_batch_destroy": (None, [vp]),
         "sa_align_batch_noalloc": (C.c_int, [C.POINTER(Read), C.c_int64, C.POINTER(Params), vp,
                                              C.POINTER(AlignedPair), C.c_int64, _i64p, C.POINTER(C.c_int32), _f64p,
@@ -173,6 +174,7 @@ def _bind(L):
         "sa_writeExpectations": (C.c_int, [C.c_char_p, vp, C.POINTER(Expectations), _f64p, _f64p, C.c_int64]),
         "sa_status_string": (C.c_char_p, [C.c_int]),
         "sa_kernel_launch_count": (C.c_int64, []),
+        "sa_allocation_count": (C.c_int64, []),
         "sa_measure_fp32_peak": (C.c_int, [C.c_int32, _f64p]),
     }
     for name, (res, args) in sig.items():
@@ -438,6 +440,10 @@ class Batch:
     def download(self, stream=None):
         _check(lib().sa_batch_download(self._h, stream), "batch_download")
 
+    def set_wait_limit(self, cycles):
+        """bound (SM clock cycles) of the worker kernel's device-side waits (sa_batch_set_wait_limit)"""
+        _check(lib().sa_batch_set_wait_limit(self._h, int(cycles)), "batch_set_wait_limit")
+
     @property
     def cells(self):
         return lib().sa_batch_cells(self._h)
@@ -571,6 +577,11 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def allocation_count():
+    """device and pinned-host allocations the library has made in this process (sa_allocation_count)"""
+    return lib().sa_allocation_count()
 
 
 def kernel_launch_count():

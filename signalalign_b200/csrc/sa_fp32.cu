@@ -137,6 +137,7 @@ struct sa_batch {
     unsigned char *dev_base = nullptr;
     std::vector<double> read_ll;
     bool downloaded = false;
+    long long wait_limit = 20000000000LL;   // clock cycles a worker may wait for a window (~10 s)
     // device timing of the last run's kernels (batches that own their device memory only)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timed = false;
@@ -591,7 +592,7 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         const int cpt = std::max(1, (b->max_width + kThreads - 1) / kThreads);
         const int cpt_pow2 = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
         a.wmax = cpt_pow2 * kThreads;
-        a.spin_limit = 20000000000LL;   // ~10 s at 2 GHz: far beyond any forward sweep
+        a.spin_limit = b->wait_limit;
         const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) worker_area_floats(cpt_pow2);
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
@@ -744,7 +745,7 @@ sa_status sa_measure_fp32_peak(int32_t device, double *tflops) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     float *sink = nullptr;
-    if (cudaMalloc(&sink, sizeof(float)) != cudaSuccess) { cudaSetDevice(prev); return SA_E_NOMEM; }
+    if (device_malloc(reinterpret_cast<void **>(&sink), sizeof(float)) != cudaSuccess) { cudaSetDevice(prev); return SA_E_NOMEM; }
     const int blocks = sms * 8, threads = 256, iters = 1 << 16;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -770,6 +771,12 @@ sa_status sa_measure_fp32_peak(int32_t device, double *tflops) {
 }
 
 int64_t sa_batch_regions(const sa_batch *b) { return b ? (int64_t) b->regions.size() : 0; }
+
+sa_status sa_batch_set_wait_limit(sa_batch *b, int64_t cycles) {
+    if (!b || cycles < 1) return SA_E_ARG;
+    b->wait_limit = (long long) cycles;
+    return SA_OK;
+}
 
 void sa_batch_destroy(sa_batch *b) { delete b; }
 
@@ -799,8 +806,12 @@ sa_status batch_plan_host(const sa_read *reads, int64_t n_reads, const sa_params
 int batch_device(const sa_batch *b) { return b->device; }
 
 bool batch_models_resident(const sa_batch *b) {
-    for (const sa_state_machine *sm : b->models)
-        if (sm->dev_dirty) return false;
+    // only the machines of reads the FP32 kernels run: reads routed to the plain form report
+    // SA_E_UNSUPPORTED on this path and never touch their machine's device tables
+    std::vector<char> used(b->models.size(), 0);
+    for (int64_t r = 0; r < b->n_regions; ++r) used[(size_t) b->regions[r].model] = 1;
+    for (size_t i = 0; i < b->models.size(); ++i)
+        if (used[i] && !model_resident(b->models[i])) return false;
     return true;
 }
 

@@ -523,7 +523,7 @@ __global__ void kmer_logs_kernel(const double *match, const double *gapy, int64_
 sa_status compute_kmer_logs(sa_state_machine *sm) {
     const int64_t n = sm->n_kmers;
     DeviceModel &d = sm->dev;
-    if (cudaMalloc(reinterpret_cast<void **>(&d.klog), sizeof(double) * 4 * (size_t) std::max<int64_t>(n, 1)) !=
+    if (device_malloc(reinterpret_cast<void **>(&d.klog), sizeof(double) * 4 * (size_t) std::max<int64_t>(n, 1)) !=
         cudaSuccess) {
         d.klog = nullptr;
         return SA_E_NOMEM;

@@ -23,6 +23,20 @@ namespace sa {
 static std::atomic<int64_t> g_launches{0};
 void count_launch(int64_t n) { g_launches += n; }
 
+static std::atomic<int64_t> g_allocations{0};
+
+cudaError_t device_malloc(void **ptr, size_t bytes) {
+    const cudaError_t rc = cudaMalloc(ptr, bytes);
+    if (rc == cudaSuccess) ++g_allocations;
+    return rc;
+}
+
+cudaError_t pinned_malloc(void **ptr, size_t bytes) {
+    const cudaError_t rc = cudaHostAlloc(ptr, bytes, cudaHostAllocDefault);
+    if (rc == cudaSuccess) ++g_allocations;
+    return rc;
+}
+
 // ------------------------------------------------------------------------------------------------
 // band geometry
 // ------------------------------------------------------------------------------------------------
@@ -548,7 +562,7 @@ void free_device_model(sa_state_machine *sm) {
 template <typename T>
 static sa_status upload(T **dst, const T *src, size_t n) {
     if (n == 0) return SA_OK;
-    if (cudaMalloc((void **) dst, n * sizeof(T)) != cudaSuccess) return SA_E_NOMEM;
+    if (device_malloc((void **) dst, n * sizeof(T)) != cudaSuccess) return SA_E_NOMEM;
     if (cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return SA_E_CUDA;
     return SA_OK;
 }
@@ -563,6 +577,11 @@ bool gapy_follows_match(const sa_state_machine *sm) {
 }
 
 static std::mutex g_model_mutex;
+
+bool model_resident(const sa_state_machine *sm) {
+    std::lock_guard<std::mutex> lock(g_model_mutex);
+    return !sm->dev_dirty;
+}
 
 sa_status ensure_device_model(sa_state_machine *sm) {
     std::lock_guard<std::mutex> lock(g_model_mutex);
@@ -813,5 +832,7 @@ const char *sa_status_string(sa_status s) {
 }
 
 int64_t sa_kernel_launch_count(void) { return g_launches.load(); }
+
+int64_t sa_allocation_count(void) { return g_allocations.load(); }
 
 }  // extern "C"

@@ -134,6 +134,15 @@ void free_device_model(sa_state_machine *sm);
 
 void count_launch(int64_t n = 1);
 
+// every cudaMalloc / cudaHostAlloc of the library goes through these two, which count the
+// successful ones (sa_allocation_count)
+cudaError_t device_malloc(void **ptr, size_t bytes);
+cudaError_t pinned_malloc(void **ptr, size_t bytes);
+
+// the machine's device tables are current (no change since its last upload), read under the lock
+// that guards the upload
+bool model_resident(const sa_state_machine *sm);
+
 // memory blocks reused across batches (sa_memory.cpp): device and pinned host blocks go back to a
 // free list; heap blocks (for callers that must not touch the CUDA allocators) are freed
 enum class MemKind { Device, Pinned, Heap };

@@ -46,12 +46,12 @@ bool allocate(MemKind kind, int device, size_t bytes, void **ptr) {
     if (kind == MemKind::Device) {
         int prev = 0;
         cudaGetDevice(&prev);
-        bool ok = cudaSetDevice(device) == cudaSuccess && cudaMalloc(ptr, bytes) == cudaSuccess;
+        bool ok = cudaSetDevice(device) == cudaSuccess && device_malloc(ptr, bytes) == cudaSuccess;
         cudaSetDevice(prev);
         if (!ok) cudaGetLastError();
         return ok;
     }
-    const bool ok = cudaHostAlloc(ptr, bytes, cudaHostAllocDefault) == cudaSuccess;
+    const bool ok = pinned_malloc(ptr, bytes) == cudaSuccess;
     if (!ok) cudaGetLastError();
     return ok;
 }

@@ -70,6 +70,9 @@ extern "C" sa_status sa_align_batch_noalloc(const sa_read *reads, int64_t n_read
             st = sa_batch_upload(b, stream);
             if (!st) st = sa_batch_run(b, stream);
             if (!st) st = sa_batch_download(b, stream);
+            // a failed step may leave copies or kernels queued that still write the array: let the
+            // stream drain before the lock lets the next caller in
+            if (st) cudaStreamSynchronize((cudaStream_t) stream);
         }
         cudaSetDevice(prev);
     }

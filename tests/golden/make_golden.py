@@ -1,6 +1,7 @@
 """Regenerate the golden fixtures in this directory from the signalAlign source tree.
 
 Usage:  python tests/golden/make_golden.py /path/to/signalAlign
+        (or with the tree's path in the SIGNALALIGN_SRC environment variable)
 
 The fixtures hold only the inputs of the reference's own known-answer tests, cut down to what
 those tests touch, so the test suite runs without the source tree:
@@ -102,4 +103,7 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SIGNALALIGN_SRC")
+    if not src:
+        sys.exit("usage: make_golden.py /path/to/signalAlign (or set SIGNALALIGN_SRC)")
+    main(src)

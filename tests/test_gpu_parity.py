@@ -381,3 +381,30 @@ def test_batch_only_degenerate_reads_and_empty_batch(api):
         assert len(alone) > 50 and np.array_equal(alone, b.pairs(i))
     empty = api.align_batch([], p)
     assert empty.cells == 0
+
+
+def test_fp32_bounded_wait_runs_out(api):
+    """Every device-side wait of the worker kernel is bounded (sa_batch_set_wait_limit).  With a
+    bound of one clock cycle the warps waiting for traceback windows give up at once: the launch
+    still ends normally, every read reports SA_E_TIMEOUT, and the context stays usable (the same
+    batch run again with the default bound gives the oracle's pairs)."""
+    cfg = synth.config1(seed=31, n_reads=2, span=(3000, 4000))
+    m = W.gaussian_model(cfg)
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED)
+    inputs = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                            scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
+    p = _p(api)
+    b = api.Batch(inputs, p)
+    b.upload()
+    b.set_wait_limit(1)
+    b.run()
+    b.download()
+    assert [b.status(i) for i in range(2)] == [9, 9]        # SA_E_TIMEOUT
+    b.set_wait_limit(20_000_000_000)
+    b.run()
+    b.download()
+    for i, rd in enumerate(cfg["reads"]):
+        assert b.status(i) == 0
+        om = W.oracle_model(m, orc.EMIT_DESCALED, rd)
+        want = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], _op(p), True, True)
+        assert W.max_posterior_error(want, b.pairs(i), p.threshold) <= FP32_TOL

@@ -11,7 +11,8 @@ from oracle import formats
 from oracle import oracle as orc
 from golden_models import load_fixture, model_from_fixture
 
-REF = "/root/reference"
+# the signalAlign source tree, for the tests that read its files directly (skipped without it)
+REF = os.environ.get("SIGNALALIGN_SRC", "")
 
 
 def test_bands_golden():
@@ -136,8 +137,8 @@ def test_banded_matches_unbanded_on_toy():
     assert {(int(p["x"]), int(p["y"])) for p in banded} == {(int(p["x"]), int(p["y"])) for p in full}
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "models", "templateSingleLevelFixed.nhdp")),
-                    reason="signalAlign source tree not mounted")
+@pytest.mark.skipif(not REF or not os.path.exists(os.path.join(REF, "models", "templateSingleLevelFixed.nhdp")),
+                    reason="SIGNALALIGN_SRC does not name a signalAlign source tree")
 def test_parse_reference_nhdp():
     """deserialize_nhdp on the reference's HDP fixture: ACEGOT 6-mers over 46657 DPs, one observed
     ancestor chain per observed leaf; every k-mer resolves to an observed row or none."""

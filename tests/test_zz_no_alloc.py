@@ -88,8 +88,10 @@ def test_noalloc_matches_align_batch_twice():
     inputs = _inputs(sm, reads)
     p = _params()
     ref = api.align_batch(inputs, p)         # allocating entry point; also makes the tables resident
+    allocations = api.allocation_count()
     for call in range(2):
         got = api.align_batch_noalloc(inputs, p)
+        assert api.allocation_count() == allocations    # no cudaMalloc / cudaHostAlloc on this path
         assert 0 < got.scratch_bytes <= api.NOALLOC_SCRATCH_BYTES
         for i in range(len(reads)):
             assert got.status(i) == 0 and ref.status(i) == 0
