@@ -114,6 +114,13 @@ int64_t sa_stateMachine_kmerId(const sa_state_machine *sm, const char *kmer);
 sa_status sa_stateMachine_getTables(const sa_state_machine *sm, double *match, double *gap_y, double *gap_x,
                                     double *transitions);
 
+/* the machine's HDP tables back on the host (for checking a .nhdp load, as deserialize_nhdp would
+ * hold them, nanopore_hdp.c:1071-1098): the grid, n_rows rows of posterior-predictive density and
+ * knot slopes, and per k-mer its row (-1: no observed ancestor).  Arrays may be NULL: a first call
+ * with NULL arrays returns the sizes.  SA_E_UNSUPPORTED for a machine without HDP tables. */
+sa_status sa_stateMachine_getHdpTables(const sa_state_machine *sm, int64_t *grid_length, int64_t *n_rows,
+                                       double *grid, double *density, double *slope, int64_t *kmer_row);
+
 void sa_stateMachine_destruct(sa_state_machine *sm);
 
 /* ---- alignment parameters (PairwiseAlignmentParameters, inc/pairwiseAligner.h:123-134) ---- */

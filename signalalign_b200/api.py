@@ -113,6 +113,7 @@ def _bind(L):
         "sa_stateMachine_kmerString": (C.c_char_p, [vp, C.c_int64]),
         "sa_stateMachine_kmerId": (C.c_int64, [vp, C.c_char_p]),
         "sa_stateMachine_getTables": (C.c_int, [vp, _f64p, _f64p, _f64p, _f64p]),
+        "sa_stateMachine_getHdpTables": (C.c_int, [vp, _i64p, _i64p, _f64p, _f64p, _f64p, _i64p]),
         "sa_stateMachine_destruct": (None, [vp]),
         "sa_params_default": (None, [C.POINTER(Params)]),
         "sa_band_construct": (C.c_int, [_i64p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _i64p, _i64p]),
@@ -301,6 +302,18 @@ class StateMachine:
         _check(lib().sa_stateMachine_getTables(self._h, m.ctypes.data_as(_f64p), y.ctypes.data_as(_f64p),
                                                x.ctypes.data_as(_f64p), t.ctypes.data_as(_f64p)), "getTables")
         return dict(match=m, gapy=y, gapx=x, t=t)
+
+    def hdp_tables(self):
+        """the HDP grid, densities, slopes and k-mer rows as loaded (sa_stateMachine_getHdpTables)"""
+        gl, nr = C.c_int64(0), C.c_int64(0)
+        _check(lib().sa_stateMachine_getHdpTables(self._h, C.byref(gl), C.byref(nr), None, None, None, None),
+               "getHdpTables")
+        g, d, s = np.zeros(gl.value), np.zeros((nr.value, gl.value)), np.zeros((nr.value, gl.value))
+        r = np.zeros(self.n_kmers, np.int64)
+        _check(lib().sa_stateMachine_getHdpTables(self._h, C.byref(gl), C.byref(nr), g.ctypes.data_as(_f64p),
+                                                  d.ctypes.data_as(_f64p), s.ctypes.data_as(_f64p),
+                                                  r.ctypes.data_as(_i64p)), "getHdpTables")
+        return dict(grid=g, density=d, slope=s, kmer_row=r)
 
 
 def getStateMachine3(model_file, device=0):

@@ -774,6 +774,20 @@ sa_status sa_stateMachine_getTables(const sa_state_machine *sm, double *match, d
     return SA_OK;
 }
 
+sa_status sa_stateMachine_getHdpTables(const sa_state_machine *sm, int64_t *grid_length, int64_t *n_rows,
+                                       double *grid, double *density, double *slope, int64_t *kmer_row) {
+    if (!sm || !grid_length || !n_rows) return SA_E_ARG;
+    const HdpTables &h = sm->hdp;
+    if (!h.present) return SA_E_UNSUPPORTED;
+    *grid_length = h.grid_length;
+    *n_rows = h.n_rows;
+    if (grid) std::copy(h.grid.begin(), h.grid.end(), grid);
+    if (density) std::copy(h.density.begin(), h.density.end(), density);
+    if (slope) std::copy(h.slope.begin(), h.slope.end(), slope);
+    if (kmer_row) std::copy(h.kmer_row.begin(), h.kmer_row.end(), kmer_row);
+    return SA_OK;
+}
+
 void sa_stateMachine_destruct(sa_state_machine *sm) {
     if (!sm) return;
     free_device_model(sm);

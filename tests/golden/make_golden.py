@@ -15,9 +15,26 @@ those tests touch, so the test suite runs without the source tree:
   (:823-851): tests/test_npReads/ZymoRef.txt, the template events and template scaling of
   tests/test_npReads/ZymoC_ch_1_file1.npRead, and the R7.3 ACEGOT template model entries for the
   k-mers of ZymoRef.  Expected: 1076 pairs.
+* zymo_banded.json -- the anchors of the banded Zymo tests (getRemappedAnchors,
+  tests/stateMachineTests.c:132-138): lastz (the reference's vendored copy, built by
+  oracle/build_lastz.sh) on ZymoRef against the read's 2D sequence, through
+  oracle/anchors.py's restatement of getBlastPairsForPairwiseAlignmentParameters, remapped by the
+  template 2D event map and filtered; with the 2D sequence and the event map themselves, so the
+  anchors can be regenerated from the fixture alone.  Expected counts (default parameters:
+  diagonal expansion 20): 1076 pairs with the scaled and the descaled R7.3 machines
+  (test_stateMachine3_getAlignedPairsWithBanding, :823-851, ragged ends); 1076 with every C of
+  the reference replaced by C, E or O and 7349 with it replaced by X (CEO paths)
+  (test_DegenerateNucleotides, :897-960, non-ragged ends); 1217 with the HDP machine at threshold
+  0.1 on the read's events as nanopore_descaleNanoporeRead leaves them
+  (test_sm3Hdp_getAlignedPairsWithBanding, :881-895).
+* testModelR73_acegot_template.model.xz, testModelR9_5mer_acgt_template.model.xz,
+  templateSingleLevelFixed.nhdp.xz -- the reference's model files (models/), compressed, byte for
+  byte: the product's loaders are tested on them and the banded tests load their machines from
+  them.
 """
 import itertools
 import json
+import lzma
 import os
 import sys
 
@@ -96,6 +113,25 @@ def main(src):
               template_params=dict(scale=float(head[5]), shift=float(head[6]), var=float(head[7]),
                                    scale_sd=float(head[8]), var_sd=float(head[9])),
               threshold=0.01, expected_pairs=1076, source="tests/stateMachineTests.c:823-851")
+    # banded Zymo anchors (lastz must have been built: oracle/build_lastz.sh)
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle import anchors as A
+    npr = A.parse_np_read(os.path.join(src, "tests", "test_npReads", "ZymoC_ch_1_file1.npRead"))
+    anchors = A.remapped_anchors(zref, npr["two_d_read"], npr["template_event_map"])
+    banded = dict(anchors=[list(a) for a in anchors], two_d_read=npr["two_d_read"],
+                  template_event_map=npr["template_event_map"], diagonal_expansion=20,
+                  expected=dict(scaled=1076, descaled=1076, C=1076, E=1076, O=1076, X=7349, hdp_threshold_0_1=1217),
+                  source="tests/stateMachineTests.c:132-138, :694-717, :823-895, :897-960")
+    with open(os.path.join(HERE, "zymo_banded.json"), "w") as fh:
+        json.dump(banded, fh, separators=(",", ":"))
+    print("wrote zymo_banded", len(anchors), "anchors")
+    for fn in ("testModelR73_acegot_template.model", "testModelR9_5mer_acgt_template.model",
+               "templateSingleLevelFixed.nhdp"):
+        with open(os.path.join(models, fn), "rb") as fh:
+            data = fh.read()
+        with open(os.path.join(HERE, fn + ".xz"), "wb") as fh:
+            fh.write(lzma.compress(data, preset=9))
+        print("wrote", fn + ".xz")
     for name, obj in (("toy6", toy6), ("toy5", toy5), ("zymo", zy)):
         with open(os.path.join(HERE, name + ".json"), "w") as fh:
             json.dump(obj, fh, separators=(",", ":"))

@@ -211,3 +211,45 @@ def test_batch_planning_with_degenerate_reads(api):
         api.align_batch_noalloc(reads, p)
     except api.SAError as e:
         assert e.status in (1, 4, 5), e
+
+
+@pytest.mark.parametrize("name, alphabet, k", [("testModelR73_acegot_template.model", "ACEGOT", 6),
+                                               ("testModelR9_5mer_acgt_template.model", "ACGT", 5)])
+def test_reference_model_files_through_product_loader(api, name, alphabet, k):
+    """stateMachine3_loadFromFile (stateMachine.c:1328-1426) on the reference's own model files
+    (models/, kept byte for byte in tests/golden): the product's loader and the oracle's restated
+    reader give identical tables, including the SWITCH_TO_X quirk (gap-Y -> gap-X stored in
+    SWITCH_TO_Y, SWITCH_TO_X left at LOG_ZERO)."""
+    from golden_models import golden_file
+    path = golden_file(name)
+    sm = api.StateMachine.load(path, api.THREE_STATE, api.EMIT_DESCALED)
+    got = sm.tables()
+    want = formats.load_model_file(path)
+    assert want["alphabet"] == alphabet and sm.kmer_length == k and sm.n_kmers == len(alphabet) ** k
+    for key in ("match", "gapy", "gapx"):
+        assert np.array_equal(got[key], want[key]), key
+    assert np.array_equal(got["t"], np.array(want["t"]))
+    assert got["t"][7] == -math.inf                     # SWITCH_TO_X
+    assert np.all(np.isfinite(got["match"]))
+
+
+def test_reference_nhdp_through_product_loader(api):
+    """deserialize_nhdp (nanopore_hdp.c:1071-1098) on the reference's templateSingleLevelFixed.nhdp
+    through the product's HDP loader: grid, per-row posterior-predictive densities and knot slopes,
+    and each k-mer's observed-ancestor row equal the oracle reader's; the R7.3 ACEGOT model's match
+    table is untouched when the HDP expected values are not applied, and with them every observed
+    k-mer's level mean and sd are the HDP's (stateMachine3_setModelToHdpExpectedValues)."""
+    from golden_models import golden_file
+    model, nhdp = golden_file("testModelR73_acegot_template.model"), golden_file("templateSingleLevelFixed.nhdp")
+    want = formats.parse_nhdp(nhdp)
+    sm = api.StateMachine.load(model, api.THREE_STATE_HDP, api.EMIT_HDP, nhdp_file=nhdp, set_hdp_expected_values=False)
+    got = sm.hdp_tables()
+    assert np.array_equal(got["grid"], want["grid"])
+    assert np.array_equal(got["density"], want["density"])
+    assert np.array_equal(got["slope"], want["slope"])
+    assert np.array_equal(got["kmer_row"], want["kmer_row"])
+    m = formats.load_model_file(model)
+    assert np.array_equal(sm.tables()["match"], m["match"])
+    sm2 = api.StateMachine.load(model, api.THREE_STATE_HDP, api.EMIT_HDP, nhdp_file=nhdp, set_hdp_expected_values=True)
+    ev = formats.hdp_expected_values(m, want)
+    assert np.allclose(sm2.tables()["match"], ev["match"], rtol=1e-12, atol=1e-12)

@@ -9,10 +9,8 @@ import pytest
 
 from oracle import formats
 from oracle import oracle as orc
-from golden_models import load_fixture, model_from_fixture
-
-# the signalAlign source tree, for the tests that read its files directly (skipped without it)
-REF = os.environ.get("SIGNALALIGN_SRC", "")
+from oracle import anchors as A
+from golden_models import golden_file, load_fixture, model_from_fixture, zymo_banded
 
 
 def test_bands_golden():
@@ -137,15 +135,68 @@ def test_banded_matches_unbanded_on_toy():
     assert {(int(p["x"]), int(p["y"])) for p in banded} == {(int(p["x"]), int(p["y"])) for p in full}
 
 
-@pytest.mark.skipif(not REF or not os.path.exists(os.path.join(REF, "models", "templateSingleLevelFixed.nhdp")),
-                    reason="SIGNALALIGN_SRC does not name a signalAlign source tree")
 def test_parse_reference_nhdp():
     """deserialize_nhdp on the reference's HDP fixture: ACEGOT 6-mers over 46657 DPs, one observed
     ancestor chain per observed leaf; every k-mer resolves to an observed row or none."""
-    h = formats.parse_nhdp(os.path.join(REF, "models", "templateSingleLevelFixed.nhdp"))
+    h = formats.parse_nhdp(golden_file("templateSingleLevelFixed.nhdp"))
     assert h["alphabet"] == "ACEGOT" and h["kmer_length"] == 6
     assert len(h["parent"]) == 46657
     assert h["density"].shape[1] == h["grid_length"] and h["slope"].shape == h["density"].shape
     rows = h["kmer_row"]
     assert rows.shape == (46656,)
     assert np.all(rows < len(h["rows"]))
+
+
+# ------------------------------------------------------------------------------------------------
+# banded, anchored, multi-window known answers (lastz anchors)
+# ------------------------------------------------------------------------------------------------
+def _zymo_models(z):
+    tp = z["template_params"]
+    m = formats.load_model_file(golden_file("testModelR73_acegot_template.model"))
+    scaled = formats.scale_model(m, tp["scale"], tp["shift"], tp["var"], tp["scale_sd"], tp["var_sd"])
+    descaled = formats.scale_noise(m, tp["scale_sd"], tp["var_sd"])
+    return m, scaled, descaled
+
+
+def test_zymo_banded_known_answers():
+    """The banded Zymo tests with the reference's own lastz anchors, default parameters (diagonal
+    expansion 20; 892 k-mers x 799 events: two traceback windows and refreshes every 10th
+    posterior anti-diagonal):
+      test_stateMachine3_getAlignedPairsWithBanding (stateMachineTests.c:823-851, via
+        test_stateMachine :694-717, ragged ends): 1076 pairs with the scaled machine
+        (getStateMachine3 + emissions_signal_scaleModel) and with the descaled machine
+        (getStateMachine3_descaled with scaleNoise);
+      test_DegenerateNucleotides (:897-960, non-ragged ends, descaled machine): 1076 pairs with
+        every C replaced by C, E or O, and 7349 with every C replaced by X (CEO paths);
+      test_sm3Hdp_getAlignedPairsWithBanding (:881-895): 1217 pairs at threshold 0.1 with the HDP
+        machine (getHdpStateMachine on templateSingleLevelFixed.nhdp, the model's level means, the
+        read's scaling) on the events as nanopore_descaleNanoporeRead leaves them."""
+    z = zymo_banded()
+    tp, ex = z["template_params"], z["expected"]
+    m, scaled, descaled = _zymo_models(z)
+    ref, ev, anc = z["reference"], z["events"], z["anchors"]
+    p = orc.params(threshold=0.01, expansion=z["expansion"])
+    got = orc.aligned_pairs(orc.OracleModel(scaled, orc.EMIT_PLAIN), ref, ev, anc, p, True, True)
+    assert len(got) == ex["scaled"]
+    assert len({(int(r["x"]), int(r["y"])) for r in got}) == len(got)
+    om = orc.OracleModel(descaled, orc.EMIT_DESCALED, tp["scale"], tp["shift"], tp["var"])
+    assert len(orc.aligned_pairs(om, ref, ev, anc, p, True, True)) == ex["descaled"]
+    for base in "CEO":
+        assert len(orc.aligned_pairs(om, ref.replace("C", base), ev, anc, p, False, False)) == ex[base]
+    deg = orc.aligned_pairs(om, ref.replace("C", "X"), ev, anc, p, False, False, options="CEO")
+    assert len(deg) == ex["X"]
+    h = formats.parse_nhdp(golden_file("templateSingleLevelFixed.nhdp"))
+    omh = orc.OracleModel(m, orc.EMIT_HDP, tp["scale"], tp["shift"], tp["var"], hdp=h)
+    ph = orc.params(threshold=0.1, expansion=z["expansion"])
+    assert len(orc.aligned_pairs(omh, ref, z["hdp_events"], anc, ph, True, True)) == ex["hdp_threshold_0_1"]
+
+
+@pytest.mark.skipif(not os.path.exists(A.LASTZ), reason="lastz not built (oracle/build_lastz.sh)")
+def test_lastz_anchors_reproduce_fixture():
+    """getRemappedAnchors (stateMachineTests.c:132-138) restated over the reference's own lastz gives
+    the committed anchors: ZymoRef against the read's 2D sequence, remapped by its template event
+    map, overlaps filtered."""
+    z = zymo_banded()
+    got = A.remapped_anchors(z["reference"], z["two_d_read"], z["template_event_map"])
+    assert [list(a) for a in got] == z["anchors"].tolist()
+    assert len(got) > 20
