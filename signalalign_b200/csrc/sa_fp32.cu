@@ -30,7 +30,6 @@ using namespace dp32;
 }  // namespace sa
 
 #include "sa_fp32_kernel.cuh"
-#include "sa_warp_kernel.cuh"
 
 namespace sa {
 namespace fp32 {
@@ -54,16 +53,6 @@ __global__ void __launch_bounds__(256) fma_probe(float *sink, int iters, float s
 // Slack after the emission and forward stores: the kernels' clamped look-ahead loads past a
 // region's last anti-diagonal stay inside the allocation.
 constexpr size_t kStoreSlack = 1024;
-
-// ring rows of a region for the warp kernels: room for four of its longest traceback windows (the
-// forward sweep runs ahead of the windows by up to that much), at least 64, at most the region
-// itself, a power of two
-int32_t ring_rows_for(int64_t n, int64_t max_span) {
-    const int64_t want = std::max<int64_t>(64, 4 * (max_span + 3));
-    int64_t r = 64;
-    while (r < want && r < n + 1) r <<= 1;
-    return (int32_t) r;
-}
 
 // device memory bound of a batch's plain-form reads
 constexpr size_t kPlainBatchMaxBytes = (size_t) 64 << 30;
@@ -99,13 +88,6 @@ struct sa_batch {
     int64_t cells = 0, out_total = 0;
     int32_t max_width = 0;
     float threshold = 0.01f;
-    // warp kernels (bands that fit one warp): per-region rings, in-place Gaussian emissions
-    bool warp = false;
-    int64_t ring_floats = 0, erow_floats = 0, n_echunks = 0;
-    Span<wk::WRegion> wregions;
-    Span<wk::WModel> wmodels;
-    Span<int4> wmeta;
-    Span<Chunk> echunks;
     // inputs, staged on the host with the device layout (one copy uploads them all)
     Span<RegionDesc> regions;
     Span<int32_t> order;
@@ -145,12 +127,6 @@ struct sa_batch {
     int32_t *d_status = nullptr;
     Control *d_ctl = nullptr;
     Event32 *d_events = nullptr;
-    wk::WRegion *d_wregions = nullptr;
-    wk::WModel *d_wmodels = nullptr;
-    int4 *d_wmeta = nullptr;
-    Chunk *d_echunks = nullptr;
-    float4 *d_events4 = nullptr;
-    int32_t *d_wflag = nullptr;
     float *d_E = nullptr, *d_F = nullptr, *d_fshift = nullptr;
     double *d_base = nullptr;
     int32_t *d_ready = nullptr;
@@ -207,41 +183,6 @@ size_t layout(sa_batch *b, unsigned char *host_in, unsigned char *host_res, unsi
     };
     const size_t nr = (size_t) b->n_regions, nd = (size_t) b->n_diags, nw = (size_t) b->n_windows;
     const size_t nreads = (size_t) b->n_reads, cells = (size_t) b->cells;
-    if (b->warp) {
-        place(b->wregions, b->d_wregions, nr, host_in, 0);
-        place(b->order, b->d_order, nr, host_in, 0);
-        place(b->wmodels, b->d_wmodels, b->models.size(), host_in, 0);
-        place(b->read_scale, b->d_read_scale, nreads, host_in, 0);
-        place(b->read_scale64, b->d_read_scale64, nreads, host_in, 0);
-        place(b->wmeta, b->d_wmeta, nd, host_in, 0);
-        place(b->windows, b->d_windows, nw, host_in, 0);
-        place(b->wtask, b->d_wtask, nw, host_in, 0);
-        place(b->echunks, b->d_echunks, (size_t) b->n_echunks, host_in, 0);
-        place(b->kmer, b->d_kmer, (size_t) b->n_kmers, host_in, 0);
-        place(b->events, b->d_events_raw, (size_t) b->n_events, host_in, 0);
-        place(b->read_win, b->d_read_win, 2 * nreads, host_in, 0);
-        b->in_bytes = (at + 255) & ~(size_t) 255;
-        at = b->in_bytes;
-        b->res_off = at;
-        place(b->read_base, b->d_read_base, nreads, host_res, b->res_off);
-        place(b->read_count, b->d_read_count, nreads, host_res, b->res_off);
-        place(b->loglik, b->d_loglik, nr, host_res, b->res_off);
-        place(b->dev_status, b->d_status, nreads, host_res, b->res_off);
-        place(b->ctl, b->d_ctl, 1, host_res, b->res_off);
-        b->res_bytes = ((at + 255) & ~(size_t) 255) - b->res_off;
-        work(b->d_events4, (size_t) b->n_events + 4);
-        work(b->d_E, (size_t) b->erow_floats + kStoreSlack);
-        work(b->d_F, (size_t) b->ring_floats + kStoreSlack);
-        work(b->d_base, nd);
-        work(b->d_fshift, nd);
-        work(b->d_ready, nw);
-        work(b->d_wflag, nw);
-        work(b->d_out, (size_t) b->out_total);
-        work(b->d_wcount, nw);
-        work(b->d_packed, (size_t) b->out_total);
-        b->dev_bytes = (at + 255) & ~(size_t) 255;
-        return b->dev_bytes;
-    }
     place(b->regions, b->d_regions, nr, host_in, 0);
     place(b->order, b->d_order, nr, host_in, 0);
     place(b->mdesc, b->d_models, b->models.size(), host_in, 0);
@@ -310,128 +251,10 @@ struct ReadPlan {
     std::vector<Region> regs;
     int64_t diags = 0, cells = 0, windows = 0, chunks = 0, out = 0;
     int32_t max_width = 0;
-    // warp kernels: per region its window bases, ring rows and emission-row floats
-    bool warp_ok = true;
-    std::vector<std::vector<int32_t>> xb;
-    std::vector<int32_t> ring_rows;
-    int64_t ring_floats = 0, erow_floats = 0, echunks = 0;
     // packing offsets
     int64_t region_base = 0, diag_base = 0, cell_base = 0, win_base = 0, chunk_base = 0, kmer_base = 0,
-            event_base = 0, out_base = 0, ring_base = 0, erow_base = 0, echunk_base = 0;
+            event_base = 0, out_base = 0;
 };
-
-// Window bases of a region for the warp kernels: per anti-diagonal d a multiple of 4, xb, such that
-// the columns of the bands of d-1, d and d+1 lie in [xb + 1, xb + 126] (a forward step reads d-1
-// and d-2 at slot x - 1, a window step d+1 and d+2 at slot x + 1, a refresh d+1's cells); changed
-// only when the band leaves it.  False if some band neighbourhood is too wide for one warp.
-bool plan_window_bases(const Region &rg, std::vector<int32_t> &xb) {
-    const int64_t n = rg.lX + rg.lY;
-    xb.resize(n + 1);
-    auto xl = [&](int64_t d) { return (int32_t) ((d + rg.xmy_l[d]) / 2); };
-    auto xr = [&](int64_t d) { return (int32_t) ((d + rg.xmy_r[d]) / 2); };
-    bool have = false;
-    int32_t cur = 0;
-    for (int64_t d = 0; d <= n; ++d) {
-        int32_t lo = xl(d), hi = xr(d);
-        if (d > 0) { lo = std::min(lo, xl(d - 1)); hi = std::max(hi, xr(d - 1)); }
-        if (d < n) { lo = std::min(lo, xl(d + 1)); hi = std::max(hi, xr(d + 1)); }
-        if (!have || lo < cur + 1 || hi > cur + wk::kSlots - 2) {
-            cur = (lo - 1) & ~3;   // rounded down (toward -inf) to a multiple of 4
-            have = true;
-            if (hi > cur + wk::kSlots - 2) return false;
-        }
-        xb[d] = cur;
-    }
-    return true;
-}
-
-// first column of an anti-diagonal's emission row (a multiple of 4) and its length (a multiple of 4)
-inline void erow_span(int32_t d, int32_t xmy_l, int32_t xmy_r, int32_t &xa, int32_t &len) {
-    const int32_t xL = (d + xmy_l) / 2, xR = (d + xmy_r) / 2;
-    xa = xL & ~3;
-    len = ((xR - xa + 1) + 3) & ~3;
-}
-
-// Packs one read's inputs for the warp kernels: per region its descriptor, per anti-diagonal the
-// band start, width and flags with the window base and emission-row offset, per window its task and
-// output segment, emission-row chunks of HDP regions; the read's k-mer ids and events.
-void pack_read_warp(sa_batch *b, int64_t r, const sa_read &rd, const ReadPlan &rp) {
-    const bool stored = rd.sm->emission == SA_EMIT_HDP;
-    for (int64_t x = 0; x < rp.lX; ++x) b->kmer[rp.kmer_base + x] = rp.kid[x];
-    for (int64_t y = 0; y < rd.n_events; ++y)
-        b->events[rp.event_base + y] = make_double2(rd.events[y * kEventParams], rd.events[y * kEventParams + 1]);
-    int64_t dbase = rp.diag_base, wbase = rp.win_base, obase = rp.out_base, ring = rp.ring_base, erow = rp.erow_base;
-    int64_t ech = rp.echunk_base;
-    std::vector<int32_t> flags;
-    for (size_t gi = 0; gi < rp.regs.size(); ++gi) {
-        const Region &rg = rp.regs[gi];
-        const int32_t region = (int32_t) (rp.region_base + (int64_t) gi);
-        wk::WRegion d;
-        std::memset(&d, 0, sizeof(d));
-        d.n = (int32_t) (rg.lX + rg.lY);
-        d.lX = (int32_t) rg.lX;
-        d.lY = (int32_t) rg.lY;
-        d.read = (int32_t) r;
-        d.n_windows = (int32_t) rg.windows.size();
-        d.model = rp.model;
-        d.ragged_left = rg.ragged_left;
-        d.ragged_right = rg.ragged_right;
-        d.diag_base = dbase;
-        d.win_base = wbase;
-        d.kmer_base = rp.kmer_base + rg.x1;
-        d.event_base = rp.event_base + rg.y1;
-        d.x1 = rg.x1;
-        d.y1 = rg.y1;
-        d.ring_base = ring;
-        d.ring_rows = rp.ring_rows[gi];
-        d.stored = stored ? 1 : 0;
-        d.e_base = stored ? erow : -1;
-        flags.assign(d.n + 2, 0);
-        for (const Window &w : rg.windows) {
-            flags[w.D] |= kFlagWindowEnd;
-            for (int32_t q = w.from; q > w.T; q -= 10) flags[q] |= kFlagRefresh;
-        }
-        const std::vector<int32_t> &xb = rp.xb[gi];
-        int64_t eoff = 0;
-        for (int32_t dd = 0; dd <= d.n; ++dd) {
-            const int32_t w = (rg.xmy_r[dd] - rg.xmy_l[dd]) / 2 + 1;
-            int32_t f = flags[dd];
-            if ((flags[dd] | flags[dd + 1]) & kFlagRefresh) f |= kFlagStoreGaps;
-            b->wmeta[dbase + dd] = make_int4(rg.xmy_l[dd], w | f, xb[dd], (int32_t) eoff);
-            if (stored) {
-                int32_t xa, len;
-                erow_span(dd, rg.xmy_l[dd], rg.xmy_r[dd], xa, len);
-                eoff += len;
-            }
-        }
-        if (stored) {
-            for (int32_t d0 = 0; d0 <= d.n; d0 += kChunkDiags) {
-                Chunk &ch = b->echunks[ech++];
-                ch.region = region;
-                ch.d0 = d0;
-                ch.nd = std::min(kChunkDiags, d.n + 1 - d0);
-                ch.pad = 0;
-                ch.cell = 0;
-            }
-        }
-        for (size_t wi = 0; wi < rg.windows.size(); ++wi) {
-            const Window &w = rg.windows[wi];
-            WindowTask &t = b->wtask[wbase + (int64_t) wi];
-            t.region = region;
-            t.first_cell = 0;
-            t.out_cap = 4 * (w.from - w.T) + 64;
-            t.pad = 0;
-            t.out_base = obase;
-            obase += t.out_cap;
-            b->windows[wbase + (int64_t) wi] = w;
-        }
-        b->wregions[region] = d;
-        dbase += d.n + 1;
-        wbase += (int64_t) rg.windows.size();
-        ring += (int64_t) d.ring_rows * wk::kRowFloats;
-        erow += eoff;
-    }
-}
 
 // Host planning of a batch (no device work): per read its regions and their windows (in parallel
 // over reads), then the packed inputs, written straight into a host staging block (pinned when
@@ -504,51 +327,23 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         }
         rp.kid.resize(rp.lX);
         for (int64_t x = 1; x <= rp.lX; ++x) rp.kid[x - 1] = pt.ids[pt.first[x]];
-        const bool stored = rd.sm->emission == SA_EMIT_HDP;
         for (const Region &rg : rp.regs) {
             const int64_t n = rg.lX + rg.lY;
             rp.diags += n + 1;
             rp.cells += rg.cells;
             rp.windows += (int64_t) rg.windows.size();
             rp.chunks += (n + kChunkDiags) / kChunkDiags;
-            int64_t span = 0;
-            for (const Window &w : rg.windows) {
-                rp.out += 4 * (int64_t) (w.from - w.T) + 64;
-                span = std::max<int64_t>(span, (int64_t) w.D - w.T + 1);
-            }
+            for (const Window &w : rg.windows) rp.out += 4 * (int64_t) (w.from - w.T) + 64;
             rp.max_width = std::max(rp.max_width, rg.max_width);
-            // warp kernels
-            rp.xb.emplace_back();
-            if (!plan_window_bases(rg, rp.xb.back())) rp.warp_ok = false;
-            const int32_t rr = ring_rows_for(n, span);
-            rp.ring_rows.push_back(rr);
-            rp.ring_floats += (int64_t) rr * wk::kRowFloats;
-            if (stored) {
-                for (int64_t d = 0; d <= n; ++d) {
-                    int32_t xa, len;
-                    erow_span((int32_t) d, rg.xmy_l[d], rg.xmy_r[d], xa, len);
-                    rp.erow_floats += len;
-                }
-                rp.echunks += (n + kChunkDiags) / kChunkDiags;
-            }
         }
     });
     // packing offsets
     int64_t nreg = 0, ndiag = 0, ncell = 0, nwin = 0, nchunk = 0, nkmer = 0, nevent = 0, nout = 0;
-    int64_t nring = 0, nerow = 0, nechunk = 0;
-    bool warp_ok = true;
     for (int64_t r = 0; r < n_reads; ++r) {
         ReadPlan &rp = plan[r];
         b->read_status[r] = rp.status;
         rp.region_base = nreg; rp.diag_base = ndiag; rp.cell_base = ncell; rp.win_base = nwin;
         rp.chunk_base = nchunk; rp.kmer_base = nkmer; rp.event_base = nevent; rp.out_base = nout;
-        rp.ring_base = nring; rp.erow_base = nerow; rp.echunk_base = nechunk;
-        if (!rp.status && !rp.plain) {
-            warp_ok = warp_ok && rp.warp_ok;
-            nring += rp.ring_floats;
-            nerow += rp.erow_floats;
-            nechunk += rp.echunks;
-        }
         b->read_first_region[r] = nreg;
         b->read_n_regions[r] = (int64_t) rp.regs.size();
         nreg += (int64_t) rp.regs.size(); ndiag += rp.diags; ncell += rp.cells; nwin += rp.windows;
@@ -566,13 +361,6 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
             b->plain_reads.push_back(reads[r]);
         }
     if (b->max_width > kMaxCpt * kThreads) return SA_E_CAPACITY;
-    // the warp kernels take every batch whose bands fit a warp; wider ones run the CTA kernels
-    // (SA_FP32_KERNELS=cta selects the CTA kernels for every batch, =warp the warp kernels)
-    const char *kern = std::getenv("SA_FP32_KERNELS");
-    b->warp = warp_ok && kern && std::strcmp(kern, "warp") == 0;
-    b->ring_floats = nring;
-    b->erow_floats = nerow;
-    b->n_echunks = b->warp ? nechunk : 0;
     b->device = device < 0 ? 0 : device;
     b->n_regions = nreg; b->n_diags = ndiag; b->n_windows = nwin; b->n_chunks = nchunk;
     b->n_kmers = nkmer; b->n_events = nevent;
@@ -592,10 +380,6 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     parallel_for(n_reads, threads, [&](int64_t r) {
         const ReadPlan &rp = plan[r];
         if (rp.status || rp.plain) return;
-        if (b->warp) {
-            pack_read_warp(b, r, reads[r], rp);
-            return;
-        }
         const sa_read &rd = reads[r];
         const sa_state_machine *sm = rd.sm;
         for (int64_t x = 0; x < rp.lX; ++x) {
@@ -673,48 +457,12 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     // largest band area first (LPT order of the forward claims)
     std::vector<int32_t> order(nreg);
     std::iota(order.begin(), order.end(), 0);
-    std::vector<int64_t> area(nreg, 0);
-    for (int64_t r = 0; r < n_reads; ++r)
-        for (size_t gi = 0; gi < plan[r].regs.size(); ++gi)
-            area[plan[r].region_base + (int64_t) gi] = plan[r].regs[gi].cells;
+    std::vector<int64_t> area(nreg);
+    for (int64_t i = 0; i < nreg; ++i)
+        area[i] = (i + 1 < nreg ? b->regions[i + 1].cell_base : b->cells) - b->regions[i].cell_base;
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) { return area[a] > area[c]; });
     std::copy(order.begin(), order.end(), b->order.data());
     return SA_OK;
-}
-
-// kernel arguments of the warp kernels
-wk::WArgs make_wargs(const sa_batch *b) {
-    wk::WArgs a;
-    std::memset(&a, 0, sizeof(a));
-    a.regions = b->d_wregions;
-    a.order = b->d_order;
-    a.n_regions = b->n_regions;
-    a.models = b->d_wmodels;
-    a.read_scale = b->d_read_scale;
-    a.read_scale64 = b->d_read_scale64;
-    a.events_raw = b->d_events_raw;
-    a.events = b->d_events4;
-    a.meta = b->d_wmeta;
-    a.windows = b->d_windows;
-    a.wtask = b->d_wtask;
-    a.n_windows = b->n_windows;
-    a.wflag = b->d_wflag;
-    a.kmer = b->d_kmer;
-    a.F = b->d_F;
-    a.E = b->d_E;
-    a.base = b->d_base;
-    a.fshift = b->d_fshift;
-    a.ready = b->d_ready;
-    a.out = b->d_out;
-    a.wcount = b->d_wcount;
-    a.loglik = b->d_loglik;
-    a.status = b->d_status;
-    a.ctl = b->d_ctl;
-    a.threshold = b->threshold;
-    a.spin_limit = b->wait_limit;
-    a.echunks = b->d_echunks;
-    a.n_echunks = b->n_echunks;
-    return a;
 }
 
 }  // namespace
@@ -759,25 +507,7 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
     int prev = 0;
     cudaGetDevice(&prev);
     if (cudaSetDevice(b->device) != cudaSuccess) return SA_E_CUDA;
-    for (size_t i = 0; i < b->models.size() && b->warp; ++i) {
-        const sa_state_machine *sm = b->models[i];
-        wk::WModel &m = b->wmodels[i];
-        std::memset(&m, 0, sizeof(m));
-        m.kc = sm->dev.kcw;
-        m.emission = sm->emission;
-        for (int j = 0; j < 9; ++j) m.t[j] = (float) sm->t[j];
-        m.has_sx = m.t[SA_T_GAP_SWITCH_TO_X] > kNegInf ? 1 : 0;
-        if (sm->emission == SA_EMIT_HDP) {
-            const HdpTables &h = sm->hdp;
-            m.hdp64.match = sm->dev.match;
-            m.hdp64.grid = sm->dev.hdp_grid;
-            m.hdp64.density = sm->dev.hdp_density;
-            m.hdp64.slope = sm->dev.hdp_slope;
-            m.hdp64.kmer_row = sm->dev.hdp_kmer_row;
-            m.hdp64.grid_length = h.grid_length;
-        }
-    }
-    for (size_t i = 0; i < b->models.size() && !b->warp; ++i) {
+    for (size_t i = 0; i < b->models.size(); ++i) {
         const sa_state_machine *sm = b->models[i];
         ModelDesc &m = b->mdesc[i];
         std::memset(&m, 0, sizeof(m));
@@ -798,15 +528,7 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
     // every input in one copy: the staging block has the device layout
     if (cudaMemcpyAsync(b->dev_base, b->host_in.ptr, b->in_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
         st = SA_E_CUDA;
-    if (!st && b->n_events > 0 && b->warp) {
-        // events outside every region stay zero (finite emissions, masked by the band)
-        if (cudaMemsetAsync(b->d_events4, 0, sizeof(float4) * (size_t) (b->n_events + 4), s) != cudaSuccess)
-            st = SA_E_CUDA;
-        const wk::WArgs a = make_wargs(b);
-        wk::prep_events_w<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(b->n_regions, 4096)), 256, 0, s>>>(a);
-        count_launch();
-        if (cudaGetLastError() != cudaSuccess) st = SA_E_CUDA;
-    } else if (!st && b->n_events > 0) {
+    if (!st && b->n_events > 0) {
         const int64_t n = b->n_events;
         prep_events<<<(unsigned) std::min<int64_t>((n + 255) / 256, 4096), 256, 0, s>>>(b->d_events_raw, b->d_events, n);
         count_launch();
@@ -830,51 +552,9 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
     // ranges, log-likelihoods), the window pair counts, and the ready queue (-1 = empty)
     if (cudaMemsetAsync(b->dev_base + b->res_off, 0, b->res_bytes, s) != cudaSuccess ||
         cudaMemsetAsync(b->d_wcount, 0, sizeof(int64_t) * std::max<size_t>(1, nw), s) != cudaSuccess ||
-        cudaMemsetAsync(b->d_ready, 0xff, sizeof(int32_t) * std::max<size_t>(1, nw), s) != cudaSuccess ||
-        (b->warp && cudaMemsetAsync(b->d_wflag, 0, sizeof(int32_t) * std::max<size_t>(1, nw), s) != cudaSuccess))
+        cudaMemsetAsync(b->d_ready, 0xff, sizeof(int32_t) * std::max<size_t>(1, nw), s) != cudaSuccess)
         st = SA_E_CUDA;
-    if (!st && nr > 0 && b->warp) {
-        const wk::WArgs a = make_wargs(b);
-        int sms = 0, per_sm = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-        sms = std::max(1, sms);
-        b->timed = false;
-        if (b->owns_device && !b->ev[0])
-            for (cudaEvent_t &e : b->ev) cudaEventCreate(&e);
-        const bool timing = b->owns_device && b->ev[3];
-        if (timing) cudaEventRecord(b->ev[0], s);
-        if (b->n_echunks > 0) {
-            wk::emission_rows_kernel<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(sms * 16, (b->n_echunks + 3) / 4)),
-                                       128, 0, s>>>(a);
-            count_launch();
-        }
-        if (timing) cudaEventRecord(b->ev[1], s);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk::warp_worker, 32 * wk::kWarps, 0);
-        // a forward warp per region and about two warps of windows per region, so small batches on
-        // other streams run beside it
-        const int64_t want = (3 * (int64_t) nr + wk::kWarps - 1) / wk::kWarps;
-        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((int64_t) sms * std::max(1, per_sm), want));
-        wk::warp_worker<<<(unsigned) grid, 32 * wk::kWarps, 0, s>>>(a);
-        if (timing) cudaEventRecord(b->ev[2], s);
-        Args g;
-        std::memset(&g, 0, sizeof(g));
-        g.wtask = b->d_wtask;
-        g.out = b->d_out;
-        g.wcount = b->d_wcount;
-        g.ctl = b->d_ctl;
-        g.n_reads = b->n_reads;
-        g.read_win = b->d_read_win;
-        g.packed = b->d_packed;
-        g.read_base = b->d_read_base;
-        g.read_count = b->d_read_count;
-        gather_pairs<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(b->n_reads, sms * 4)), 256, 0, s>>>(g);
-        if (timing) {
-            cudaEventRecord(b->ev[3], s);
-            b->timed = true;
-        }
-        count_launch(2);
-        if (cudaGetLastError() != cudaSuccess) st = SA_E_CUDA;
-    } else if (!st && nr > 0) {
+    if (!st && nr > 0) {
         Args a;
         std::memset(&a, 0, sizeof(a));
         a.regions = b->d_regions;
@@ -1090,7 +770,7 @@ sa_status sa_measure_fp32_peak(int32_t device, double *tflops) {
     return st;
 }
 
-int64_t sa_batch_regions(const sa_batch *b) { return b ? b->n_regions : 0; }
+int64_t sa_batch_regions(const sa_batch *b) { return b ? (int64_t) b->regions.size() : 0; }
 
 sa_status sa_batch_set_wait_limit(sa_batch *b, int64_t cycles) {
     if (!b || cycles < 1) return SA_E_ARG;
@@ -1129,8 +809,7 @@ bool batch_models_resident(const sa_batch *b) {
     // only the machines of reads the FP32 kernels run: reads routed to the plain form report
     // SA_E_UNSUPPORTED on this path and never touch their machine's device tables
     std::vector<char> used(b->models.size(), 0);
-    for (int64_t r = 0; r < b->n_regions; ++r)
-        used[(size_t) (b->warp ? b->wregions[r].model : b->regions[r].model)] = 1;
+    for (int64_t r = 0; r < b->n_regions; ++r) used[(size_t) b->regions[r].model] = 1;
     for (size_t i = 0; i < b->models.size(); ++i)
         if (used[i] && !model_resident(b->models[i])) return false;
     return true;

@@ -552,7 +552,7 @@ void free_device_model(sa_state_machine *sm) {
     cudaSetDevice(d.device);
     cudaFree(d.match); cudaFree(d.gapy); cudaFree(d.gapx); cudaFree(d.klog);
     cudaFree(d.hdp_grid); cudaFree(d.hdp_density); cudaFree(d.hdp_slope); cudaFree(d.hdp_kmer_row);
-    cudaFree(d.kc32); cudaFree(d.gapx32); cudaFree(d.kcw);
+    cudaFree(d.kc32); cudaFree(d.gapx32);
     int dev = d.device;
     d = DeviceModel();
     d.device = dev;
@@ -595,7 +595,6 @@ sa_status ensure_device_model(sa_state_machine *sm) {
     const int64_t n = sm->n_kmers;
     std::vector<KmerConst32> kc(n);
     std::vector<float> gx(n);
-    std::vector<float4> kw(2 * n);
     for (int64_t i = 0; i < n; ++i) {
         const double *m = &sm->match[i * 5], *y = &sm->gapy[i * 5];
         KmerConst32 &c = kc[i];
@@ -609,15 +608,12 @@ sa_status ensure_device_model(sa_state_machine *sm) {
         c.half_lambda = (float) (0.5 * m[4]);
         c.gapx = (float) sm->gapx[i];
         gx[i] = (float) sm->gapx[i];
-        kw[2 * i] = make_float4((float) m[0], (float) (-0.5 / (m[1] * m[1])), (float) (-0.5 / (y[1] * y[1])), c.k_m);
-        kw[2 * i + 1] = make_float4(c.k_y, c.inv_nu, (float) (-0.5 * m[4]), c.gapx);
     }
     if (!st) st = upload(&d.match, sm->match.data(), sm->match.size());
     if (!st) st = upload(&d.gapy, sm->gapy.data(), sm->gapy.size());
     if (!st) st = upload(&d.gapx, sm->gapx.data(), sm->gapx.size());
     if (!st) st = upload(&d.kc32, kc.data(), kc.size());
     if (!st) st = upload(&d.gapx32, gx.data(), gx.size());
-    if (!st) st = upload(&d.kcw, kw.data(), kw.size());
     if (!st && sm->hdp.present) {
         const HdpTables &h = sm->hdp;
         st = upload(&d.hdp_grid, h.grid.data(), h.grid.size());

@@ -51,9 +51,6 @@ struct DeviceModel {
     // FP32 tables
     KmerConst32 *kc32 = nullptr;
     float *gapx32 = nullptr;
-    // per k-mer constants of the warp kernels' in-place Gaussian emissions, two float4:
-    // {mu, -1/(2 sd^2), -1/(2 sd_y^2), k_m}, {k_y, 1/noise mean, -lambda/2, gap-X log probability}
-    float4 *kcw = nullptr;
 };
 
 }  // namespace sa

@@ -40,20 +40,20 @@ def test_scratch_size_matches_header():
 
 
 def test_rejects_batch_larger_than_scratch():
-    """eight 15 kb reads need more than the scratch array: SA_E_CAPACITY before any device work, with
+    """two 15 kb reads need more than the scratch array: SA_E_CAPACITY before any device work, with
     the bytes needed reported"""
-    cfg = synth.config1(seed=21, n_reads=8, span=(15000, 15000))
+    cfg = synth.config1(seed=21, n_reads=2, span=(15000, 15000))
     sm = W.gpu_model(api, W.gaussian_model(cfg), orc.EMIT_DESCALED)
     with pytest.raises(api.SAError) as ei:
         api.align_batch_noalloc(_inputs(sm, cfg["reads"]), _params())
     assert ei.value.status == 11   # SA_E_CAPACITY
     keep = []
     arr = api._read_array(_inputs(sm, cfg["reads"]), keep)
-    off = np.zeros(9, np.int64)
-    status = np.zeros(8, np.int32)
+    off = np.zeros(3, np.int64)
+    status = np.zeros(2, np.int32)
     need = C.c_int64(0)
     p = _params()
-    st = api.lib().sa_align_batch_noalloc(arr, 8, C.byref(p), None, None, 0, off.ctypes.data_as(api._i64p),
+    st = api.lib().sa_align_batch_noalloc(arr, 2, C.byref(p), None, None, 0, off.ctypes.data_as(api._i64p),
                                           status.ctypes.data_as(C.POINTER(C.c_int32)), None, C.byref(need))
     assert st == 11
     assert need.value > api.NOALLOC_SCRATCH_BYTES
