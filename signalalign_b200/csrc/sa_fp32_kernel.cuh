@@ -585,7 +585,11 @@ __global__ void __launch_bounds__(32 * kEmitWarps) emission_kernel(const __grid_
 // The sweep is unrolled by three anti-diagonals: ring slots, shared maxima and the look-ahead
 // registers are indexed by d mod 3 at compile time, so nothing rotates and every look-ahead load
 // has three anti-diagonals to land.
-template <int CPT>
+// kSX: the machine's SWITCH_TO_X transition is finite.  A .model file leaves it at LOG_ZERO
+// (stateMachine3_loadTransitionsFromFile stores gap-Y -> gap-X in SWITCH_TO_Y, stateMachine.c:1139),
+// and logAdd(v, LOG_ZERO) is v exactly, so without it the gap-X state of the forward sweep and the
+// gap-Y state of the backward sweep take one logAdd less (the same values, bit for bit).
+template <int CPT, bool kSX>
 struct ForwardSweep {
     const Ctx &c;
     const Args &A;
@@ -691,7 +695,8 @@ struct ForwardSweep {
             // logAdd depends only on the difference of its arguments, so the cell's emission (and
             // the shift to this anti-diagonal's base) is added once after each state's fold
             float vX = lae(tab, lM[j] + t[T_OX], lX[j] + t[T_EX]);
-            vX = lae(tab, vX, lY[j] + t[T_SX]) + (eX[j] + shL);
+            if (kSX) vX = lae(tab, vX, lY[j] + t[T_SX]);
+            vX = vX + (eX[j] + shL);
             float vM = lae(tab, mM[j] + t[T_MC], mX[j] + t[T_MFGX]);
             vM = lae(tab, vM, mY[j] + t[T_MFGY]) + (eM[j] + shM);
             float vY = lae(tab, uM[j] + t[T_OY], uY[j] + t[T_EY]) + (eY[j] + shL);
@@ -811,8 +816,13 @@ struct ForwardSweep {
 
 template <int CPT>
 __device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
-    ForwardSweep<CPT> f(c, sh, ring);
-    f.run();
+    if (c.t[T_SX] > kNegInf) {
+        ForwardSweep<CPT, true> f(c, sh, ring);
+        f.run();
+    } else {
+        ForwardSweep<CPT, false> f(c, sh, ring);
+        f.run();
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -853,7 +863,7 @@ __device__ __forceinline__ void write_pairs(const Ctx &c, Shared *sh, const Wind
     n_out += before;
 }
 
-template <int CPT>
+template <int CPT, bool kSX>
 __device__ void window_task(const Ctx &c, Shared *sh, float *ring, float *chain, int64_t gw) {
     const Args &A = *c.A;
     const RegionDesc &R = c.R;
@@ -1019,7 +1029,7 @@ __device__ void window_task(const Ctx &c, Shared *sh, float *ring, float *chain,
                 const float ble = rg.st(1, 1)[il] + (eXl[j] + shU);
                 vM = lae(tab, vM, ble + t[T_OX]);
                 vX = lae(tab, vX, ble + t[T_EX]);
-                vY = lae(tab, vY, ble + t[T_SX]);
+                if (kSX) vY = lae(tab, vY, ble + t[T_SX]);
                 if (i >= W0) vM = vX = vY = kNegInf;
                 rg.st(0, 0)[i] = vM;
                 rg.st(0, 1)[i] = vX;
@@ -1130,7 +1140,7 @@ __device__ void window_task(const Ctx &c, Shared *sh, float *ring, float *chain,
 // warp reduction, pairs numbered by ballots, no block barrier.  Look-ahead loads go to registers
 // indexed by the parity of the step, so they land without register moves; the operands of a
 // refresh (one anti-diagonal in ten) are loaded when it happens.
-template <int WCPT>
+template <int WCPT, bool kSX>
 struct WarpWindow {
     const Ctx &c;
     const Args &A;
@@ -1283,7 +1293,7 @@ struct WarpWindow {
                 const float le = ble[j] + (qX[K][j] + shU);
                 vM = lae(tab, vM, le + t[T_OX]);
                 vX = lae(tab, vX, le + t[T_EX]);
-                vY = lae(tab, vY, le + t[T_SX]);
+                if (kSX) vY = lae(tab, vY, le + t[T_SX]);
                 const bool in = lane + 32 * j < W0;
                 bM[j] = in ? vM : kNegInf;
                 bX[j] = in ? vX : kNegInf;
@@ -1522,8 +1532,13 @@ __global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(cons
             if (id < 0) break;
             Ctx c;
             ctx_init(c, A, A.wtask[id].region);
-            WarpWindow<kWarpWindowCpt> w(c, wring, wchain, sh->la);
-            w.run(id);
+            if (c.t[T_SX] > kNegInf) {
+                WarpWindow<kWarpWindowCpt, true> w(c, wring, wchain, sh->la);
+                w.run(id);
+            } else {
+                WarpWindow<kWarpWindowCpt, false> w(c, wring, wchain, sh->la);
+                w.run(id);
+            }
         }
     } else {
         float *ring = area, *chain = area + 9 * (A.wmax + 2);
@@ -1537,7 +1552,8 @@ __global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(cons
             if (id < 0) break;
             Ctx c;
             ctx_init(c, A, A.wtask[id].region);
-            window_task<CPT>(c, sh, ring, chain, id);
+            if (c.t[T_SX] > kNegInf) window_task<CPT, true>(c, sh, ring, chain, id);
+            else window_task<CPT, false>(c, sh, ring, chain, id);
             __syncthreads();
         }
     }
