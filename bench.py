@@ -217,6 +217,16 @@ def time_oracle(m, reads, budget_s, threads):
     return tot / dt, tot, dt, len(chosen)
 
 
+def launch_source(device):
+    """where the worker's launch configuration came from: the tuner's table row for this device, or
+    the library's defaults"""
+    import torch
+    from signalalign_b200 import api, tune
+    name = torch.cuda.get_device_name(device)
+    rows = tune.read_table(api.LAUNCH_CONFIGS)
+    return "tuned (python -m signalalign_b200.tune, %s)" % name if (name, 1) in rows else "defaults"
+
+
 def run_reference(args):
     """`--impl reference`: the reference path on the host cores.  signalAlign's C sources need the
     un-vendored sonLib library, so the reference arm is the FP64 CPU restatement (the oracle), which
@@ -669,6 +679,8 @@ def main():
                 "warmup": max(3, args.warmup), "ms_per_step": t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "global_batch": args.reads * world, "regions": b.regions,
+                           "launch_config": api.get_launch_config(local, 1),
+                           "launch_config_source": launch_source(local),
                            "cells_per_step_per_gpu": cells, "parallelism": "dp%d (read sharding)" % world,
                            "l2": "flushed between timed steps (256 MiB write); forward store >> L2"},
                 "reads_per_sec": reads_per_s,

@@ -231,6 +231,32 @@ int64_t sa_batch_regions(const sa_batch *b);
  * forward / traceback-window worker, the pair gather.  Waits for them.  SA_E_ARG if the batch has
  * not run (no counterpart in signalAlign: a diagnostic of this engine) */
 sa_status sa_batch_kernel_ms(const sa_batch *b, double *emission_ms, double *worker_ms, double *gather_ms);
+/* ---- launch configuration of the batched FP32 kernels, and its tuner (no counterpart in signalAlign,
+ * which has no GPU code) ----
+ * Per device (by name) and band-width class (1: bands up to 128 cells, 2: up to 256, 4: up to 512)
+ * one configuration; a device without one uses the defaults below, measured on B200. */
+typedef struct {
+    int32_t ctas_per_sm;           /* worker CTAs per SM (at most the kernel's occupancy; default 2) */
+    int32_t grid_per_region;       /* worker grid at most this many CTAs per region (default 3) */
+    int32_t warp_windows;          /* class 1: a traceback window per warp (1, default) or per CTA (0) */
+    int32_t emission_ctas_per_sm;  /* emission kernel grid, CTAs per SM (default 16) */
+} sa_launch_config;
+
+/* the configuration sa_batch_run uses on `device` for a width class */
+sa_status sa_getLaunchConfig(int32_t device, int32_t width_class, sa_launch_config *cfg);
+/* sets it for every device with the same name as `device` (values out of range: SA_E_ARG) */
+sa_status sa_setLaunchConfig(int32_t device, int32_t width_class, const sa_launch_config *cfg);
+/* Times every candidate configuration on a created and uploaded batch (`repeats` runs each after
+ * one untimed run, device time of its kernels by CUDA events), sets the fastest for the batch's
+ * device and width class, and returns it with its mean time; *n_tried counts the candidates.
+ * The batch's results are those of its last run. */
+sa_status sa_tuneLaunchConfig(sa_batch *b, void *stream, int32_t repeats, sa_launch_config *best, double *best_ms,
+                              int32_t *n_tried);
+/* Reads configurations from a text file, one per line: device name, width class and the four
+ * fields, tab-separated (lines starting with '#' are comments); they apply to devices of that name.
+ * A missing file is SA_E_FILE. */
+sa_status sa_loadLaunchConfigs(const char *path);
+
 /* Bound, in SM clock cycles, of every device-side wait of the batch's worker kernel (a warp waiting
  * for a traceback window to be published).  Default 2e10 (about 10 s), far beyond any forward sweep.
  * A wait that runs out sets the batch's error flag: every other waiter leaves, the kernel ends

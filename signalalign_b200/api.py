@@ -14,6 +14,8 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsa_b200.so")
+# launch configurations chosen by the tuner (python -m signalalign_b200.tune), read when the library loads
+LAUNCH_CONFIGS = os.path.join(_HERE, "launch_configs.tsv")
 
 THREE_STATE, THREE_STATE_HDP = 2, 7
 EMIT_PLAIN, EMIT_DESCALED, EMIT_HDP = 0, 1, 2
@@ -31,6 +33,15 @@ class SAError(RuntimeError):
     def __init__(self, status, where=""):
         self.status = int(status)
         super().__init__("%s: %s (status %d)" % (where, STATUS.get(self.status, "unknown"), self.status))
+
+
+class LaunchConfig(C.Structure):
+    """sa_launch_config: launch choices of the batched FP32 kernels"""
+    _fields_ = [("ctas_per_sm", C.c_int32), ("grid_per_region", C.c_int32), ("warp_windows", C.c_int32),
+                ("emission_ctas_per_sm", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Params(C.Structure):
@@ -137,6 +148,10 @@ def _bind(L):
         "sa_batch_kernel_ms": (C.c_int, [vp, _f64p, _f64p, _f64p]),
         "sa_batch_transfer_bytes": (C.c_int, [vp, _i64p, _i64p]),
         "sa_batch_set_wait_limit": (C.c_int, [vp, C.c_int64]),
+        "sa_getLaunchConfig": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(LaunchConfig)]),
+        "sa_setLaunchConfig": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(LaunchConfig)]),
+        "sa_tuneLaunchConfig": (C.c_int, [vp, vp, C.c_int32, C.POINTER(LaunchConfig), _f64p, C.POINTER(C.c_int32)]),
+        "sa_loadLaunchConfigs": (C.c_int, [C.c_char_p]),
         "sa_batch_destroy": (None, [vp]),
         "sa_align_batch_noalloc": (C.c_int, [C.POINTER(Read), C.c_int64, C.POINTER(Params), vp,
                                              C.POINTER(AlignedPair), C.c_int64, _i64p, C.POINTER(C.c_int32), _f64p,
@@ -195,6 +210,8 @@ def lib():
             raise ImportError("libsa_b200.so is not built (run `python -m signalalign_b200.build` or "
                               "__graft_entry__.build())")
         _lib = _bind(C.CDLL(LIB_PATH))
+        if os.path.exists(LAUNCH_CONFIGS):
+            _check(_lib.sa_loadLaunchConfigs(LAUNCH_CONFIGS.encode()), "loadLaunchConfigs")
     return _lib
 
 
@@ -595,6 +612,26 @@ class Server:
 def allocation_count():
     """device and pinned-host allocations the library has made in this process (sa_allocation_count)"""
     return lib().sa_allocation_count()
+
+
+def get_launch_config(device=0, width_class=1):
+    """the launch configuration sa_batch_run uses on `device` for a band-width class (1, 2, 4)"""
+    c = LaunchConfig()
+    _check(lib().sa_getLaunchConfig(device, width_class, C.byref(c)), "getLaunchConfig")
+    return c.as_dict()
+
+
+def set_launch_config(device, width_class, cfg):
+    c = LaunchConfig(**cfg)
+    _check(lib().sa_setLaunchConfig(device, width_class, C.byref(c)), "setLaunchConfig")
+
+
+def tune_launch_config(batch, stream=None, repeats=3):
+    """sa_tuneLaunchConfig on an uploaded Batch: (best configuration, its mean ms, candidates tried)"""
+    c, ms, n = LaunchConfig(), C.c_double(0), C.c_int32(0)
+    _check(lib().sa_tuneLaunchConfig(batch._h, stream, repeats, C.byref(c), C.byref(ms), C.byref(n)),
+           "tuneLaunchConfig")
+    return c.as_dict(), ms.value, n.value
 
 
 def kernel_launch_count():

@@ -13,7 +13,12 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <sstream>
+#include <string>
 #include <thread>
 #include <type_traits>
 #include <vector>
@@ -75,6 +80,50 @@ struct Span {
     size_t size() const { return n; }
     T &operator[](size_t i) const { return p[i]; }
 };
+
+// ------------------------------------------------------------------------------------------------
+// launch configurations of the batched kernels, per device name and band-width class
+// ------------------------------------------------------------------------------------------------
+namespace {
+
+std::mutex g_launch_mutex;
+std::map<std::pair<std::string, int>, sa_launch_config> g_launch;   // (device name, width class)
+
+// the choices measured on B200: two worker CTAs per SM, at most three CTAs per region (a forward CTA
+// and about two CTAs of window warps, so small batches on other streams run beside it), a window
+// per warp for bands up to 128 cells, 16 emission CTAs per SM
+sa_launch_config default_launch() { return sa_launch_config{2, 3, 1, 16}; }
+
+bool valid_launch(const sa_launch_config &c) {
+    return c.ctas_per_sm >= 1 && c.ctas_per_sm <= 32 && c.grid_per_region >= 1 && c.grid_per_region <= 64 &&
+           (c.warp_windows == 0 || c.warp_windows == 1) && c.emission_ctas_per_sm >= 1 &&
+           c.emission_ctas_per_sm <= 64;
+}
+
+bool valid_width_class(int w) { return w == 1 || w == 2 || w == 4; }
+
+std::string device_name(int device) {
+    static std::mutex m;
+    static std::map<int, std::string> names;
+    std::lock_guard<std::mutex> lock(m);
+    auto it = names.find(device);
+    if (it != names.end()) return it->second;
+    cudaDeviceProp prop;
+    std::string name;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) name = prop.name;
+    else cudaGetLastError();
+    if (!name.empty()) names[device] = name;
+    return name;
+}
+
+sa_launch_config launch_for(int device, int width_class) {
+    const std::string name = device_name(device);
+    std::lock_guard<std::mutex> lock(g_launch_mutex);
+    auto it = g_launch.find({name, width_class});
+    return it != g_launch.end() ? it->second : default_launch();
+}
+
+}  // namespace
 
 struct sa_batch {
     int device = 0;
@@ -138,6 +187,9 @@ struct sa_batch {
     std::vector<double> read_ll;
     bool downloaded = false;
     long long wait_limit = 20000000000LL;   // clock cycles a worker may wait for a window (~10 s)
+    bool has_cfg = false;                   // the tuner's candidate instead of the device's table
+    sa_launch_config cfg{};
+    int width_class = 1;
     // device timing of the last run's kernels (batches that own their device memory only)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool timed = false;
@@ -591,7 +643,10 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         a.read_count = b->d_read_count;
         const int cpt = std::max(1, (b->max_width + kThreads - 1) / kThreads);
         const int cpt_pow2 = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
+        b->width_class = cpt_pow2;
+        const sa_launch_config cfg = b->has_cfg ? b->cfg : launch_for(b->device, cpt_pow2);
         a.wmax = cpt_pow2 * kThreads;
+        a.warp_windows = cfg.warp_windows;
         a.spin_limit = b->wait_limit;
         const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) worker_area_floats(cpt_pow2);
         int sms = 0, per_sm = 0;
@@ -602,16 +657,15 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
             for (cudaEvent_t &e : b->ev) cudaEventCreate(&e);
         const bool timing = b->owns_device && b->ev[3];
         if (timing) cudaEventRecord(b->ev[0], s);
-        emission_kernel<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(sms * 16, (a.n_chunks + kEmitWarps - 1) /
-                                                                                            kEmitWarps)),
+        emission_kernel<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>((int64_t) sms * cfg.emission_ctas_per_sm,
+                                                                            (a.n_chunks + kEmitWarps - 1) / kEmitWarps)),
                           32 * kEmitWarps, 0, s>>>(a);
         if (timing) cudaEventRecord(b->ev[1], s);
         auto launch = [&](auto kern) {
             if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
-            // a small batch takes a forward CTA and about two CTAs of window warps per region, so
-            // small batches on other streams run beside it
-            const int64_t grid = std::min<int64_t>((int64_t) sms * std::max(1, per_sm), 3 * (int64_t) nr);
+            per_sm = std::max(1, std::min(per_sm, cfg.ctas_per_sm));
+            const int64_t grid = std::min<int64_t>((int64_t) sms * per_sm, (int64_t) cfg.grid_per_region * (int64_t) nr);
             kern<<<(unsigned) grid, kThreads, smem, s>>>(a);
         };
         if (cpt_pow2 == 1) launch(worker_kernel<1>);
@@ -776,6 +830,97 @@ sa_status sa_batch_set_wait_limit(sa_batch *b, int64_t cycles) {
     if (!b || cycles < 1) return SA_E_ARG;
     b->wait_limit = (long long) cycles;
     return SA_OK;
+}
+
+sa_status sa_getLaunchConfig(int32_t device, int32_t width_class, sa_launch_config *cfg) {
+    if (!cfg || device < 0 || !valid_width_class(width_class)) return SA_E_ARG;
+    *cfg = launch_for(device, width_class);
+    return SA_OK;
+}
+
+sa_status sa_setLaunchConfig(int32_t device, int32_t width_class, const sa_launch_config *cfg) {
+    if (!cfg || device < 0 || !valid_width_class(width_class) || !valid_launch(*cfg)) return SA_E_ARG;
+    const std::string name = device_name(device);
+    if (name.empty()) return SA_E_CUDA;
+    std::lock_guard<std::mutex> lock(g_launch_mutex);
+    g_launch[{name, width_class}] = *cfg;
+    return SA_OK;
+}
+
+sa_status sa_loadLaunchConfigs(const char *path) {
+    if (!path) return SA_E_ARG;
+    std::ifstream in(path);
+    if (!in) return SA_E_FILE;
+    std::string line;
+    std::vector<std::pair<std::pair<std::string, int>, sa_launch_config>> rows;
+    while (std::getline(in, line)) {
+        if (line.empty() || line[0] == '#') continue;
+        std::vector<std::string> f;
+        std::stringstream ss(line);
+        std::string tok;
+        while (std::getline(ss, tok, '\t')) f.push_back(tok);
+        if (f.size() != 6) return SA_E_FILE;
+        sa_launch_config c;
+        int wc = 0;
+        try {
+            wc = std::stoi(f[1]);
+            c.ctas_per_sm = std::stoi(f[2]);
+            c.grid_per_region = std::stoi(f[3]);
+            c.warp_windows = std::stoi(f[4]);
+            c.emission_ctas_per_sm = std::stoi(f[5]);
+        } catch (...) {
+            return SA_E_FILE;
+        }
+        if (!valid_width_class(wc) || !valid_launch(c)) return SA_E_FILE;
+        rows.push_back({{f[0], wc}, c});
+    }
+    std::lock_guard<std::mutex> lock(g_launch_mutex);
+    for (const auto &r : rows) g_launch[r.first] = r.second;
+    return SA_OK;
+}
+
+sa_status sa_tuneLaunchConfig(sa_batch *b, void *stream, int32_t repeats, sa_launch_config *best, double *best_ms,
+                              int32_t *n_tried) {
+    if (!b || !best || !best_ms || !n_tried || repeats < 1 || !b->owns_device) return SA_E_ARG;
+    const int cpt = std::max(1, (b->max_width + kThreads - 1) / kThreads);
+    const int wc = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
+    std::vector<sa_launch_config> cand;
+    for (int cps : {1, 2})
+        for (int gpr : {2, 3, 4, 6})
+            for (int ww : {1, 0})
+                for (int ecs : {8, 16, 32}) {
+                    if (wc != 1 && (ww == 0 || cps == 2)) continue;   // wider bands: CTA windows, one CTA per SM
+                    cand.push_back(sa_launch_config{cps, gpr, ww, ecs});
+                }
+    double best_t = 1e300;
+    sa_launch_config best_c = default_launch();
+    int tried = 0;
+    for (const sa_launch_config &c : cand) {
+        b->has_cfg = true;
+        b->cfg = c;
+        double total = 0.0;
+        for (int r = 0; r <= repeats; ++r) {
+            sa_status st = sa_batch_run(b, stream);
+            double em = 0, wk = 0, ga = 0;
+            if (!st) st = sa_batch_kernel_ms(b, &em, &wk, &ga);
+            if (st) {
+                b->has_cfg = false;
+                return st;
+            }
+            if (r > 0) total += em + wk + ga;   // the first run is untimed
+        }
+        ++tried;
+        const double t = total / repeats;
+        if (t < best_t) {
+            best_t = t;
+            best_c = c;
+        }
+    }
+    b->has_cfg = false;
+    *best = best_c;
+    *best_ms = best_t;
+    *n_tried = tried;
+    return sa_setLaunchConfig(b->device, wc, &best_c);
 }
 
 void sa_batch_destroy(sa_batch *b) { delete b; }

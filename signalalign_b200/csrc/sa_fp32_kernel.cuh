@@ -166,6 +166,7 @@ struct Args {
     Control *ctl;
     float threshold;
     int32_t wmax;                   // ring width (cells); rings hold wmax + 2 floats per state
+    int32_t warp_windows;           // bands up to 128 cells: a window per warp (else per CTA)
     long long spin_limit;           // clock cycles a worker may wait for a window
     // gather
     int64_t n_reads;
@@ -1517,8 +1518,9 @@ __global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(cons
         forward_task<CPT>(c, sh, area);
         __syncthreads();
     }
-    // traceback windows, in publication order
-    if (CPT == 1) {
+    // traceback windows, in publication order: one per warp for bands up to 128 cells (when the
+    // launch configuration asks for it), else one per CTA
+    if (CPT == 1 && A.warp_windows) {
         const int lane = tid & 31, warp = tid >> 5;
         float *wring = area + warp * kWarpWindowFloats;
         float *wchain = wring + 9 * (kWarpWindowWidth + 2);

@@ -1,0 +1,91 @@
+"""Autotuner of the batched FP32 kernels' launch configuration.
+
+    python -m signalalign_b200.tune [--reads 256] [--seed 1] [--repeats 3] [--device 0]
+
+Builds the benchmark workload (seeded synthetic reads, reference spans ~U(2 kb, 20 kb), 6-mer ACGT
+Gaussian table, diagonal expansion 50), uploads it once, and times every candidate configuration
+on it through sa_tuneLaunchConfig: worker CTAs per SM, the worker grid's CTAs per region, one
+traceback window per warp or per CTA, and the emission kernel's grid.  The fastest is written to
+launch_configs.tsv beside the library (one row per device name and band-width class; rows of other
+devices and classes are kept), which the library reads when it loads.
+"""
+import argparse
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def workload(n_reads, seed):
+    from signalalign_b200 import synth
+    cfg = synth.config1(seed=seed, n_reads=n_reads)
+    return cfg, synth.model_text(cfg["alphabet"], cfg["k"], cfg["table"])
+
+
+def read_table(path):
+    rows = {}
+    if os.path.exists(path):
+        with open(path) as fh:
+            for line in fh:
+                if not line.strip() or line.startswith("#"):
+                    continue
+                f = line.rstrip("\n").split("\t")
+                rows[(f[0], int(f[1]))] = [int(v) for v in f[2:]]
+    return rows
+
+
+def write_table(path, rows):
+    with open(path, "w") as fh:
+        fh.write("# device name\twidth class\tctas_per_sm\tgrid_per_region\twarp_windows\temission_ctas_per_sm\n")
+        for (name, wc), v in sorted(rows.items()):
+            fh.write("\t".join([name, str(wc)] + [str(x) for x in v]) + "\n")
+
+
+def tune(n_reads=256, seed=1, repeats=3, device=0, path=None):
+    """Times the candidates on the workload, sets and saves the fastest; returns a summary dict."""
+    import tempfile
+    import torch
+    from signalalign_b200 import api
+    torch.cuda.set_device(device)
+    cfg, text = workload(n_reads, seed)
+    with tempfile.NamedTemporaryFile("w", suffix=".model", delete=False) as fh:
+        fh.write(text)
+        mpath = fh.name
+    try:
+        sm = api.StateMachine.load(mpath, api.THREE_STATE, api.EMIT_DESCALED, device=device)
+    finally:
+        os.unlink(mpath)
+    p = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=50, threshold=0.01)
+    reads = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                           scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
+    b = api.Batch(reads, p)
+    b.upload()
+    before = api.get_launch_config(device, 1)
+    best, best_ms, tried = api.tune_launch_config(b, None, repeats)
+    name = torch.cuda.get_device_name(device)
+    path = path or api.LAUNCH_CONFIGS
+    rows = read_table(path)
+    rows[(name, 1)] = [best["ctas_per_sm"], best["grid_per_region"], best["warp_windows"],
+                       best["emission_ctas_per_sm"]]
+    write_table(path, rows)
+    return {"device": name, "width_class": 1, "workload_reads": n_reads, "candidates": tried, "repeats": repeats,
+            "previous": before, "best": best, "best_kernels_ms": best_ms, "table": path}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reads", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--repeats", type=int, default=3)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--out", default=None, help="table to write (default: launch_configs.tsv beside the library)")
+    a = ap.parse_args()
+    print(json.dumps(tune(a.reads, a.seed, a.repeats, a.device, a.out)), flush=True)
+
+
+if __name__ == "__main__":
+    main()

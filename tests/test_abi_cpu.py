@@ -253,3 +253,24 @@ def test_reference_nhdp_through_product_loader(api):
     sm2 = api.StateMachine.load(model, api.THREE_STATE_HDP, api.EMIT_HDP, nhdp_file=nhdp, set_hdp_expected_values=True)
     ev = formats.hdp_expected_values(m, want)
     assert np.allclose(sm2.tables()["match"], ev["match"], rtol=1e-12, atol=1e-12)
+
+
+def test_launch_config_table(api, tmp_path):
+    """sa_loadLaunchConfigs reads the tuner's table (tab-separated: device name, width class, four
+    fields); malformed rows and missing files are SA_E_FILE; without a device (or for a device the
+    table does not name) the defaults apply."""
+    good = tmp_path / "cfg.tsv"
+    good.write_text("# device\twidth\tcps\tgpr\tww\tecs\nNo Such GPU\t1\t1\t4\t0\t8\nNo Such GPU\t2\t1\t2\t0\t16\n")
+    assert api.lib().sa_loadLaunchConfigs(str(good).encode()) == 0
+    for bad in ("No Such GPU\t3\t1\t4\t0\t8\n", "No Such GPU\t1\t0\t4\t0\t8\n", "No Such GPU\t1\t1\t4\n",
+                "No Such GPU\t1\tx\t4\t0\t8\n"):
+        p = tmp_path / "bad.tsv"
+        p.write_text(bad)
+        assert api.lib().sa_loadLaunchConfigs(str(p).encode()) == 8
+    assert api.lib().sa_loadLaunchConfigs(str(tmp_path / "missing.tsv").encode()) == 8
+    with pytest.raises(api.SAError):
+        api.get_launch_config(0, 3)
+    import torch
+    if not torch.cuda.is_available():
+        assert api.get_launch_config(0, 1) == dict(ctas_per_sm=2, grid_per_region=3, warp_windows=1,
+                                                   emission_ctas_per_sm=16)

@@ -408,3 +408,44 @@ def test_fp32_bounded_wait_runs_out(api):
         om = W.oracle_model(m, orc.EMIT_DESCALED, rd)
         want = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], _op(p), True, True)
         assert W.max_posterior_error(want, b.pairs(i), p.threshold) <= FP32_TOL
+
+
+def test_fp32_launch_configurations(api):
+    """Every launch configuration the tuner can choose gives the oracle's pairs: a traceback window
+    per CTA instead of per warp (FP32 tolerance: different sweep code), and grid shapes (identical
+    pairs: each window is computed the same way whichever CTA runs it).  Then the tuner itself on a
+    small batch: it tries the candidates, sets the fastest for the device, and the batch's results
+    after it are still the oracle's."""
+    cfg = synth.config1(seed=41, n_reads=6, span=(800, 3000))
+    m = W.gaussian_model(cfg)
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED)
+    inputs = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                            scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
+    p = _p(api)
+    default = api.get_launch_config(0, 1)
+    wants = []
+    for rd in cfg["reads"]:
+        om = W.oracle_model(m, orc.EMIT_DESCALED, rd)
+        wants.append(orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], _op(p), True, True))
+    try:
+        base = api.align_batch(inputs, p)
+        for c in (dict(default, warp_windows=0), dict(default, ctas_per_sm=1, grid_per_region=2),
+                  dict(default, grid_per_region=6, emission_ctas_per_sm=8)):
+            api.set_launch_config(0, 1, c)
+            b = api.align_batch(inputs, p)
+            for i, want in enumerate(wants):
+                assert b.status(i) == 0
+                assert W.max_posterior_error(want, b.pairs(i), p.threshold) <= FP32_TOL, (c, i)
+                if c["warp_windows"] == default["warp_windows"]:
+                    assert np.array_equal(b.pairs(i), base.pairs(i)), (c, i)
+        api.set_launch_config(0, 1, default)
+        b = api.Batch(inputs, p)
+        b.upload()
+        best, ms, tried = api.tune_launch_config(b, None, 1)
+        assert tried >= 8 and ms > 0
+        assert api.get_launch_config(0, 1) == best
+        b.download()
+        for i, want in enumerate(wants):
+            assert W.max_posterior_error(want, b.pairs(i), p.threshold) <= FP32_TOL
+    finally:
+        api.set_launch_config(0, 1, default)
