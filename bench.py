@@ -293,6 +293,8 @@ def run_serve(args):
         cap = len(sat) / (time.perf_counter() - t0)
         rate = args.load * cap
         arrivals = np.cumsum(r.exponential(1.0 / rate, n))
+        stats0 = srv.stats()
+        allocs0, alloc_ms0 = api.allocation_count(), api.allocation_ms()
         sampler = ClockSampler(0)
         sampler.start()
         tickets = []
@@ -307,15 +309,37 @@ def run_serve(args):
         res = []
         for t, L, c in tickets:
             srv.wait(t, 600000.0)
-            st, pairs, ll, lat = srv.result(t)
-            res.append((st, L, c, lat))
+            st, pairs, ll, lat = srv.result(t, release=False)
+            q, l = srv.timing(t)
+            srv.release(t)
+            res.append((st, L, c, lat, q, l))
         wall = time.perf_counter() - t0
         clocks = sampler.stop()
+        stats = {k: v - stats0[k] for k, v in srv.stats().items()}
+        allocs, alloc_ms = api.allocation_count() - allocs0, api.allocation_ms() - alloc_ms0
+        blog = srv.batch_log()
     finally:
         srv.close()
+    # micro-batches on the device at once (device event times of their kernels)
+    ev = sorted([(b[0], 1) for b in blog] + [(b[1], -1) for b in blog], key=lambda e: (e[0], e[1]))
+    conc = peak = 0
+    for _, d in ev:
+        conc += d
+        peak = max(peak, conc)
     lat = np.array([x[3] for x in res])
     spans_ok = np.array([x[1] for x in res])
-    ten = lat[(spans_ok >= 8000) & (spans_ok <= 12000)]
+    sel = (spans_ok >= 8000) & (spans_ok <= 12000)
+    ten = lat[sel]
+    # where the 8-12 kb reads' time went: waiting for a stream and budget, planning and upload of
+    # their micro-batch, and the rest (kernels until the read was published, copy of its pairs)
+    queue = np.array([x[4] for x in res])[sel]
+    launch = np.array([x[5] for x in res])[sel]
+    run = ten - queue - launch
+
+    def pct(v):
+        return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)), "max": float(np.max(v))} \
+            if len(v) else None
+    worst = int(np.argmax(ten)) if len(ten) else None
     cells = sum(x[2] for x in res)
     line = {"metric": "serving_p99_latency_ms", "value": float(np.percentile(lat, 99)), "unit": "ms",
             "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
@@ -329,7 +353,18 @@ def run_serve(args):
             "reads_8to12kb": int(len(ten)),
             "capacity_reads_per_sec": cap, "offered_reads_per_sec": rate,
             "achieved_reads_per_sec": n / wall, "cells_per_sec": cells / wall,
-            "errors": int(sum(1 for x in res if x[0] != 0)), "clocks": clocks}
+            "errors": int(sum(1 for x in res if x[0] != 0)),
+            "reads_finished_on_publication": stats["reads_early"],
+            "reads_finished_at_batch_end": stats["reads_at_batch_end"],
+            "micro_batches": stats["batches"], "max_concurrent_micro_batches": peak,
+            "breakdown_8to12kb_ms": {"queue": pct(queue), "plan_upload_launch": pct(launch), "kernels_and_copy": pct(run),
+                                     "slowest": None if worst is None else
+                                     {"total": float(ten[worst]), "queue": float(queue[worst]),
+                                      "plan_upload_launch": float(launch[worst]), "kernels_and_copy": float(run[worst])}},
+            "dispatcher_ms": {"admit": stats["admit_ms"], "plan": stats["plan_ms"], "upload": stats["upload_ms"],
+                              "fetch": stats["fetch_ms"], "finish": stats["finish_ms"], "wall": 1000.0 * wall},
+            "allocations_in_timed_run": {"count": allocs, "ms": alloc_ms},
+            "clocks": clocks}
     print(json.dumps(line), flush=True)
 
 

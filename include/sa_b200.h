@@ -314,7 +314,9 @@ sa_status sa_align_batch_noalloc(const sa_read *reads, int64_t n_reads, const sa
  * A dispatcher thread admits waiting reads into a new micro-batch whenever a stream is free and the
  * band cells in flight (estimated as (reference_length + n_events + 1) x (diagonal_expansion + 1)
  * per read) stay within max_inflight_cells; each micro-batch runs on its own stream, beside the ones
- * already on the device.  A read's result does not depend on which reads share its micro-batch. */
+ * already on the device.  A read finishes as soon as its own traceback windows have: the worker
+ * kernel publishes it to mapped host memory and its pairs are copied while the kernel runs on.
+ * A read's result does not depend on which reads share its micro-batch. */
 typedef struct sa_server sa_server;
 sa_status sa_server_create(int32_t device, int64_t max_inflight_cells, int32_t max_batches, sa_server **out);
 /* queue one read (its arrays are copied); *ticket identifies it */
@@ -328,6 +330,25 @@ sa_status sa_server_result(sa_server *s, int64_t ticket, int32_t *status, const 
 sa_status sa_server_release(sa_server *s, int64_t ticket);
 /* finishes the queued reads, then stops the dispatcher */
 void sa_server_destroy(sa_server *s);
+typedef struct sa_server_counters {
+    int64_t reads_early;          /* reads finished when the kernel published them */
+    int64_t reads_at_batch_end;   /* reads finished with their micro-batch (plain form, errors) */
+    int64_t batches;              /* micro-batches finished */
+    double admit_ms;              /* dispatcher time planning, uploading and launching micro-batches */
+    double fetch_ms;              /* dispatcher time copying published reads' pairs */
+    double finish_ms;             /* dispatcher time finishing micro-batches */
+    double plan_ms;               /* the planning part of admit_ms (sa_batch_create) */
+    double upload_ms;             /* the upload part of admit_ms (sa_batch_upload) */
+} sa_server_counters;
+sa_status sa_server_stats(sa_server *s, sa_server_counters *out);
+/* a finished read's wait: from submission to the start of its micro-batch's admission, and from
+ * there to its kernels' launch (planning and upload); both 0 for a read that was never launched.
+ * The rest of its latency is the kernels and the copy of its pairs. */
+sa_status sa_server_read_timing(sa_server *s, int64_t ticket, double *queue_ms, double *launch_ms);
+/* per finished micro-batch, in finishing order, three doubles: device time of its start (before its
+ * emission kernel) and of its worker kernel's end, in ms from the server's creation, and its read
+ * count (0, 0 when the batch was not timed); min(capacity, n) triples are written */
+sa_status sa_server_batch_log(sa_server *s, double *out, int64_t capacity, int64_t *n_batches);
 
 /* ---- EM expectations: the same path with the expectation epilogue (pairwiseAligner.c:1983-2003) ---- */
 
@@ -528,6 +549,8 @@ int64_t sa_kernel_launch_count(void);
  * this process (no counterpart in signalAlign: a diagnostic; memory pools reuse blocks, so a warm
  * steady state adds none) */
 int64_t sa_allocation_count(void);
+/* host time those allocation calls took, in milliseconds */
+double sa_allocation_ms(void);
 /* FP32 FMA issue rate of `device` in TFLOP/s, measured by a short probe kernel (the denominator of
  * the engine's compute roofline; no counterpart in signalAlign) */
 sa_status sa_measure_fp32_peak(int32_t device, double *tflops);

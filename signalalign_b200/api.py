@@ -163,6 +163,9 @@ def _bind(L):
                                        _f64p, _f64p]),
         "sa_server_release": (C.c_int, [vp, C.c_int64]),
         "sa_server_destroy": (None, [vp]),
+        "sa_server_stats": (C.c_int, [vp, C.POINTER(ServerCounters)]),
+        "sa_server_read_timing": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "sa_server_batch_log": (C.c_int, [vp, C.POINTER(C.c_double), C.c_int64, _i64p]),
         "sa_filterToRemoveOverlap": (C.c_int, [_i64p, C.c_int64, _i64p, _i64p]),
         "sa_guideAlignmentToRebasedAnchorPairs": (C.c_int, [C.POINTER(GuideAlignment), C.POINTER(CigarOp), C.c_int64,
                                                             C.c_int64, _i64p, C.c_int64, _i64p]),
@@ -191,6 +194,7 @@ def _bind(L):
         "sa_status_string": (C.c_char_p, [C.c_int]),
         "sa_kernel_launch_count": (C.c_int64, []),
         "sa_allocation_count": (C.c_int64, []),
+        "sa_allocation_ms": (C.c_double, []),
         "sa_measure_fp32_peak": (C.c_int, [C.c_int32, _f64p]),
     }
     for name, (res, args) in sig.items():
@@ -565,6 +569,12 @@ def align_batch_noalloc(reads, p, stream=None, pair_capacity=None):
     raise SAError(6, "align_batch_noalloc")
 
 
+class ServerCounters(C.Structure):
+    _fields_ = [("reads_early", C.c_int64), ("reads_at_batch_end", C.c_int64), ("batches", C.c_int64),
+                ("admit_ms", C.c_double), ("fetch_ms", C.c_double), ("finish_ms", C.c_double),
+                ("plan_ms", C.c_double), ("upload_ms", C.c_double)]
+
+
 class Server:
     """Continuous-batching serving loop (sa_server_*): submit reads as they arrive, wait for each."""
 
@@ -600,6 +610,32 @@ class Server:
             lib().sa_server_release(self._h, ticket)
         return st.value, pairs, ll.value, lat.value
 
+    def stats(self):
+        """sa_server_counters as a dict: reads finished on publication / at their micro-batch's end,
+        micro-batches, and the dispatcher's time admitting, fetching and finishing (ms)"""
+        c = ServerCounters()
+        _check(lib().sa_server_stats(self._h, C.byref(c)), "server_stats")
+        return {f: getattr(c, f) for f, _ in ServerCounters._fields_}
+
+    def timing(self, ticket):
+        """(queue_ms, launch_ms) of a finished read not yet released"""
+        q, l = C.c_double(0), C.c_double(0)
+        _check(lib().sa_server_read_timing(self._h, ticket, C.byref(q), C.byref(l)), "server_read_timing")
+        return q.value, l.value
+
+    def release(self, ticket):
+        _check(lib().sa_server_release(self._h, ticket), "server_release")
+
+    def batch_log(self):
+        """per finished micro-batch (start_ms, worker_end_ms, reads): device times from the server's
+        creation, in finishing order"""
+        n = C.c_int64(0)
+        _check(lib().sa_server_batch_log(self._h, None, 0, C.byref(n)), "server_batch_log")
+        out = np.zeros(3 * max(n.value, 1), np.float64)
+        _check(lib().sa_server_batch_log(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), n.value, C.byref(n)),
+               "server_batch_log")
+        return [tuple(out[3 * i: 3 * i + 3]) for i in range(n.value)]
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value and _lib is not None:
             _lib.sa_server_destroy(self._h)
@@ -612,6 +648,11 @@ class Server:
 def allocation_count():
     """device and pinned-host allocations the library has made in this process (sa_allocation_count)"""
     return lib().sa_allocation_count()
+
+
+def allocation_ms():
+    """host time the library's device and pinned-host allocations took, in ms (sa_allocation_ms)"""
+    return lib().sa_allocation_ms()
 
 
 def get_launch_config(device=0, width_class=1):

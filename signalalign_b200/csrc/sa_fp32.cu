@@ -150,11 +150,12 @@ struct sa_batch {
     Span<int32_t> kmer;
     Span<float> gapx;
     Span<double2> events;
-    Span<int64_t> read_win;                 // per read: first window, window count
+    Span<int64_t> read_win;                 // per read: first window, window count, first region, region count
     // results, mirrored from one contiguous device range (one copy downloads them all)
     Span<int64_t> read_base, read_count;
     Span<double> loglik;
     Span<int32_t> dev_status;
+    Span<int32_t> read_wdone;
     Span<Control> ctl;
     size_t in_bytes = 0, res_off = 0, res_bytes = 0, dev_bytes = 0;
     // device pointers
@@ -174,6 +175,7 @@ struct sa_batch {
     int64_t *d_read_base = nullptr, *d_read_count = nullptr;
     double *d_loglik = nullptr;
     int32_t *d_status = nullptr;
+    int32_t *d_read_wdone = nullptr;
     Control *d_ctl = nullptr;
     Event32 *d_events = nullptr;
     float *d_E = nullptr, *d_F = nullptr, *d_fshift = nullptr;
@@ -183,6 +185,9 @@ struct sa_batch {
     int64_t *d_wcount = nullptr;
     // memory
     MemBlock host_in, host_res, host_pairs, dev;
+    MemBlock host_done;                     // per-read completion records (mapped pinned memory)
+    ReadDone *d_done = nullptr;             // their device address
+    int32_t run_seq = 0;                    // runs with per-read completion (a record's `done`)
     unsigned char *dev_base = nullptr;
     std::vector<double> read_ll;
     bool downloaded = false;
@@ -206,6 +211,7 @@ struct sa_batch {
         mem_put(host_in);
         mem_put(host_res);
         mem_put(host_pairs);
+        mem_put(host_done);
         if (owns_device) mem_put(dev);
     }
 };
@@ -247,7 +253,7 @@ size_t layout(sa_batch *b, unsigned char *host_in, unsigned char *host_res, unsi
     place(b->kmer, b->d_kmer, (size_t) b->n_kmers, host_in, 0);
     place(b->gapx, b->d_gapx, (size_t) b->n_kmers, host_in, 0);
     place(b->events, b->d_events_raw, (size_t) b->n_events, host_in, 0);
-    place(b->read_win, b->d_read_win, 2 * nreads, host_in, 0);
+    place(b->read_win, b->d_read_win, 4 * nreads, host_in, 0);
     b->in_bytes = (at + 255) & ~(size_t) 255;
     at = b->in_bytes;
     b->res_off = at;
@@ -255,6 +261,7 @@ size_t layout(sa_batch *b, unsigned char *host_in, unsigned char *host_res, unsi
     place(b->read_count, b->d_read_count, nreads, host_res, b->res_off);
     place(b->loglik, b->d_loglik, nr, host_res, b->res_off);
     place(b->dev_status, b->d_status, nreads, host_res, b->res_off);
+    place(b->read_wdone, b->d_read_wdone, nreads, host_res, b->res_off);
     place(b->ctl, b->d_ctl, 1, host_res, b->res_off);
     b->res_bytes = ((at + 255) & ~(size_t) 255) - b->res_off;
     work(b->d_events, (size_t) b->n_events);
@@ -357,7 +364,9 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     }
     std::vector<char> fp32_tables(b->models.size());
     for (size_t i = 0; i < b->models.size(); ++i) fp32_tables[i] = gapy_follows_match(b->models[i]);
-    const int threads = planning_threads();
+    // a thread per few reads: starting a thread costs about as much as planning a short read, so
+    // micro-batches of a few reads (a serving loop's) plan on the calling thread alone
+    const int threads = (int) std::min<int64_t>(planning_threads(), std::max<int64_t>(1, n_reads / 4));
     // k-mer ids, regions and windows of each read
     parallel_for(n_reads, threads, [&](int64_t r) {
         ReadPlan &rp = plan[r];
@@ -425,8 +434,10 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     for (int64_t r = 0; r < n_reads; ++r) {
         b->read_scale[r] = scale[r];
         b->read_scale64[r] = scale64[r];
-        b->read_win[2 * r] = plan[r].win_base;
-        b->read_win[2 * r + 1] = plan[r].windows;
+        b->read_win[4 * r] = plan[r].win_base;
+        b->read_win[4 * r + 1] = plan[r].windows;
+        b->read_win[4 * r + 2] = plan[r].region_base;
+        b->read_win[4 * r + 3] = (int64_t) plan[r].regs.size();
     }
     // the packed inputs, read by read
     parallel_for(n_reads, threads, [&](int64_t r) {
@@ -600,6 +611,9 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
     if (cudaSetDevice(b->device) != cudaSuccess) return SA_E_CUDA;
     const size_t nr = (size_t) b->n_regions, nw = (size_t) b->n_windows;
     sa_status st = SA_OK;
+    // every run gets a new number (from 1), also one that launches nothing: a record counts for the
+    // run whose number it holds
+    if (b->d_done) ++b->run_seq;
     // what the kernels expect cleared: the results block (counters, per-read status and pair
     // ranges, log-likelihoods), the window pair counts, and the ready queue (-1 = empty)
     if (cudaMemsetAsync(b->dev_base + b->res_off, 0, b->res_bytes, s) != cudaSuccess ||
@@ -641,6 +655,9 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         a.packed = b->d_packed;
         a.read_base = b->d_read_base;
         a.read_count = b->d_read_count;
+        a.read_wdone = b->d_read_wdone;
+        a.done_host = b->d_done;
+        a.done_seq = b->run_seq;
         const int cpt = std::max(1, (b->max_width + kThreads - 1) / kThreads);
         const int cpt_pow2 = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
         b->width_class = cpt_pow2;
@@ -672,12 +689,14 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         else if (cpt_pow2 == 2) launch(worker_kernel<2>);
         else launch(worker_kernel<4>);
         if (timing) cudaEventRecord(b->ev[2], s);
-        gather_pairs<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(b->n_reads, sms * 4)), 256, 0, s>>>(a);
+        // with per-read completion the worker has gathered every read it finished
+        if (!b->d_done)
+            gather_pairs<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(b->n_reads, sms * 4)), 256, 0, s>>>(a);
         if (timing) {
             cudaEventRecord(b->ev[3], s);
             b->timed = true;
         }
-        count_launch(3);
+        count_launch(b->d_done ? 2 : 3);
         if (cudaGetLastError() != cudaSuccess) st = SA_E_CUDA;
     }
     if (!st && b->plain) st = plain_run(b->plain, s);
@@ -967,5 +986,49 @@ size_t batch_bind_scratch(sa_batch *b, unsigned char *base) {
 }
 
 void batch_release_host(sa_batch *b) { delete b; }
+
+sa_status batch_publish_reads(sa_batch *b) {
+    if (!b || !b->owns_device) return SA_E_ARG;
+    if (b->d_done) return SA_OK;
+    const size_t bytes = sizeof(ReadDone) * (size_t) std::max<int64_t>(1, b->n_reads);
+    sa_status st = mem_get(MemKind::Pinned, b->device, bytes, b->host_done);
+    if (st) return st;
+    // pinned memory is mapped into every device's address space (unified addressing)
+    void *dptr = nullptr;
+    if (cudaHostGetDevicePointer(&dptr, b->host_done.ptr, 0) != cudaSuccess) {
+        cudaGetLastError();
+        mem_put(b->host_done);
+        return SA_E_CUDA;
+    }
+    std::memset(b->host_done.ptr, 0, bytes);
+    b->d_done = static_cast<ReadDone *>(dptr);
+    return SA_OK;
+}
+
+const ReadDone *batch_read_records(const sa_batch *b) {
+    return b && b->d_done ? static_cast<const ReadDone *>(b->host_done.ptr) : nullptr;
+}
+
+int32_t batch_run_seq(const sa_batch *b) { return b ? b->run_seq : 0; }
+
+sa_status batch_fetch_read(const sa_batch *b, const ReadDone &rec, sa_aligned_pair *dst, cudaStream_t stream) {
+    if (!b || rec.n_pairs < 0 || rec.first_pair < 0 || rec.first_pair + rec.n_pairs > b->out_total) return SA_E_ARG;
+    if (rec.n_pairs == 0) return SA_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(b->device) != cudaSuccess) return SA_E_CUDA;
+    const bool ok = cudaMemcpyAsync(dst, b->d_packed + rec.first_pair, sizeof(sa_aligned_pair) * (size_t) rec.n_pairs,
+                                    cudaMemcpyDeviceToHost, stream) == cudaSuccess &&
+                    cudaStreamSynchronize(stream) == cudaSuccess;
+    cudaSetDevice(prev);
+    return ok ? SA_OK : SA_E_CUDA;
+}
+
+bool batch_run_events(const sa_batch *b, cudaEvent_t *start, cudaEvent_t *end) {
+    if (!b || !b->timed) return false;
+    *start = b->ev[0];
+    *end = b->ev[2];
+    return true;
+}
 
 }  // namespace sa

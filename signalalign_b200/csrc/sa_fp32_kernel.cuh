@@ -170,10 +170,14 @@ struct Args {
     long long spin_limit;           // clock cycles a worker may wait for a window
     // gather
     int64_t n_reads;
-    const int64_t *read_win;        // per read: first window, window count
+    const int64_t *read_win;        // per read: first window, window count, first region, region count
     sa_aligned_pair *packed;
     int64_t *read_base;             // per read: first pair in the packed output
     int64_t *read_count;
+    // per-read completion (null: the gather launch packs every read after the worker)
+    int32_t *read_wdone;            // per read: windows finished
+    ReadDone *done_host;            // per read: record in mapped host memory
+    int32_t done_seq;               // this run's number, written to a record's `done`
 };
 
 struct Shared {
@@ -182,6 +186,8 @@ struct Shared {
     int32_t wcnt[2][kMaxCpt][kWarps];
     float fold[2];
     int32_t task_id;
+    int32_t done_read;
+    long long red[kWarps + 1];
 };
 
 // The reference's lookup (pairwiseAligner.c:237-248) picks one of four cubics by d <= 1, <= 2.5,
@@ -1494,6 +1500,123 @@ __device__ __forceinline__ int32_t wait_ready(const Args &A, int64_t slot) {
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// per-read gather and completion
+// ------------------------------------------------------------------------------------------------
+template <int NT>
+__device__ __forceinline__ void group_sync() {
+    if (NT == 32) __syncwarp();
+    else __syncthreads();
+}
+
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One read's windows' pairs concatenated in window order (regions, then windows: the reference's
+// emission order) into a range of the packed output claimed from the packed counter; sets the
+// read's range.  Run by a group of NT threads (one warp, or a whole CTA of NT threads with `red`
+// holding NT / 32 + 1 shared slots); every thread returns the range.  Window counts and pairs were
+// written by other CTAs, so they are read through L2.
+template <int NT>
+__device__ void gather_read(const Args &A, int64_t r, int tid, long long *red, long long &base, long long &tot) {
+    const int64_t w0 = A.read_win[4 * r], nw = A.read_win[4 * r + 1];
+    long long mine = 0;
+    for (int64_t k = tid; k < nw; k += NT)
+        mine += min(__ldcg(A.wcount + w0 + k), (int64_t) A.wtask[w0 + k].out_cap);
+    mine = warp_sum_ll(mine);
+    if (NT == 32) {
+        tot = mine;
+        base = tid == 0 && tot > 0 ? (long long) atomicAdd(&A.ctl->packed, (unsigned long long) tot) : 0;
+        base = __shfl_sync(0xffffffffu, base, 0);
+    } else {
+        if ((tid & 31) == 0) red[tid >> 5] = mine;
+        __syncthreads();
+        tot = 0;
+        for (int w = 0; w < NT / 32; ++w) tot += red[w];
+        if (tid == 0) red[NT / 32] = tot > 0 ? (long long) atomicAdd(&A.ctl->packed, (unsigned long long) tot) : 0;
+        __syncthreads();
+        base = red[NT / 32];
+    }
+    // 32 windows at a time: lane j of every warp holds window k0 + j's count and an inclusive scan
+    // of the counts, so the group copies window after window without a barrier between them
+    const int j = tid & 31;
+    long long run = 0;
+    for (int64_t k0 = 0; k0 < nw; k0 += 32) {
+        long long cnt = 0, ob = 0;
+        if (k0 + j < nw) {
+            cnt = min(__ldcg(A.wcount + w0 + k0 + j), (int64_t) A.wtask[w0 + k0 + j].out_cap);
+            ob = A.wtask[w0 + k0 + j].out_base;
+        }
+        long long inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (j >= o) inc += v;
+        }
+        const int m = (int) min((int64_t) 32, nw - k0);
+        for (int jj = 0; jj < m; ++jj) {
+            const long long c = __shfl_sync(0xffffffffu, cnt, jj);
+            const long long at = run + __shfl_sync(0xffffffffu, inc, jj) - c;
+            const int4 *src = reinterpret_cast<const int4 *>(A.out + __shfl_sync(0xffffffffu, ob, jj));
+            int4 *dst = reinterpret_cast<int4 *>(A.packed + base + at);
+            for (long long q = tid; q < 2 * c; q += NT) dst[q] = __ldcg(src + q);
+        }
+        run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    group_sync<NT>();
+    if (tid == 0) {
+        A.read_base[r] = base;
+        A.read_count[r] = tot;
+    }
+}
+
+// After a group of NT threads (tid 0..NT-1) finished traceback window `window`, with batches that
+// publish reads as they finish: the window is counted against its read, and the group that
+// finishes the read's last window gathers the read and writes its record to mapped host memory,
+// `done` last after a system-scope fence (the host then copies the pairs while the kernel runs on).
+template <int NT>
+__device__ void window_done(const Args &A, int64_t window, int tid, Shared *sh) {
+    if (!A.done_host) return;
+    __threadfence();   // this thread's pairs, count and total before the count below
+    group_sync<NT>();
+    int32_t last = -1;
+    if (tid == 0) {
+        const int32_t r = A.regions[A.wtask[window].region].read;
+        if (atomicAdd(A.read_wdone + r, 1) + 1 == (int32_t) A.read_win[4 * r + 1]) last = r;
+        __threadfence();
+    }
+    if (NT == 32) {
+        last = __shfl_sync(0xffffffffu, last, 0);
+    } else {
+        if (tid == 0) sh->done_read = last;
+        __syncthreads();
+        last = sh->done_read;
+        __syncthreads();
+    }
+    if (last < 0) return;
+    __threadfence();   // the read's other windows, counted before the last increment
+    long long base, tot;
+    gather_read<NT>(A, last, tid, sh->red, base, tot);
+    __threadfence_system();   // this thread's packed pairs before the record
+    group_sync<NT>();
+    if (tid == 0) {
+        const int64_t g0 = A.read_win[4 * last + 2], ng = A.read_win[4 * last + 3];
+        double ll = 0.0;
+        for (int64_t g = 0; g < ng; ++g) ll += __ldcg(A.loglik + g0 + g);
+        ReadDone *rec = A.done_host + last;
+        rec->first_pair = base;
+        rec->n_pairs = tot;
+        rec->log_likelihood = ll;
+        rec->status = __ldcg(A.status + last);
+        __threadfence_system();
+        *((volatile int32_t *) &rec->done) = A.done_seq;
+    }
+    group_sync<NT>();
+}
+
 // CPT: cells per thread of the forward sweep (128 threads per region).  The first claims are
 // forward sweeps, one per CTA; once none is left, windows are claimed: one per warp for bands up to
 // kWarpWindowWidth cells wide, one per CTA for wider bands.
@@ -1541,6 +1664,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(cons
                 WarpWindow<kWarpWindowCpt, false> w(c, wring, wchain, sh->la);
                 w.run(id);
             }
+            window_done<32>(A, id, lane, sh);
         }
     } else {
         float *ring = area, *chain = area + 9 * (A.wmax + 2);
@@ -1557,6 +1681,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(cons
             if (c.t[T_SX] > kNegInf) window_task<CPT, true>(c, sh, ring, chain, id);
             else window_task<CPT, false>(c, sh, ring, chain, id);
             __syncthreads();
+            window_done<kThreads>(A, id, tid, sh);
         }
     }
 }
@@ -1565,36 +1690,11 @@ __global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(cons
 // gather: per read, its windows' pairs in order into the packed output
 // ------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) gather_pairs(const __grid_constant__ Args A) {
-    __shared__ int64_t s_cnt[256];
-    __shared__ int64_t s_base, s_run;
-    const int tid = threadIdx.x;
+    __shared__ long long red[256 / 32 + 1];
+    long long base, tot;
     for (int64_t r = blockIdx.x; r < A.n_reads; r += gridDim.x) {
-        const int64_t w0 = A.read_win[2 * r], nw = A.read_win[2 * r + 1];
-        // total pairs of the read
-        int64_t mine = 0;
-        for (int64_t k = tid; k < nw; k += blockDim.x)
-            mine += min(A.wcount[w0 + k], (int64_t) A.wtask[w0 + k].out_cap);
-        s_cnt[tid] = mine;
+        gather_read<256>(A, r, threadIdx.x, red, base, tot);
         __syncthreads();
-        if (tid == 0) {
-            int64_t tot = 0;
-            for (int k = 0; k < (int) blockDim.x; ++k) tot += s_cnt[k];
-            s_base = tot > 0 ? (int64_t) atomicAdd(&A.ctl->packed, (unsigned long long) tot) : 0;
-            s_run = 0;
-            A.read_base[r] = s_base;
-            A.read_count[r] = tot;
-        }
-        __syncthreads();
-        // copy window by window, in order (a pair is two 16-byte words)
-        for (int64_t k = 0; k < nw; ++k) {
-            const int64_t cnt = min(A.wcount[w0 + k], (int64_t) A.wtask[w0 + k].out_cap);
-            const int4 *src = reinterpret_cast<const int4 *>(A.out + A.wtask[w0 + k].out_base);
-            int4 *dst = reinterpret_cast<int4 *>(A.packed + s_base + s_run);
-            for (int64_t q = tid; q < 2 * cnt; q += blockDim.x) dst[q] = src[q];
-            __syncthreads();
-            if (tid == 0) s_run += cnt;
-            __syncthreads();
-        }
     }
 }
 

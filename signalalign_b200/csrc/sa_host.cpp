@@ -5,6 +5,7 @@
 // the routine it re-implements (paths inside the signalAlign tree).
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -24,17 +25,25 @@ static std::atomic<int64_t> g_launches{0};
 void count_launch(int64_t n) { g_launches += n; }
 
 static std::atomic<int64_t> g_allocations{0};
+static std::atomic<int64_t> g_allocation_ns{0};
 
-cudaError_t device_malloc(void **ptr, size_t bytes) {
-    const cudaError_t rc = cudaMalloc(ptr, bytes);
+namespace {
+template <typename Fn>
+cudaError_t counted(Fn &&fn) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const cudaError_t rc = fn();
+    g_allocation_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
     if (rc == cudaSuccess) ++g_allocations;
     return rc;
 }
+}  // namespace
+
+cudaError_t device_malloc(void **ptr, size_t bytes) {
+    return counted([&]() { return cudaMalloc(ptr, bytes); });
+}
 
 cudaError_t pinned_malloc(void **ptr, size_t bytes) {
-    const cudaError_t rc = cudaHostAlloc(ptr, bytes, cudaHostAllocDefault);
-    if (rc == cudaSuccess) ++g_allocations;
-    return rc;
+    return counted([&]() { return cudaHostAlloc(ptr, bytes, cudaHostAllocDefault); });
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -848,5 +857,7 @@ const char *sa_status_string(sa_status s) {
 int64_t sa_kernel_launch_count(void) { return g_launches.load(); }
 
 int64_t sa_allocation_count(void) { return g_allocations.load(); }
+
+double sa_allocation_ms(void) { return 1e-6 * (double) g_allocation_ns.load(); }
 
 }  // extern "C"

@@ -165,6 +165,31 @@ size_t batch_bind_scratch(sa_batch *b, unsigned char *base);
 // frees the host side only (the device area belongs to the caller)
 void batch_release_host(sa_batch *b);
 
+// Per-read completion of a batch (the serving loop): the worker kernel's group that finishes a
+// read's last traceback window gathers the read's pairs into the packed output and writes the
+// read's record to mapped host memory, `done` last after a system-scope fence.  Reads that run no
+// window in the FP32 kernels (plan errors, plain-form reads, reads without windows) and reads of a
+// run whose bounded wait gave up get no record; their results come from sa_batch_download.  A
+// record belongs to the batch's latest run when its `done` equals batch_run_seq (runs are numbered
+// from 1, so records need no clearing between runs).
+struct ReadDone {
+    int64_t first_pair;       // in the packed output
+    int64_t n_pairs;
+    double log_likelihood;    // the read's regions' totals summed in region order
+    int32_t status;           // the read's device status (SA_OK or SA_E_OUTPUT)
+    int32_t done;             // the publishing run's number
+};
+// before sa_batch_run (batches that own their device memory): every later run publishes its reads;
+// the gather launch after the worker is then left out
+sa_status batch_publish_reads(sa_batch *b);
+// n_reads records (nullptr before batch_publish_reads) and the number of the latest run
+const ReadDone *batch_read_records(const sa_batch *b);
+int32_t batch_run_seq(const sa_batch *b);
+// copies a published read's pairs into dst on `stream` and waits for the copy
+sa_status batch_fetch_read(const sa_batch *b, const ReadDone &rec, sa_aligned_pair *dst, cudaStream_t stream);
+// timing events of the last run: before the emission kernel, after the worker kernel
+bool batch_run_events(const sa_batch *b, cudaEvent_t *start, cudaEvent_t *end);
+
 // the plain FP64 form over a set of reads (sa_fp64.cu): every region one CTA of one launch, F and
 // B in rings of the longest traceback window.  Used by the single-read entry and, inside batches,
 // for reads whose references have degenerate ('X') positions.

@@ -3,9 +3,12 @@
 // A batch needs one device block (inputs, stores, outputs) and two pinned host blocks (staged
 // inputs, results).  cudaMalloc / cudaHostAlloc of hundreds of megabytes cost milliseconds and can
 // synchronise the device, so released blocks go to a free list and the next batch of a similar size
-// takes one from there.  A request takes the smallest free block that is at least as large and at
-// most twice as large; otherwise a new block is allocated (rounded up to 2 MiB).  If an allocation
-// fails, the free blocks of that kind are released and the allocation is tried once more.
+// takes one from there.  Blocks come in power-of-two sizes (2 MiB and up), so batches whose sizes
+// vary (a serving loop's micro-batches) settle on a few size classes and stop allocating: a request
+// takes the smallest free block that is at least as large, otherwise a new block of the request's
+// class: an allocation (pinning host pages, mapping device memory) takes milliseconds, which a
+// serving loop cannot hide, while a larger block costs only idle memory.  If an allocation fails,
+// the free blocks of that kind are released and the allocation is tried once more.
 #include <algorithm>
 #include <cstdlib>
 #include <mutex>
@@ -73,7 +76,7 @@ sa_status mem_get(MemKind kind, int device, size_t bytes, MemBlock &out) {
     for (size_t i = 0; i < g_free.size(); ++i) {
         const MemBlock &b = g_free[i];
         if (b.kind != kind || (kind == MemKind::Device && b.device != device)) continue;
-        if (b.bytes < bytes || b.bytes > 2 * bytes + kRound) continue;
+        if (b.bytes < bytes) continue;
         if (best == g_free.size() || b.bytes < g_free[best].bytes) best = i;
     }
     if (best < g_free.size()) {
@@ -81,7 +84,8 @@ sa_status mem_get(MemKind kind, int device, size_t bytes, MemBlock &out) {
         g_free.erase(g_free.begin() + (std::ptrdiff_t) best);
         return SA_OK;
     }
-    const size_t rounded = (bytes + kRound - 1) / kRound * kRound;
+    size_t rounded = kRound;
+    while (rounded < bytes) rounded <<= 1;
     void *p = nullptr;
     if (!allocate(kind, device, rounded, &p)) {
         release_free(kind, device);
