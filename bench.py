@@ -716,6 +716,7 @@ def main():
                 "config": {"workload": WORKLOAD, "global_batch": args.reads * world, "regions": b.regions,
                            "launch_config": api.get_launch_config(local, 1),
                            "launch_config_source": launch_source(local),
+                           "forward_segments": dict(b.segment_info(), policy=list(api.get_segment_policy())),
                            "cells_per_step_per_gpu": cells, "parallelism": "dp%d (read sharding)" % world,
                            "l2": "flushed between timed steps (256 MiB write); forward store >> L2"},
                 "reads_per_sec": reads_per_s,
@@ -744,9 +745,10 @@ def main():
                 "critical_path": {"longest_region_antidiagonals": longest,
                                   "worker_ns_per_antidiagonal": wk_ms * 1e6 / longest,
                                   "alone_worker_ms": alone_ms, "frac": alone_ms / wk_ms,
-                                  "note": "the forward sweep of one region is sequential over its anti-diagonals; "
-                                          "alone_worker_ms is the worker kernel on the longest read alone (the "
-                                          "batch's latency bound), frac = alone / batch worker time"},
+                                  "note": "a region's forward sweep is sequential over its anti-diagonals unless "
+                                          "it is cut into forward segments; alone_worker_ms is the worker kernel "
+                                          "on the longest read alone (its segments on separate CTAs), frac = "
+                                          "alone / batch worker time"},
                 "gpu_launches": launches, "clocks": clocks}
     if world > 1:
         dist.barrier()
@@ -759,6 +761,7 @@ def main():
         # accuracy of the batched FP32 form against the FP64 oracle on every read of the batch
         bb = api.align_batch(reads, p, sptr)
         line["accuracy"] = accuracy_vs_oracle(m, cfg["reads"], bb.pairs, bb.log_likelihood, 0.01, threads)
+        line["accuracy"]["forward_segments"] = bb.segment_info()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -263,6 +263,30 @@ sa_status sa_loadLaunchConfigs(const char *path);
  * normally, and every read of the batch reports SA_E_TIMEOUT.  No counterpart in signalAlign (its
  * CPU code never waits); a diagnostic of this engine's bounded waits. */
 sa_status sa_batch_set_wait_limit(sa_batch *b, int64_t cycles);
+
+/* ---- forward segments (no counterpart in signalAlign, whose forward sweep runs once per region) ----
+ * A region's forward sweep is sequential over its anti-diagonals, so the longest read of a batch
+ * bounds the batch.  The batched form cuts it at traceback-window starts into segments that run at
+ * the same time on different CTAs.  Each segment after the first sweeps max(warmup_diags, 10 x the
+ * region's widest anti-diagonal) anti-diagonals before its own from a flat start; its values then
+ * equal the true ones minus one constant (the recursion depends only on differences of log values,
+ * and the start's influence dies out within a few band widths).  Where two segments meet, the kernel checks that on two
+ * anti-diagonals (every cell within 2e-5 + 1e-6 x its distance below the anti-diagonal's maximum);
+ * posteriors do not depend on the constant, and the log-likelihood adds it back.  A read whose
+ * check disagrees is re-run unsegmented in sa_batch_download, so results never depend on it.
+ * segment_diags: < 0 keeps every region whole; > 0 caps a segment's sweep (warm-up included);
+ * 0 (default) picks twice the batch's forward anti-diagonals per worker CTA, at least 4096 (a large
+ * batch, bound by its total work, then keeps nearly every region whole; a small one splits).
+ * warmup_diags: default 1024, at least 64.  Applies to batches created afterwards. */
+sa_status sa_setSegmentPolicy(int32_t segment_diags, int32_t warmup_diags);
+sa_status sa_getSegmentPolicy(int32_t *segment_diags, int32_t *warmup_diags);
+/* segments and stitches of a batch; after a download, reads re-run unsegmented and the largest
+ * deviation from the constant over the agreeing stitches */
+sa_status sa_batch_segment_info(const sa_batch *b, int64_t *n_segments, int64_t *n_stitches, int64_t *n_redone,
+                                double *max_spread);
+/* scale of the stitch tolerance for the batch's next runs (default 1; a negative scale makes every
+ * stitch disagree, which exercises the unsegmented re-run) */
+sa_status sa_batch_set_stitch_tolerance(sa_batch *b, double scale);
 void sa_batch_destroy(sa_batch *b);
 
 /* ---- batched FP32 form without device allocation (no counterpart in signalAlign) ---- */

@@ -148,6 +148,10 @@ def _bind(L):
         "sa_batch_kernel_ms": (C.c_int, [vp, _f64p, _f64p, _f64p]),
         "sa_batch_transfer_bytes": (C.c_int, [vp, _i64p, _i64p]),
         "sa_batch_set_wait_limit": (C.c_int, [vp, C.c_int64]),
+        "sa_setSegmentPolicy": (C.c_int, [C.c_int32, C.c_int32]),
+        "sa_getSegmentPolicy": (C.c_int, [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+        "sa_batch_segment_info": (C.c_int, [vp, _i64p, _i64p, _i64p, _f64p]),
+        "sa_batch_set_stitch_tolerance": (C.c_int, [vp, C.c_double]),
         "sa_getLaunchConfig": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(LaunchConfig)]),
         "sa_setLaunchConfig": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(LaunchConfig)]),
         "sa_tuneLaunchConfig": (C.c_int, [vp, vp, C.c_int32, C.POINTER(LaunchConfig), _f64p, C.POINTER(C.c_int32)]),
@@ -478,6 +482,18 @@ class Batch:
         """bound (SM clock cycles) of the worker kernel's device-side waits (sa_batch_set_wait_limit)"""
         _check(lib().sa_batch_set_wait_limit(self._h, int(cycles)), "batch_set_wait_limit")
 
+    def set_stitch_tolerance(self, scale):
+        """scale of the forward-segment stitch tolerance (negative: every stitch disagrees and every
+        segmented read is re-run unsegmented at download)"""
+        _check(lib().sa_batch_set_stitch_tolerance(self._h, float(scale)), "batch_set_stitch_tolerance")
+
+    def segment_info(self):
+        """dict: forward segments, stitches, reads re-run unsegmented, largest stitch deviation"""
+        a, b, c, d = C.c_int64(0), C.c_int64(0), C.c_int64(0), C.c_double(0)
+        _check(lib().sa_batch_segment_info(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
+               "batch_segment_info")
+        return dict(segments=a.value, stitches=b.value, redone=c.value, max_spread=d.value)
+
     @property
     def cells(self):
         return lib().sa_batch_cells(self._h)
@@ -653,6 +669,18 @@ def allocation_count():
 def allocation_ms():
     """host time the library's device and pinned-host allocations took, in ms (sa_allocation_ms)"""
     return lib().sa_allocation_ms()
+
+
+def set_segment_policy(segment_diags=0, warmup_diags=1024):
+    """forward segments of later batches: segment_diags < 0 keeps regions whole, > 0 caps a segment's
+    sweep, 0 picks the cap from the batch (sa_setSegmentPolicy)"""
+    _check(lib().sa_setSegmentPolicy(int(segment_diags), int(warmup_diags)), "setSegmentPolicy")
+
+
+def get_segment_policy():
+    a, b = C.c_int32(0), C.c_int32(0)
+    _check(lib().sa_getSegmentPolicy(C.byref(a), C.byref(b)), "getSegmentPolicy")
+    return a.value, b.value
 
 
 def get_launch_config(device=0, width_class=1):

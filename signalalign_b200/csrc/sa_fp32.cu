@@ -134,12 +134,15 @@ struct sa_batch {
     std::vector<int32_t> read_status;       // host planning status per read
     std::vector<int64_t> read_first_region, read_n_regions;
     int64_t n_regions = 0, n_diags = 0, n_windows = 0, n_chunks = 0, n_kmers = 0, n_events = 0;
+    int64_t n_segs = 0, n_stitch = 0, stitch_floats = 0;
     int64_t cells = 0, out_total = 0;
     int32_t max_width = 0;
     float threshold = 0.01f;
     // inputs, staged on the host with the device layout (one copy uploads them all)
     Span<RegionDesc> regions;
+    Span<Segment> segs;
     Span<int32_t> order;
+    Span<StitchDesc> stitch;
     Span<ModelDesc> mdesc;
     Span<ReadScale32> read_scale;
     Span<ReadScale64> read_scale64;
@@ -150,17 +153,27 @@ struct sa_batch {
     Span<int32_t> kmer;
     Span<float> gapx;
     Span<double2> events;
-    Span<int64_t> read_win;                 // per read: first window, window count, first region, region count
+    Span<int64_t> read_win;                 // per read: first window, window count, first region, region
+                                            // count, first stitch, stitch count, units, 0
     // results, mirrored from one contiguous device range (one copy downloads them all)
     Span<int64_t> read_base, read_count;
     Span<double> loglik;
     Span<int32_t> dev_status;
     Span<int32_t> read_wdone;
+    Span<int32_t> seg_fail;
+    Span<StitchRes> stitch_res;
     Span<Control> ctl;
     size_t in_bytes = 0, res_off = 0, res_bytes = 0, dev_bytes = 0;
     // device pointers
     RegionDesc *d_regions = nullptr;
+    Segment *d_segs = nullptr;
     int32_t *d_order = nullptr;
+    StitchDesc *d_stitch = nullptr;
+    StitchRes *d_stitch_res = nullptr;
+    float *d_stitch_vals = nullptr;
+    int32_t *d_seg_fail = nullptr;
+    Segment *d_redo_segs = nullptr;         // reads re-run unsegmented after a disagreeing stitch
+    int32_t *d_redo_order = nullptr;
     ModelDesc *d_models = nullptr;
     ReadScale32 *d_read_scale = nullptr;
     ReadScale64 *d_read_scale64 = nullptr;
@@ -192,6 +205,9 @@ struct sa_batch {
     std::vector<double> read_ll;
     bool downloaded = false;
     long long wait_limit = 20000000000LL;   // clock cycles a worker may wait for a window (~10 s)
+    float stitch_tol = 1.0f;                // scale of the stitch tolerance (negative: all disagree)
+    std::vector<char> redone;               // per read: re-run unsegmented after a disagreement
+    int64_t n_redone = 0;
     bool has_cfg = false;                   // the tuner's candidate instead of the device's table
     sa_launch_config cfg{};
     int width_class = 1;
@@ -242,7 +258,9 @@ size_t layout(sa_batch *b, unsigned char *host_in, unsigned char *host_res, unsi
     const size_t nr = (size_t) b->n_regions, nd = (size_t) b->n_diags, nw = (size_t) b->n_windows;
     const size_t nreads = (size_t) b->n_reads, cells = (size_t) b->cells;
     place(b->regions, b->d_regions, nr, host_in, 0);
-    place(b->order, b->d_order, nr, host_in, 0);
+    place(b->segs, b->d_segs, (size_t) b->n_segs, host_in, 0);
+    place(b->order, b->d_order, (size_t) b->n_segs, host_in, 0);
+    place(b->stitch, b->d_stitch, (size_t) b->n_stitch, host_in, 0);
     place(b->mdesc, b->d_models, b->models.size(), host_in, 0);
     place(b->read_scale, b->d_read_scale, nreads, host_in, 0);
     place(b->read_scale64, b->d_read_scale64, nreads, host_in, 0);
@@ -253,7 +271,7 @@ size_t layout(sa_batch *b, unsigned char *host_in, unsigned char *host_res, unsi
     place(b->kmer, b->d_kmer, (size_t) b->n_kmers, host_in, 0);
     place(b->gapx, b->d_gapx, (size_t) b->n_kmers, host_in, 0);
     place(b->events, b->d_events_raw, (size_t) b->n_events, host_in, 0);
-    place(b->read_win, b->d_read_win, 4 * nreads, host_in, 0);
+    place(b->read_win, b->d_read_win, 8 * nreads, host_in, 0);
     b->in_bytes = (at + 255) & ~(size_t) 255;
     at = b->in_bytes;
     b->res_off = at;
@@ -262,6 +280,8 @@ size_t layout(sa_batch *b, unsigned char *host_in, unsigned char *host_res, unsi
     place(b->loglik, b->d_loglik, nr, host_res, b->res_off);
     place(b->dev_status, b->d_status, nreads, host_res, b->res_off);
     place(b->read_wdone, b->d_read_wdone, nreads, host_res, b->res_off);
+    place(b->seg_fail, b->d_seg_fail, nreads, host_res, b->res_off);
+    place(b->stitch_res, b->d_stitch_res, (size_t) b->n_stitch, host_res, b->res_off);
     place(b->ctl, b->d_ctl, 1, host_res, b->res_off);
     b->res_bytes = ((at + 255) & ~(size_t) 255) - b->res_off;
     work(b->d_events, (size_t) b->n_events);
@@ -273,6 +293,9 @@ size_t layout(sa_batch *b, unsigned char *host_in, unsigned char *host_res, unsi
     work(b->d_out, (size_t) b->out_total);
     work(b->d_wcount, nw);
     work(b->d_packed, (size_t) b->out_total);
+    work(b->d_stitch_vals, (size_t) b->stitch_floats);
+    work(b->d_redo_segs, nr);
+    work(b->d_redo_order, nr);
     b->dev_bytes = (at + 255) & ~(size_t) 255;
     return b->dev_bytes;
 }
@@ -299,6 +322,44 @@ int planning_threads() {
     return (int) std::max(1u, std::thread::hardware_concurrency());
 }
 
+// Forward segments.  A region's forward sweep is cut at traceback-window starts into segments that
+// run at the same time; every later segment first sweeps `warm` anti-diagonals from a flat start.
+// Policy: segment_diags < 0 keeps every region whole, > 0 caps a segment's sweep (warm-up included)
+// at that many anti-diagonals, 0 picks the cap from the batch: twice the forward anti-diagonals per
+// worker CTA, at least kSegMin.  A batch's worker time is about the larger of its longest forward
+// chain and its total work (forward and traceback-window work per anti-diagonal together cost about
+// twice a worker CTA's forward step, measured on B200), so only chains longer than the total work
+// are cut: a large batch keeps nearly every region whole (no warm-up overhead), a small one (a
+// serving micro-batch) splits its long reads for latency.
+std::atomic<int32_t> g_seg_target{0};
+std::atomic<int32_t> g_seg_warm{1024};
+constexpr int64_t kSegMin = 4096;
+
+// Warm-up of a region's later segments: the start's influence dies out over a few band widths
+// (measured on the oracle's FP64 sweep: within 4.2 widths at diagonal expansion 50, 5.9 at 200), so
+// ten widths of the region's widest anti-diagonal, and at least the policy's warm-up.
+int32_t region_warm(const Region &rg, int32_t warm) { return std::max<int32_t>(warm, 10 * rg.max_width); }
+
+// Window indices (>= 1) whose T starts a new segment of region rg: k pieces of about equal sweep
+// time (L + warm each; the first piece owns L + warm anti-diagonals and needs no warm-up), each
+// cut at the first window start at or after its ideal place, none leaving less than L / 2 behind.
+void plan_cuts(const Region &rg, int64_t target, int32_t warm, std::vector<int32_t> &cuts) {
+    cuts.clear();
+    const int64_t n = rg.lX + rg.lY;
+    if (target <= (int64_t) warm + 64 || n <= target) return;
+    const int64_t k = (n - warm + (target - warm) - 1) / (target - warm);
+    if (k < 2) return;
+    const double L = (double) (n - warm) / (double) k;
+    size_t j = 1;
+    for (int64_t i = 1; i < k; ++i) {
+        const double want = (double) warm + (double) i * L;
+        while (j < rg.windows.size() && (double) rg.windows[j].T < want) ++j;
+        if (j >= rg.windows.size() || (double) (n - rg.windows[j].T) < L / 2) break;
+        cuts.push_back((int32_t) j);
+        ++j;
+    }
+}
+
 // one read's plan before packing
 struct ReadPlan {
     sa_status status = SA_OK;
@@ -308,12 +369,16 @@ struct ReadPlan {
     int64_t lX = 0;
     std::vector<int32_t> kid;   // k-mer id per column 1..lX
     std::vector<Region> regs;
+    std::vector<std::vector<int32_t>> cuts;   // per region: windows that start a forward segment
     int64_t diags = 0, cells = 0, windows = 0, chunks = 0, out = 0;
+    int64_t segs = 0, stitches = 0, stitch_floats = 0;
     int32_t max_width = 0;
     // packing offsets
     int64_t region_base = 0, diag_base = 0, cell_base = 0, win_base = 0, chunk_base = 0, kmer_base = 0,
-            event_base = 0, out_base = 0;
+            event_base = 0, out_base = 0, seg_base = 0, stitch_base = 0, stitch_voff = 0;
 };
+
+int32_t band_width(const Region &rg, int64_t d) { return (rg.xmy_r[d] - rg.xmy_l[d]) / 2 + 1; }
 
 // Host planning of a batch (no device work): per read its regions and their windows (in parallel
 // over reads), then the packed inputs, written straight into a host staging block (pinned when
@@ -398,17 +463,57 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
             rp.max_width = std::max(rp.max_width, rg.max_width);
         }
     });
+    // forward segments: the cap from the policy and the batch's forward anti-diagonals per worker CTA
+    {
+        int64_t fwd_diags = 0;
+        int32_t mw = 0;
+        for (int64_t r = 0; r < n_reads; ++r) {
+            fwd_diags += plan[r].diags;
+            mw = std::max(mw, plan[r].max_width);
+        }
+        const int32_t policy = g_seg_target.load(), warm = g_seg_warm.load();
+        int64_t target = policy;
+        if (policy == 0) {
+            const int cpt = std::max(1, (mw + kThreads - 1) / kThreads);
+            const int wc = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
+            int sms = 0;
+            if (device < 0 || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+                cudaGetLastError();
+                sms = 0;
+            }
+            if (sms <= 0) sms = 148;
+            const int64_t slots = (int64_t) sms * std::max(1, launch_for(std::max(device, 0), wc).ctas_per_sm);
+            target = std::max<int64_t>(kSegMin, 2 * fwd_diags / slots);
+        }
+        for (int64_t r = 0; r < n_reads; ++r) {
+            ReadPlan &rp = plan[r];
+            rp.cuts.assign(rp.regs.size(), {});
+            for (size_t gi = 0; gi < rp.regs.size(); ++gi) {
+                const Region &rg = rp.regs[gi];
+                if (policy >= 0) plan_cuts(rg, target, region_warm(rg, warm), rp.cuts[gi]);
+                rp.segs += 1 + (int64_t) rp.cuts[gi].size();
+                rp.stitches += (int64_t) rp.cuts[gi].size();
+                for (int32_t j : rp.cuts[gi]) {
+                    const int32_t bd = rg.windows[j].T;
+                    rp.stitch_floats += 6 * (int64_t) (band_width(rg, bd - 1) + band_width(rg, bd));
+                }
+            }
+        }
+    }
     // packing offsets
     int64_t nreg = 0, ndiag = 0, ncell = 0, nwin = 0, nchunk = 0, nkmer = 0, nevent = 0, nout = 0;
+    int64_t nseg = 0, nstitch = 0, nsfloat = 0;
     for (int64_t r = 0; r < n_reads; ++r) {
         ReadPlan &rp = plan[r];
         b->read_status[r] = rp.status;
         rp.region_base = nreg; rp.diag_base = ndiag; rp.cell_base = ncell; rp.win_base = nwin;
         rp.chunk_base = nchunk; rp.kmer_base = nkmer; rp.event_base = nevent; rp.out_base = nout;
+        rp.seg_base = nseg; rp.stitch_base = nstitch; rp.stitch_voff = nsfloat;
         b->read_first_region[r] = nreg;
         b->read_n_regions[r] = (int64_t) rp.regs.size();
         nreg += (int64_t) rp.regs.size(); ndiag += rp.diags; ncell += rp.cells; nwin += rp.windows;
         nchunk += rp.chunks; nout += rp.out;
+        nseg += rp.segs; nstitch += rp.stitches; nsfloat += rp.stitch_floats;
         if (!rp.status && !rp.plain) {
             nkmer += rp.lX;
             nevent += reads[r].n_events;
@@ -424,6 +529,7 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     if (b->max_width > kMaxCpt * kThreads) return SA_E_CAPACITY;
     b->device = device < 0 ? 0 : device;
     b->n_regions = nreg; b->n_diags = ndiag; b->n_windows = nwin; b->n_chunks = nchunk;
+    b->n_segs = nseg; b->n_stitch = nstitch; b->stitch_floats = nsfloat;
     b->n_kmers = nkmer; b->n_events = nevent;
     b->cells = ncell;
     b->out_total = nout;
@@ -434,10 +540,14 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
     for (int64_t r = 0; r < n_reads; ++r) {
         b->read_scale[r] = scale[r];
         b->read_scale64[r] = scale64[r];
-        b->read_win[4 * r] = plan[r].win_base;
-        b->read_win[4 * r + 1] = plan[r].windows;
-        b->read_win[4 * r + 2] = plan[r].region_base;
-        b->read_win[4 * r + 3] = (int64_t) plan[r].regs.size();
+        b->read_win[8 * r] = plan[r].win_base;
+        b->read_win[8 * r + 1] = plan[r].windows;
+        b->read_win[8 * r + 2] = plan[r].region_base;
+        b->read_win[8 * r + 3] = (int64_t) plan[r].regs.size();
+        b->read_win[8 * r + 4] = plan[r].stitch_base;
+        b->read_win[8 * r + 5] = plan[r].stitches;
+        b->read_win[8 * r + 6] = plan[r].windows + plan[r].stitches;
+        b->read_win[8 * r + 7] = 0;
     }
     // the packed inputs, read by read
     parallel_for(n_reads, threads, [&](int64_t r) {
@@ -453,7 +563,8 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
         for (int64_t y = 0; y < rd.n_events; ++y)
             b->events[rp.event_base + y] = make_double2(rd.events[y * kEventParams], rd.events[y * kEventParams + 1]);
         int64_t dbase = rp.diag_base, cbase = rp.cell_base, wbase = rp.win_base, chbase = rp.chunk_base,
-                obase = rp.out_base;
+                obase = rp.out_base, sgbase = rp.seg_base, stbase = rp.stitch_base, vbase = rp.stitch_voff;
+        const int32_t warm = g_seg_warm.load();
         std::vector<int32_t> flags;
         std::vector<int64_t> off;
         for (size_t gi = 0; gi < rp.regs.size(); ++gi) {
@@ -478,8 +589,11 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
             d.y1 = rg.y1;
             // per anti-diagonal meta: band start, width, window end / refresh / stored gap states
             flags.assign(d.n + 2, 0);
+            // a window is published once the forward sweep has passed the last anti-diagonal it
+            // reads (`from`), not its traceback anti-diagonal D: its backward sweep from D reads
+            // emissions only above `from`
             for (const Window &w : rg.windows) {
-                flags[w.D] |= kFlagWindowEnd;
+                flags[w.from] |= kFlagWindowEnd;
                 for (int32_t q = w.from; q > w.T; q -= 10) flags[q] |= kFlagRefresh;
             }
             off.resize(d.n + 1);
@@ -506,25 +620,186 @@ sa_status plan_batch(const sa_read *reads, int64_t n_reads, const sa_params *p, 
                 t.region = region;
                 t.first_cell = (int32_t) off[w.D];
                 t.out_cap = 4 * (w.from - w.T) + 64;
-                t.pad = 0;
+                t.side = -1;
                 t.out_base = obase;
                 obase += t.out_cap;
                 b->windows[wbase + (int64_t) wi] = w;
             }
+            // forward segments and the stitches between them
+            const std::vector<int32_t> &cuts = rp.cuts[gi];
+            for (size_t q = 0; q <= cuts.size(); ++q) {
+                Segment sg;
+                std::memset(&sg, 0, sizeof(sg));
+                sg.region = region;
+                sg.d_begin = q == 0 ? 0 : rg.windows[cuts[q - 1]].T;
+                sg.d_end = q == cuts.size() ? d.n : rg.windows[cuts[q]].T;
+                sg.stitch_in = q == 0 ? -1 : (int32_t) (stbase + (int64_t) q - 1);
+                sg.stitch_out = q == cuts.size() ? -1 : (int32_t) (stbase + (int64_t) q);
+                if (q == 0) {
+                    sg.warm = 0;
+                    sg.wi0 = 0;
+                    sg.cell0 = 1;   // anti-diagonal 0 has one cell
+                } else {
+                    // warm = 2 mod 3: d_begin closes a group of three steps of the sweep
+                    const int32_t wr = region_warm(rg, warm);
+                    sg.warm = wr + ((2 - wr) % 3 + 3) % 3;
+                    sg.wi0 = cuts[q - 1];
+                    sg.cell0 = off[sg.d_begin - sg.warm];
+                }
+                b->segs[sgbase + (int64_t) q] = sg;
+            }
+            for (size_t q = 0; q < cuts.size(); ++q) {
+                const int32_t bd = rg.windows[cuts[q]].T;
+                StitchDesc &sd = b->stitch[stbase + (int64_t) q];
+                sd.region = region;
+                sd.read = (int32_t) r;
+                sd.w0 = band_width(rg, bd - 1);
+                sd.w1 = band_width(rg, bd);
+                sd.voff = vbase;
+                vbase += 6 * (int64_t) (sd.w0 + sd.w1);
+                b->wtask[wbase + cuts[q]].side = (int32_t) (stbase + (int64_t) q);
+            }
+            sgbase += 1 + (int64_t) cuts.size();
+            stbase += (int64_t) cuts.size();
             b->regions[region] = d;
             dbase += d.n + 1;
             cbase += acc;
             wbase += (int64_t) rg.windows.size();
         }
     });
-    // largest band area first (LPT order of the forward claims)
-    std::vector<int32_t> order(nreg);
+    // longest sweep first (LPT order of the forward claims)
+    std::vector<int32_t> order(nseg);
     std::iota(order.begin(), order.end(), 0);
-    std::vector<int64_t> area(nreg);
-    for (int64_t i = 0; i < nreg; ++i)
-        area[i] = (i + 1 < nreg ? b->regions[i + 1].cell_base : b->cells) - b->regions[i].cell_base;
-    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) { return area[a] > area[c]; });
+    std::vector<int64_t> len(nseg);
+    for (int64_t i = 0; i < nseg; ++i) len[i] = (int64_t) b->segs[i].d_end - b->segs[i].d_begin + b->segs[i].warm;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) { return len[a] > len[c]; });
     std::copy(order.begin(), order.end(), b->order.data());
+    b->redone.assign(n_reads, 0);
+    b->n_redone = 0;
+    return SA_OK;
+}
+
+// kernel arguments of a batch's run (launch-dependent fields set by the caller)
+Args batch_args(const sa_batch *b) {
+    Args a;
+    std::memset(&a, 0, sizeof(a));
+    a.regions = b->d_regions;
+    a.n_regions = b->n_regions;
+    a.segs = b->d_segs;
+    a.order = b->d_order;
+    a.n_segs = b->n_segs;
+    a.stitch = b->d_stitch;
+    a.stitch_res = b->d_stitch_res;
+    a.stitch_vals = b->d_stitch_vals;
+    a.seg_fail = b->d_seg_fail;
+    a.stitch_tol = b->stitch_tol;
+    a.use_side = 1;
+    a.models = b->d_models;
+    a.read_scale = b->d_read_scale;
+    a.read_scale64 = b->d_read_scale64;
+    a.events_raw = b->d_events_raw;
+    a.meta = b->d_meta;
+    a.windows = b->d_windows;
+    a.wtask = b->d_wtask;
+    a.n_windows = b->n_windows;
+    a.chunks = b->d_chunks;
+    a.n_chunks = b->n_chunks;
+    a.kmer = b->d_kmer;
+    a.gapx = b->d_gapx;
+    a.events = b->d_events;
+    a.E = b->d_E;
+    a.F = b->d_F;
+    a.base = b->d_base;
+    a.fshift = b->d_fshift;
+    a.ready = b->d_ready;
+    a.out = b->d_out;
+    a.wcount = b->d_wcount;
+    a.loglik = b->d_loglik;
+    a.status = b->d_status;
+    a.ctl = b->d_ctl;
+    a.threshold = b->threshold;
+    a.n_reads = b->n_reads;
+    a.read_win = b->d_read_win;
+    a.packed = b->d_packed;
+    a.read_base = b->d_read_base;
+    a.read_count = b->d_read_count;
+    a.read_wdone = b->d_read_wdone;
+    a.done_host = b->d_done;
+    a.done_seq = b->run_seq;
+    const int cpt = std::max(1, (b->max_width + kThreads - 1) / kThreads);
+    a.wmax = (cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4)) * kThreads;
+    a.warp_windows = 1;
+    a.spin_limit = b->wait_limit;
+    return a;
+}
+
+// the persistent worker over a.n_segs forward segments and a.n_windows windows
+void launch_worker(const sa_batch *b, const Args &a, const sa_launch_config &cfg, int sms, cudaStream_t s) {
+    const int cls = a.wmax / kThreads;
+    const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) worker_area_floats(cls);
+    auto launch = [&](auto kern) {
+        int per_sm = 0;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+        per_sm = std::max(1, std::min(per_sm, cfg.ctas_per_sm));
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((int64_t) sms * per_sm,
+                                                                    (int64_t) cfg.grid_per_region * a.n_segs));
+        kern<<<(unsigned) grid, kThreads, smem, s>>>(a);
+    };
+    if (cls == 1) launch(worker_kernel<1>);
+    else if (cls == 2) launch(worker_kernel<2>);
+    else launch(worker_kernel<4>);
+}
+
+// Reads whose stitch disagreed run again with every region as one segment (after the batch's
+// results were downloaded): their windows are re-run and every read re-gathered.  The stitch
+// tolerance makes this rare; the redo keeps the result exact whatever the input.
+sa_status redo_disagreed(sa_batch *b, cudaStream_t s) {
+    std::vector<Segment> segs;
+    int64_t nwin = 0;
+    for (int64_t r = 0; r < b->n_reads; ++r) {
+        if (!b->seg_fail[r] || b->redone[r]) continue;
+        b->redone[r] = 1;
+        ++b->n_redone;
+        for (int64_t g = b->read_first_region[r]; g < b->read_first_region[r] + b->read_n_regions[r]; ++g) {
+            Segment sg;
+            std::memset(&sg, 0, sizeof(sg));
+            sg.region = (int32_t) g;
+            sg.d_end = b->regions[g].n;
+            sg.stitch_in = sg.stitch_out = -1;
+            sg.cell0 = 1;
+            segs.push_back(sg);
+            nwin += b->regions[g].n_windows;
+        }
+    }
+    if (segs.empty()) return SA_OK;
+    std::vector<int32_t> order(segs.size());
+    std::iota(order.begin(), order.end(), 0);
+    const size_t nw = (size_t) std::max<int64_t>(1, nwin);
+    if (cudaMemcpyAsync(b->d_redo_segs, segs.data(), sizeof(Segment) * segs.size(), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(b->d_redo_order, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaMemsetAsync(b->d_ctl, 0, sizeof(Control), s) != cudaSuccess ||
+        cudaMemsetAsync(b->d_ready, 0xff, sizeof(int32_t) * nw, s) != cudaSuccess)
+        return SA_E_CUDA;
+    Args a = batch_args(b);
+    a.segs = b->d_redo_segs;
+    a.order = b->d_redo_order;
+    a.n_segs = (int64_t) segs.size();
+    a.n_windows = nwin;
+    a.use_side = 0;          // T of every window comes from the unsegmented sweep's store
+    a.done_host = nullptr;   // every read is gathered below
+    const sa_launch_config cfg = b->has_cfg ? b->cfg : launch_for(b->device, a.wmax / kThreads);
+    a.warp_windows = cfg.warp_windows;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    sms = std::max(1, sms);
+    launch_worker(b, a, cfg, sms, s);
+    gather_pairs<<<(unsigned) std::max<int64_t>(1, std::min<int64_t>(b->n_reads, sms * 4)), 256, 0, s>>>(a);
+    count_launch(2);
+    // the pages the host reads in the pageable copies above stay alive until the stream drains
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return SA_E_CUDA;
     return SA_OK;
 }
 
@@ -621,52 +896,13 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
         cudaMemsetAsync(b->d_ready, 0xff, sizeof(int32_t) * std::max<size_t>(1, nw), s) != cudaSuccess)
         st = SA_E_CUDA;
     if (!st && nr > 0) {
-        Args a;
-        std::memset(&a, 0, sizeof(a));
-        a.regions = b->d_regions;
-        a.order = b->d_order;
-        a.n_regions = (int64_t) nr;
-        a.models = b->d_models;
-        a.read_scale = b->d_read_scale;
-        a.read_scale64 = b->d_read_scale64;
-        a.events_raw = b->d_events_raw;
-        a.meta = b->d_meta;
-        a.windows = b->d_windows;
-        a.wtask = b->d_wtask;
-        a.n_windows = (int64_t) nw;
-        a.chunks = b->d_chunks;
-        a.n_chunks = b->n_chunks;
-        a.kmer = b->d_kmer;
-        a.gapx = b->d_gapx;
-        a.events = b->d_events;
-        a.E = b->d_E;
-        a.F = b->d_F;
-        a.base = b->d_base;
-        a.fshift = b->d_fshift;
-        a.ready = b->d_ready;
-        a.out = b->d_out;
-        a.wcount = b->d_wcount;
-        a.loglik = b->d_loglik;
-        a.status = b->d_status;
-        a.ctl = b->d_ctl;
-        a.threshold = b->threshold;
-        a.n_reads = b->n_reads;
-        a.read_win = b->d_read_win;
-        a.packed = b->d_packed;
-        a.read_base = b->d_read_base;
-        a.read_count = b->d_read_count;
-        a.read_wdone = b->d_read_wdone;
-        a.done_host = b->d_done;
-        a.done_seq = b->run_seq;
+        Args a = batch_args(b);
         const int cpt = std::max(1, (b->max_width + kThreads - 1) / kThreads);
         const int cpt_pow2 = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
         b->width_class = cpt_pow2;
         const sa_launch_config cfg = b->has_cfg ? b->cfg : launch_for(b->device, cpt_pow2);
-        a.wmax = cpt_pow2 * kThreads;
         a.warp_windows = cfg.warp_windows;
-        a.spin_limit = b->wait_limit;
-        const size_t smem = sizeof(Shared) + sizeof(float) * (size_t) worker_area_floats(cpt_pow2);
-        int sms = 0, per_sm = 0;
+        int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
         sms = std::max(1, sms);
         b->timed = false;
@@ -678,16 +914,7 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
                                                                             (a.n_chunks + kEmitWarps - 1) / kEmitWarps)),
                           32 * kEmitWarps, 0, s>>>(a);
         if (timing) cudaEventRecord(b->ev[1], s);
-        auto launch = [&](auto kern) {
-            if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
-            per_sm = std::max(1, std::min(per_sm, cfg.ctas_per_sm));
-            const int64_t grid = std::min<int64_t>((int64_t) sms * per_sm, (int64_t) cfg.grid_per_region * (int64_t) nr);
-            kern<<<(unsigned) grid, kThreads, smem, s>>>(a);
-        };
-        if (cpt_pow2 == 1) launch(worker_kernel<1>);
-        else if (cpt_pow2 == 2) launch(worker_kernel<2>);
-        else launch(worker_kernel<4>);
+        launch_worker(b, a, cfg, sms, s);
         if (timing) cudaEventRecord(b->ev[2], s);
         // with per-read completion the worker has gathered every read it finished
         if (!b->d_done)
@@ -704,7 +931,6 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
     b->downloaded = false;
     return st;
 }
-
 sa_status sa_batch_download(sa_batch *b, void *stream) {
     if (!b) return SA_E_ARG;
     cudaStream_t s = (cudaStream_t) stream;
@@ -722,6 +948,16 @@ sa_status sa_batch_download(sa_batch *b, void *stream) {
                    cudaSuccess)
         st = SA_E_CUDA;
     if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = SA_E_CUDA;
+    // reads whose stitch disagreed: re-run unsegmented, then the results block again
+    bool redo = false;
+    for (int64_t r = 0; r < b->n_reads && !st && b->n_stitch > 0; ++r) redo = redo || (b->seg_fail[r] && !b->redone[r]);
+    if (redo && !st) {
+        st = redo_disagreed(b, s);
+        if (!st && cudaMemcpyAsync(b->host_res.ptr, b->dev_base + b->res_off, b->res_bytes, cudaMemcpyDeviceToHost,
+                                   s) != cudaSuccess)
+            st = SA_E_CUDA;
+        if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = SA_E_CUDA;
+    }
     const size_t npairs = st ? 0 : (size_t) b->ctl[0].packed;
     const size_t pair_bytes = std::max<size_t>(npairs, 1) * sizeof(sa_aligned_pair);
     if (!st && b->host_pairs.bytes < pair_bytes) {
@@ -742,6 +978,9 @@ sa_status sa_batch_download(sa_batch *b, void *stream) {
             continue;
         }
         for (int64_t i = 0; i < b->read_n_regions[r]; ++i) b->read_ll[r] += b->loglik[b->read_first_region[r] + i];
+        // each region's total is in its last segment's frame: the stitches' constants bring it back
+        if (!b->redone[r])
+            for (int64_t q = 0; q < b->read_win[8 * r + 5]; ++q) b->read_ll[r] += b->stitch_res[b->read_win[8 * r + 4] + q].delta;
     }
     cudaSetDevice(prev);
     b->downloaded = st == SA_OK;
@@ -848,6 +1087,40 @@ int64_t sa_batch_regions(const sa_batch *b) { return b ? (int64_t) b->regions.si
 sa_status sa_batch_set_wait_limit(sa_batch *b, int64_t cycles) {
     if (!b || cycles < 1) return SA_E_ARG;
     b->wait_limit = (long long) cycles;
+    return SA_OK;
+}
+
+sa_status sa_setSegmentPolicy(int32_t segment_diags, int32_t warmup_diags) {
+    if (warmup_diags < 64 || (segment_diags > 0 && segment_diags <= warmup_diags + 64)) return SA_E_ARG;
+    g_seg_target.store(segment_diags < 0 ? -1 : segment_diags);
+    g_seg_warm.store(warmup_diags);
+    return SA_OK;
+}
+
+sa_status sa_getSegmentPolicy(int32_t *segment_diags, int32_t *warmup_diags) {
+    if (!segment_diags || !warmup_diags) return SA_E_ARG;
+    *segment_diags = g_seg_target.load();
+    *warmup_diags = g_seg_warm.load();
+    return SA_OK;
+}
+
+sa_status sa_batch_segment_info(const sa_batch *b, int64_t *n_segments, int64_t *n_stitches, int64_t *n_redone,
+                                double *max_spread) {
+    if (!b || !n_segments || !n_stitches || !n_redone || !max_spread) return SA_E_ARG;
+    *n_segments = b->n_segs;
+    *n_stitches = b->n_stitch;
+    *n_redone = b->downloaded ? b->n_redone : 0;
+    double m = 0.0;
+    if (b->downloaded)
+        for (int64_t q = 0; q < b->n_stitch; ++q)
+            if (b->stitch_res[q].result == kStitchAgreed) m = std::max(m, (double) b->stitch_res[q].spread);
+    *max_spread = m;
+    return SA_OK;
+}
+
+sa_status sa_batch_set_stitch_tolerance(sa_batch *b, double scale) {
+    if (!b || !(scale == scale)) return SA_E_ARG;
+    b->stitch_tol = (float) scale;
     return SA_OK;
 }
 

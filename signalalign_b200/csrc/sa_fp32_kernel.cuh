@@ -4,13 +4,14 @@
 //      emission store.  Fully parallel (a warp per run of 32 anti-diagonals); it takes the
 //      Gaussian / HDP density work off the sequential sweeps.
 //   2. worker_kernel: persistent CTAs of 128 threads pull tasks from one device counter.  The first
-//      claims are the regions' forward sweeps (largest band first); every later claim is a slot of
-//      a ready queue of traceback windows.  A forward sweep runs the whole region anti-diagonal by
-//      anti-diagonal (cells spread over the threads, neighbours through a 3-slot shared-memory
-//      ring, one barrier per anti-diagonal), stores the forward match values (and, on the
-//      anti-diagonals a total-probability refresh reads, the gap states) to HBM, and publishes each
-//      traceback window of getPosteriorProbsWithBanding (pairwiseAligner.c:1319-1333) to the ready
-//      queue as soon as it has passed the window's traceback anti-diagonal.  A window task runs
+//      claims are forward segments (longest first); every later claim is a slot of a ready queue of
+//      traceback windows.  A forward segment sweeps a run of a region's anti-diagonals (the whole
+//      region, or a piece of a long one; see Segment) anti-diagonal by anti-diagonal (cells spread
+//      over the threads, neighbours through a 3-slot shared-memory ring, one barrier per
+//      anti-diagonal), stores the forward match values (and, on the anti-diagonals a
+//      total-probability refresh reads, the gap states) to HBM, and publishes each traceback window
+//      of getPosteriorProbsWithBanding (pairwiseAligner.c:1319-1333) to the ready queue as soon as it
+//      has passed the last anti-diagonal whose forward values the window reads.  A window task runs
 //      that window's backward sweep in its own ring with the posterior test and the reference's
 //      total-probability refreshes fused in, and writes its pairs to the window's output segment.
 //      Windows of one region are independent given the forward store, so the backward work of a
@@ -18,9 +19,10 @@
 //   3. gather_pairs: per read, the windows' segments concatenated in order (regions, then windows:
 //      the reference's emission order) into one packed buffer.
 //
-// A window slot is claimed only after every forward sweep has been claimed, and forward sweeps
-// never wait, so every wait on the ready queue ends once the forward sweeps progress; the wait is
-// bounded anyway (SA_E_TIMEOUT).
+// A window slot is claimed only after every forward segment has been claimed, and forward segments
+// never wait (a stitch is checked by whichever of its two segments finishes second), so every wait
+// on the ready queue ends once the forward sweeps progress; the wait is bounded anyway
+// (SA_E_TIMEOUT).
 //
 // The recursion is bound by instruction issue and latency, so the inner loops are branch-free: the
 // rings carry a -inf cell on each side and every slot beyond the anti-diagonal's width holds -inf,
@@ -104,9 +106,49 @@ struct WindowTask {
     int32_t region;
     int32_t first_cell;   // region-relative first cell of its traceback anti-diagonal D
     int32_t out_cap;      // pair slots of its output segment
-    int32_t pad;
+    int32_t side;         // T starts a forward segment: the stitch whose copy of T it reads, else -1
     int64_t out_base;     // first pair slot of its output segment
 };
+
+// One forward segment: a run of a region's anti-diagonals swept by one CTA.  A region's forward
+// sweep is cut at traceback-window starts into segments that run at the same time on different
+// CTAs.  Every segment after the first starts `warm` anti-diagonals before its first owned one
+// from a flat vector (every band cell 0 in every state).  The recursion commutes with adding a
+// constant to every value (logAdd(x + c, y + c) = logAdd(x, y) + c, pairwiseAligner.c:234-254), and
+// the influence of the start vector dies out: within a few hundred anti-diagonals the segment's
+// values are the true ones minus one constant, and the stitch where two segments meet checks that
+// on both anti-diagonals the recursion carries over (b-1 and b).  Posteriors are unaffected by the
+// constant: a window's total probability comes from its own forward values, so it cancels.
+struct Segment {
+    int32_t region;
+    int32_t d_begin;      // owned anti-diagonals: (d_begin, d_end]; the first segment also owns 0
+    int32_t d_end;
+    int32_t warm;         // anti-diagonals swept before d_begin (0 for a region's first segment)
+    int32_t wi0;          // region-relative index of the first window it publishes
+    int32_t stitch_in;    // stitch at d_begin (-1: first segment)
+    int32_t stitch_out;   // stitch at d_end (-1: last segment)
+    int32_t pad;
+    int64_t cell0;        // region-relative first cell of the first anti-diagonal it computes
+};
+
+// where two segments meet, at anti-diagonal b: values of b-1 and b from both sides
+struct StitchDesc {
+    int32_t region, read;
+    int32_t w0, w1;       // widths of b-1 and b
+    int64_t voff;         // first float of [later segment: b-1, b | earlier segment: b-1, b], M|X|Y each
+};
+
+// result of a stitch (cleared before every run)
+struct StitchRes {
+    double sbase[2];      // FP64 bases of b-1, b in the later segment's sweep
+    double tbase[2];      // and in the earlier segment's
+    double delta;         // earlier-segment value - later-segment value (the constant)
+    float spread;         // largest deviation from the constant, over the cells (diagnostic)
+    int32_t arrive;       // sides that have written their values
+    int32_t result;       // 0 pending, 1 agreed, 2 disagreed
+    int32_t pad;
+};
+constexpr int kStitchAgreed = 1, kStitchDisagreed = 2;
 
 // a run of up to kChunkDiags anti-diagonals of one region (emission kernel)
 struct Chunk {
@@ -139,8 +181,16 @@ __host__ __device__ constexpr int worker_area_floats(int cpt) {
 
 struct Args {
     const RegionDesc *regions;
-    const int32_t *order;           // forward claims: regions by band area, largest first
     int64_t n_regions;
+    const Segment *segs;
+    const int32_t *order;           // forward claims: segments by length, longest first
+    int64_t n_segs;
+    const StitchDesc *stitch;
+    StitchRes *stitch_res;
+    float *stitch_vals;
+    int32_t *seg_fail;              // per read: a stitch disagreed (the read is re-run unsegmented)
+    float stitch_tol;               // scale of the stitch tolerance (negative: every stitch disagrees)
+    int32_t use_side;               // windows at segment starts read the stitch copy of T
     const ModelDesc *models;
     const ReadScale32 *read_scale;
     const ReadScale64 *read_scale64;
@@ -170,7 +220,8 @@ struct Args {
     long long spin_limit;           // clock cycles a worker may wait for a window
     // gather
     int64_t n_reads;
-    const int64_t *read_win;        // per read: first window, window count, first region, region count
+    const int64_t *read_win;        // per read: first window, window count, first region, region
+                                    // count, first stitch, stitch count, units (windows + stitches), 0
     sa_aligned_pair *packed;
     int64_t *read_base;             // per read: first pair in the packed output
     int64_t *read_count;
@@ -188,6 +239,7 @@ struct Shared {
     int32_t task_id;
     int32_t done_read;
     long long red[kWarps + 1];
+    double cmp[3][kWarps];          // stitch check: per-warp largest value, its difference, spread
 };
 
 // The reference's lookup (pairwiseAligner.c:237-248) picks one of four cubics by d <= 1, <= 2.5,
@@ -596,17 +648,120 @@ __global__ void __launch_bounds__(32 * kEmitWarps) emission_kernel(const __grid_
 // (stateMachine3_loadTransitionsFromFile stores gap-Y -> gap-X in SWITCH_TO_Y, stateMachine.c:1139),
 // and logAdd(v, LOG_ZERO) is v exactly, so without it the gap-X state of the forward sweep and the
 // gap-Y state of the backward sweep take one logAdd less (the same values, bit for bit).
+template <int NT>
+__device__ void read_unit_done(const Args &A, int32_t r, int tid, Shared *sh);
+
+// Checks stitch si once both segments have written their values of b-1 and b (whole CTA).  With
+// a_i the earlier segment's FP64 value of a cell and s_i the later one's, the stitch agrees when
+// both have the same -inf cells and every a_i - s_i lies within 2e-5 + 1e-6 (a_max - a_i) of the
+// difference at the largest a_i (FP32 rounding of each sweep's values is a few ulp of their
+// magnitude below the anti-diagonal's maximum).  The difference at the largest value becomes the
+// stitch's constant; a disagreement marks the read for an unsegmented re-run.
+__device__ __forceinline__ void stitch_check(const Args &A, Shared *sh, int32_t si) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const StitchDesc sd = A.stitch[si];
+    StitchRes &res = A.stitch_res[si];
+    const double sb0 = __ldcg(&res.sbase[0]), sb1 = __ldcg(&res.sbase[1]);
+    const double tb0 = __ldcg(&res.tbase[0]), tb1 = __ldcg(&res.tbase[1]);
+    const int32_t nv = 3 * (sd.w0 + sd.w1);
+    const float *spec = A.stitch_vals + sd.voff, *tru = spec + nv;
+    // the largest earlier-segment value and the difference there
+    double amax = -INFINITY, dref = 0.0;
+    for (int q = tid; q < nv; q += kThreads) {
+        const bool j = q >= 3 * sd.w0;
+        const float tv = __ldcg(tru + q), sv = __ldcg(spec + q);
+        if (tv > kNegInf && sv > kNegInf) {
+            const double a = (double) tv + (j ? tb1 : tb0);
+            if (a > amax) {
+                amax = a;
+                dref = a - ((double) sv + (j ? sb1 : sb0));
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double a2 = __shfl_xor_sync(0xffffffffu, amax, o), d2 = __shfl_xor_sync(0xffffffffu, dref, o);
+        if (a2 > amax || (a2 == amax && d2 < dref)) {
+            amax = a2;
+            dref = d2;
+        }
+    }
+    if (lane == 0) {
+        sh->cmp[0][warp] = amax;
+        sh->cmp[1][warp] = dref;
+    }
+    __syncthreads();
+    amax = sh->cmp[0][0];
+    dref = sh->cmp[1][0];
+    for (int w = 1; w < kWarps; ++w) {
+        const double a2 = sh->cmp[0][w], d2 = sh->cmp[1][w];
+        if (a2 > amax || (a2 == amax && d2 < dref)) {
+            amax = a2;
+            dref = d2;
+        }
+    }
+    // every cell against it
+    const double scale = (double) A.stitch_tol;
+    bool ok = scale >= 0.0;
+    double spread = 0.0;
+    for (int q = tid; q < nv; q += kThreads) {
+        const bool j = q >= 3 * sd.w0;
+        const float tv = __ldcg(tru + q), sv = __ldcg(spec + q);
+        const bool ft = tv > kNegInf, fs = sv > kNegInf;
+        if (ft != fs) {
+            ok = false;
+        } else if (ft) {
+            const double a = (double) tv + (j ? tb1 : tb0);
+            const double dev = fabs((a - ((double) sv + (j ? sb1 : sb0))) - dref);
+            spread = fmax(spread, dev);
+            if (!(dev <= scale * (2e-5 + 1e-6 * (amax - a)))) ok = false;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) spread = fmax(spread, __shfl_xor_sync(0xffffffffu, spread, o));
+    __syncthreads();   // cmp[0..1] read by every thread
+    if (lane == 0) sh->cmp[2][warp] = spread;
+    ok = __syncthreads_and(ok);
+    if (tid == 0) {
+        for (int w = 1; w < kWarps; ++w) spread = fmax(spread, sh->cmp[2][w]);
+        res.delta = dref;
+        res.spread = (float) spread;
+        res.result = ok ? kStitchAgreed : kStitchDisagreed;
+        if (!ok) atomicExch(A.seg_fail + sd.read, 1);
+        __threadfence();
+    }
+    __syncthreads();
+    read_unit_done<kThreads>(A, sd.read, tid, sh);
+}
+
+// One side of stitch si has written its values (whole CTA, after its sweep): the side that arrives
+// second checks the stitch.
+__device__ __forceinline__ void stitch_arrive(const Args &A, Shared *sh, int32_t si) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        sh->done_read = atomicAdd(&A.stitch_res[si].arrive, 1);
+        __threadfence();
+    }
+    __syncthreads();
+    const bool second = sh->done_read == 1;
+    __syncthreads();
+    if (second) stitch_check(A, sh, si);
+}
+
 template <int CPT, bool kSX>
 struct ForwardSweep {
     const Ctx &c;
     const Args &A;
     const RegionDesc &R;
+    const Segment &S;
     Shared *sh;
-    float *ring;                  // 3 slots x 3 states x (wmax + 2); slot of d is (d - 1) mod 3
+    float *ring;                  // 3 slots x 3 states x (wmax + 2); slot of d is (d - s) mod 3
     const float4 *tab;
     int tid, lane, warp, wmax, stride;
     int64_t db;
     int32_t n;
+    int32_t dbeg, dend;           // owned anti-diagonals (dbeg, dend] (0 is owned by a first segment)
     float *Fd;                    // forward store of the anti-diagonal being computed
     const float *Ereg;
     // band facts: metas of d-2, d-1, d (m2, m1, m0); by phase, decoded metas of d+1 .. d+3 and
@@ -625,8 +780,8 @@ struct ForwardSweep {
     float qshift;                 // with d mod 32 == q
     int32_t wi;
 
-    __device__ __forceinline__ ForwardSweep(const Ctx &cc, Shared *s, float *r)
-        : c(cc), A(*cc.A), R(cc.R), sh(s), ring(r) {}
+    __device__ __forceinline__ ForwardSweep(const Ctx &cc, const Segment &sg, Shared *s, float *r)
+        : c(cc), A(*cc.A), R(cc.R), S(sg), sh(s), ring(r) {}
 
     __device__ __forceinline__ float *slot(int k, int state) const { return ring + (k * 3 + state) * stride + 1; }
 
@@ -694,6 +849,7 @@ struct ForwardSweep {
         // the recursion on d (stateMachine3_cellCalculate order: lower -> gap-X, middle -> match,
         // upper -> gap-Y, each state accumulated from LOG_ZERO)
         const float shL = -delta0, shM = -delta1 - delta0;
+        const bool own = d > dbeg;   // warm-up anti-diagonals of a later segment store nothing
         const bool store_gaps = (m0.flags & kFlagStoreGaps) != 0;
         float lm = kNegInf;
 #pragma unroll
@@ -712,7 +868,7 @@ struct ForwardSweep {
             slot(S0, 0)[i] = vM;
             slot(S0, 1)[i] = vX;
             slot(S0, 2)[i] = vY;
-            if (in) {
+            if (in && own) {
                 Fd[ST_M * W0 + i] = vM;
                 if (store_gaps) {
                     Fd[ST_X * W0 + i] = vX;
@@ -727,15 +883,16 @@ struct ForwardSweep {
             if (lane == 0) sh->part[S1][warp] = wm;
         }
         // base and shift of d: lane d mod 32 of warp 0 keeps them, and the warp writes them out 32
-        // at a time and before a window is published (its backward sweep reads them)
-        const bool window_end = (m0.flags & kFlagWindowEnd) != 0;
+        // at a time and before a window is published (its backward sweep reads them); only the
+        // segment's own anti-diagonals
+        const bool window_end = own && (m0.flags & kFlagWindowEnd) != 0;
         if (warp == 0) {
             const int q = d & 31;
             if (lane == q) {
                 qbase = base0;
                 qshift = delta0;
             }
-            if ((q == 31 || window_end || d == n) && lane <= q) {
+            if ((q == 31 || window_end || d == dend) && lane <= q && d - q + lane > dbeg) {
                 A.base[db + (d - q) + lane] = qbase;
                 A.fshift[db + (d - q) + lane] = qshift;
             }
@@ -744,7 +901,7 @@ struct ForwardSweep {
         __syncthreads();
         if (window_end && tid == 0) {
             const unsigned q = atomicAdd(&A.ctl->pub, 1u);
-            atomicExch(A.ready + q, (int32_t) (R.win_base + wi));
+            if ((int64_t) q < A.n_windows) atomicExch(A.ready + q, (int32_t) (R.win_base + wi));
             ++wi;
         }
         lm_prev = lm;
@@ -757,6 +914,35 @@ struct ForwardSweep {
         m0 = near[(P + 1) % 3];   // meta of d+1, decoded two steps ago
     }
 
+    // After the step of anti-diagonal b (the ring holds b-2, b-1, b): the values of b-1 and b go to
+    // stitch si with their FP64 bases, as its later side (this segment starts at b) or its earlier
+    // side (this segment ends at b).  base0 and delta0 / delta1 already describe b+1.
+    __device__ void stitch_capture(int32_t si, bool later, int32_t b, int32_t s) {
+        const StitchDesc sd = A.stitch[si];
+        float *v = A.stitch_vals + sd.voff + (later ? 0 : 3 * (sd.w0 + sd.w1));
+        const double base_b = base0 - (double) delta0, base_b1 = base_b - (double) delta1;
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+            const int k = ((b - 1 + part - s) % 3 + 3) % 3;   // ring slot of anti-diagonal x: (x - s) mod 3
+            const int32_t W = part ? sd.w1 : sd.w0;
+            float *o = v + (part ? 3 * sd.w0 : 0);
+            for (int i = tid; i < W; i += kThreads) {
+                o[i] = slot(k, 0)[i];
+                o[W + i] = slot(k, 1)[i];
+                o[2 * W + i] = slot(k, 2)[i];
+            }
+        }
+        if (tid == 0) {
+            double *bs = later ? A.stitch_res[si].sbase : A.stitch_res[si].tbase;
+            bs[0] = base_b1;
+            bs[1] = base_b;
+        }
+    }
+
+    // The sweep starts at anti-diagonal s = d_begin - warm (1 for a region's first segment); the
+    // phase of anti-diagonal d (its ring slot and look-ahead registers) is (d - s) mod 3.  A later
+    // segment's warm is 2 mod 3 (the planner picks it so): d_begin is the last step of a group of
+    // three, so the stepping loop can stop there, with d_begin - 1 and d_begin in the ring.
     __device__ void run() {
         tab = sh->la;
         tid = threadIdx.x;
@@ -766,42 +952,60 @@ struct ForwardSweep {
         stride = wmax + 2;
         db = R.diag_base;
         n = R.n;
-        Fd = A.F + 3 * R.cell_base;
+        dbeg = S.d_begin;
+        dend = S.d_end;
+        const int32_t s = dbeg - S.warm + (dbeg == 0 ? 1 : 0);
+        Fd = A.F + 3 * (R.cell_base + S.cell0);
         Ereg = A.E + 2 * R.cell_base;
         ring_init(ring, wmax);
         __syncthreads();
-        // anti-diagonal 0 (slot 2): startStateProb / raggedStartStateProb (stateMachine.c:1022-1032)
-        const float s0 = R.ragged_left ? kNegInf : 0.0f, s1 = R.ragged_left ? 0.0f : kNegInf;
-        if (tid == 0) {
-            Fd[ST_M] = s0; Fd[ST_X] = s1; Fd[ST_Y] = s1;
-            slot(2, 0)[0] = s0;
-            slot(2, 1)[0] = s1;
-            slot(2, 2)[0] = s1;
-            A.base[db] = 0.0;
-            A.fshift[db] = 0.0f;
+        if (dbeg == 0) {
+            // anti-diagonal 0 (slot 2): startStateProb / raggedStartStateProb (stateMachine.c:1022-1032)
+            const float s0 = R.ragged_left ? kNegInf : 0.0f, s1 = R.ragged_left ? 0.0f : kNegInf;
+            if (tid == 0) {
+                float *F0 = A.F + 3 * R.cell_base;   // anti-diagonal 0 has one cell
+                F0[ST_M] = s0; F0[ST_X] = s1; F0[ST_Y] = s1;
+                slot(2, 0)[0] = s0;
+                slot(2, 1)[0] = s1;
+                slot(2, 2)[0] = s1;
+                A.base[db] = 0.0;
+                A.fshift[db] = 0.0f;
+            }
+            m2 = Meta{0, 0, 0};
+            m1 = decode_meta(raw_meta(A, db, 0, n), true);
+            lm_prev = tid == 0 ? fmaxf(s0, s1) : kNegInf;
+        } else {
+            // a later segment: every band cell of s-2 (slot 1) and s-1 (slot 2) starts at 0
+            m2 = decode_meta(raw_meta(A, db, s - 2, n), true);
+            m1 = decode_meta(raw_meta(A, db, s - 1, n), true);
+            for (int i = tid; i < wmax; i += kThreads) {
+#pragma unroll
+                for (int st = 0; st < 3; ++st) {
+                    if (i < m2.W) slot(1, st)[i] = 0.0f;
+                    if (i < m1.W) slot(2, st)[i] = 0.0f;
+                }
+            }
+            if (tid < kWarps) sh->part[1][tid] = 0.0f;   // maximum of s-2
+            lm_prev = 0.0f;                               // maximum of s-1
         }
-        Fd += 3;   // anti-diagonal 0 has one cell
-        m2 = Meta{0, 0, 0};
-        m1 = decode_meta(raw_meta(A, db, 0, n), true);
-        m0 = decode_meta(raw_meta(A, db, 1, n), 1 <= n);
-        const Meta ma = decode_meta(raw_meta(A, db, 2, n), 2 <= n);
-        const Meta mb = decode_meta(raw_meta(A, db, 3, n), 3 <= n);
-        // look-ahead of d = 1, 2, 3 (phases 0, 1, 2); metas of d = 2, 3 decoded, 4, 5, 6 raw
-        int32_t off = 1;
-        prefetch<0>(1, m0, off);
+        // look-ahead: metas of s, s+1, s+2 decoded, s+3 .. s+5 raw; emissions of s .. s+2 requested
+        int32_t off = (int32_t) S.cell0;
+        m0 = decode_meta(raw_meta(A, db, s, n), s <= n);
+        const Meta ma = decode_meta(raw_meta(A, db, s + 1, n), s + 1 <= n);
+        const Meta mb = decode_meta(raw_meta(A, db, s + 2, n), s + 2 <= n);
+        prefetch<0>(s, m0, off);
         off += m0.W;
-        prefetch<1>(2, ma, off);
+        prefetch<1>(s + 1, ma, off);
         off += ma.W;
-        prefetch<2>(3, mb, off);
+        prefetch<2>(s + 2, mb, off);
         off += mb.W;
-        eoff3 = off;   // first cell of d = 4
+        eoff3 = off;   // first cell of s + 3
         near[0] = Meta{0, 0, 0};
         near[1] = ma;
         near[2] = mb;
-        raw[0] = raw_meta(A, db, 4, n);
-        raw[1] = raw_meta(A, db, 5, n);
-        raw[2] = raw_meta(A, db, 6, n);
-        lm_prev = tid == 0 ? fmaxf(s0, s1) : kNegInf;
+        raw[0] = raw_meta(A, db, s + 3, n);
+        raw[1] = raw_meta(A, db, s + 4, n);
+        raw[2] = raw_meta(A, db, s + 5, n);
         // Renormalisation: base(d + 1) = base(d - 2) + max(d - 2), known one step ahead, so neither
         // the reduction nor the shared-memory read of the warps' maxima sits on the recursion's
         // path.  delta(d) = base(d) - base(d-1) is a float and base(d) = base(d-1) + delta(d).
@@ -809,25 +1013,35 @@ struct ForwardSweep {
         base0 = 0.0;
         qbase = 0.0;   // anti-diagonal 0 (lane 0 of the first block): base 0, shift 0
         qshift = 0.0f;
-        wi = 0;
+        wi = S.wi0;
         __syncthreads();
-        for (int32_t d = 1; d <= n; d += 3) {
-            step<0>(d);
-            if (d + 1 > n) break;
-            step<1>(d + 1);
-            if (d + 2 > n) break;
-            step<2>(d + 2);
+        // the stepping loop stops once at d_begin when the segment starts at a stitch
+        int32_t d = s, stop = S.stitch_in >= 0 ? dbeg : dend;
+        for (;;) {
+            for (; d <= stop; d += 3) {
+                step<0>(d);
+                if (d + 1 > stop) break;
+                step<1>(d + 1);
+                if (d + 2 > stop) break;
+                step<2>(d + 2);
+            }
+            if (stop == dend) break;
+            stitch_capture(S.stitch_in, true, dbeg, s);   // whole groups ran: d == d_begin + 1
+            stop = dend;
         }
+        if (S.stitch_out >= 0) stitch_capture(S.stitch_out, false, dend, s);
+        if (S.stitch_in >= 0) stitch_arrive(A, sh, S.stitch_in);
+        if (S.stitch_out >= 0) stitch_arrive(A, sh, S.stitch_out);
     }
 };
 
 template <int CPT>
-__device__ void forward_task(const Ctx &c, Shared *sh, float *ring) {
+__device__ void forward_task(const Ctx &c, const Segment &sg, Shared *sh, float *ring) {
     if (c.t[T_SX] > kNegInf) {
-        ForwardSweep<CPT, true> f(c, sh, ring);
+        ForwardSweep<CPT, true> f(c, sg, sh, ring);
         f.run();
     } else {
-        ForwardSweep<CPT, false> f(c, sh, ring);
+        ForwardSweep<CPT, false> f(c, sg, sh, ring);
         f.run();
     }
 }
@@ -884,6 +1098,10 @@ __device__ void window_task(const Ctx &c, Shared *sh, float *ring, float *chain,
     const float *Ereg = A.E + 2 * R.cell_base;
     const Window W = A.windows[gw];
     const WindowTask wt = A.wtask[gw];
+    // a window whose T starts a forward segment reads that segment's own copy of T, kept by the
+    // stitch: the store holds the earlier segment's, whose values differ by the stitch's constant
+    const float *Tside = A.use_side && wt.side >= 0 ? A.stitch_vals + A.stitch[wt.side].voff + 3 * A.stitch[wt.side].w0
+                                                    : nullptr;
     int64_t n_out = 0;
     double ll = 0.0;
     ring_init(ring, wmax);
@@ -993,7 +1211,7 @@ __device__ void window_task(const Ctx &c, Shared *sh, float *ring, float *chain,
             if (refresh_m) {
                 // gap states of d-1; match-through inputs of a refresh at d-1: match emissions of
                 // the d cells and forward values of d-2
-                const float *Fmm = Freg + 3 * (Wmm > 0 ? offmm : offm);
+                const float *Fmm = Tside && d - 2 == T ? Tside : Freg + 3 * (Wmm > 0 ? offmm : offm);
                 const int32_t Wml = Wmm > 0 ? Wmm : Wm;
 #pragma unroll
                 for (int j = 0; j < CPT; ++j) {
@@ -1159,6 +1377,7 @@ struct WarpWindow {
     int64_t db;
     int32_t n, D, T, from;
     const float *Freg, *Ereg;
+    const float *Tside;           // the forward segment's own copy of T (see window_task), or null
     float *s0, *s1, *s2;          // ring slots of d, d+1, d+2
     Meta mpp, mp, m0, mm;         // band facts of d+2, d+1, d, d-1
     int2 raw_mmm;                 // raw band facts of d-2
@@ -1208,8 +1427,9 @@ struct WarpWindow {
     };
 
     __device__ __forceinline__ void load_refresh(RefreshOps &o, const Meta &m, int32_t off, const Meta &m1, int32_t off1,
-                                                 const Meta &m_1, int32_t off_1) const {
-        const float *Fd = Freg + 3 * off, *Fm = Freg + 3 * off_1, *E1 = Ereg + 2 * off1;
+                                                 const Meta &m_1, int32_t off_1, int32_t d_1) const {
+        const float *Fd = Freg + 3 * off, *E1 = Ereg + 2 * off1;
+        const float *Fm = Tside && d_1 == T ? Tside : Freg + 3 * off_1;
 #pragma unroll
         for (int j = 0; j < WCPT; ++j) {
             const int i = lane + 32 * j;
@@ -1259,7 +1479,7 @@ struct WarpWindow {
         prefetch<1 - K>(d - 1, mm, offm, m0, off0, mp, offp);
         const bool refresh_next = d - 1 > T && d - 1 <= from && (mm.flags & kFlagRefresh) != 0;
         RefreshOps rops;
-        if (refresh_next) load_refresh(rops, mm, offm, m0, off0, mmm, offm - mmm.W);
+        if (refresh_next) load_refresh(rops, mm, offm, m0, off0, mmm, offm - mmm.W, d - 2);
         // the recursion on d (D itself holds the end-state values); B of the cells kept in registers
         float lm = kNegInf;
         float bM[WCPT], bX[WCPT], bY[WCPT];
@@ -1426,6 +1646,7 @@ struct WarpWindow {
         D = Wn.D;
         T = Wn.T;
         from = Wn.from;
+        Tside = A.use_side && wt.side >= 0 ? A.stitch_vals + A.stitch[wt.side].voff + 3 * A.stitch[wt.side].w0 : nullptr;
         for (int i = lane; i < 9 * stride; i += 32) ring[i] = kNegInf;
         s0 = ring + 1;
         s1 = ring + 3 * stride + 1;
@@ -1456,7 +1677,7 @@ struct WarpWindow {
         prefetch<0>(D, m0, off0, mp, offp, mpp, offp);
         if (D <= from && (m0.flags & kFlagRefresh) != 0) {
             RefreshOps o;
-            load_refresh(o, m0, off0, mp, offp, mm, off0 - mm.W);
+            load_refresh(o, m0, off0, mp, offp, mm, off0 - mm.W, D - 1);
             store_refresh(o);
         }
         mx_last = kNegInf;
@@ -1522,7 +1743,7 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
 // written by other CTAs, so they are read through L2.
 template <int NT>
 __device__ void gather_read(const Args &A, int64_t r, int tid, long long *red, long long &base, long long &tot) {
-    const int64_t w0 = A.read_win[4 * r], nw = A.read_win[4 * r + 1];
+    const int64_t w0 = A.read_win[8 * r], nw = A.read_win[8 * r + 1];
     long long mine = 0;
     for (int64_t k = tid; k < nw; k += NT)
         mine += min(__ldcg(A.wcount + w0 + k), (int64_t) A.wtask[w0 + k].out_cap);
@@ -1573,20 +1794,22 @@ __device__ void gather_read(const Args &A, int64_t r, int tid, long long *red, l
     }
 }
 
-// After a group of NT threads (tid 0..NT-1) finished traceback window `window`, with batches that
-// publish reads as they finish: the window is counted against its read, and the group that
-// finishes the read's last window gathers the read and writes its record to mapped host memory,
-// `done` last after a system-scope fence (the host then copies the pairs while the kernel runs on).
+// After a group of NT threads (tid 0..NT-1) finished a unit of read r (a traceback window, or the
+// check of a stitch between two forward segments), with batches that publish reads as they finish:
+// the unit is counted against its read, and the group that finishes the read's last unit gathers
+// the read and writes its record to mapped host memory, `done` last after a system-scope fence (the
+// host then copies the pairs while the kernel runs on).  A read with a disagreeing stitch gets no
+// record: the host re-runs it unsegmented and its result comes from the download.
 template <int NT>
-__device__ void window_done(const Args &A, int64_t window, int tid, Shared *sh) {
+__device__ void read_unit_done(const Args &A, int32_t r, int tid, Shared *sh) {
     if (!A.done_host) return;
     __threadfence();   // this thread's pairs, count and total before the count below
     group_sync<NT>();
     int32_t last = -1;
     if (tid == 0) {
-        const int32_t r = A.regions[A.wtask[window].region].read;
-        if (atomicAdd(A.read_wdone + r, 1) + 1 == (int32_t) A.read_win[4 * r + 1]) last = r;
+        if (atomicAdd(A.read_wdone + r, 1) + 1 == (int32_t) A.read_win[8 * r + 6]) last = r;
         __threadfence();
+        if (last >= 0 && __ldcg(A.seg_fail + r)) last = -1;
     }
     if (NT == 32) {
         last = __shfl_sync(0xffffffffu, last, 0);
@@ -1603,9 +1826,12 @@ __device__ void window_done(const Args &A, int64_t window, int tid, Shared *sh) 
     __threadfence_system();   // this thread's packed pairs before the record
     group_sync<NT>();
     if (tid == 0) {
-        const int64_t g0 = A.read_win[4 * last + 2], ng = A.read_win[4 * last + 3];
+        const int64_t g0 = A.read_win[8 * last + 2], ng = A.read_win[8 * last + 3];
+        const int64_t s0 = A.read_win[8 * last + 4], ns = A.read_win[8 * last + 5];
         double ll = 0.0;
         for (int64_t g = 0; g < ng; ++g) ll += __ldcg(A.loglik + g0 + g);
+        // each region's last window is in its last segment's frame: add the stitches' constants
+        for (int64_t q = 0; q < ns; ++q) ll += __ldcg(&A.stitch_res[s0 + q].delta);
         ReadDone *rec = A.done_host + last;
         rec->first_pair = base;
         rec->n_pairs = tot;
@@ -1627,18 +1853,19 @@ __global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(cons
     float *area = reinterpret_cast<float *>(sh + 1);
     const int tid = threadIdx.x;
     if (tid < 16) log_add_piece(tid, sh->la[tid]);
-    // forward sweeps
+    // forward segments
     for (;;) {
         if (tid == 0) {
             const unsigned claim = atomicAdd(&A.ctl->claim, 1u);
-            sh->task_id = claim < (unsigned) A.n_regions ? A.order[claim] : -1;
+            sh->task_id = claim < (unsigned) A.n_segs ? A.order[claim] : -1;
         }
         __syncthreads();
         const int32_t id = sh->task_id;
         if (id < 0) break;
+        const Segment sg = A.segs[id];
         Ctx c;
-        ctx_init(c, A, id);
-        forward_task<CPT>(c, sh, area);
+        ctx_init(c, A, sg.region);
+        forward_task<CPT>(c, sg, sh, area);
         __syncthreads();
     }
     // traceback windows, in publication order: one per warp for bands up to 128 cells (when the
@@ -1664,7 +1891,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(cons
                 WarpWindow<kWarpWindowCpt, false> w(c, wring, wchain, sh->la);
                 w.run(id);
             }
-            window_done<32>(A, id, lane, sh);
+            read_unit_done<32>(A, c.R.read, lane, sh);
         }
     } else {
         float *ring = area, *chain = area + 9 * (A.wmax + 2);
@@ -1681,7 +1908,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(cons
             if (c.t[T_SX] > kNegInf) window_task<CPT, true>(c, sh, ring, chain, id);
             else window_task<CPT, false>(c, sh, ring, chain, id);
             __syncthreads();
-            window_done<kThreads>(A, id, tid, sh);
+            read_unit_done<kThreads>(A, c.R.read, tid, sh);
         }
     }
 }

@@ -1,0 +1,125 @@
+"""Forward segments of the batched FP32 form (sa_setSegmentPolicy).
+
+A region's forward sweep is cut at traceback-window starts into segments swept at the same time;
+each later segment warms up from a flat start and is checked where it meets the previous one (the
+stitch).  What is checked here:
+
+* segmented and unsegmented runs of the same reads give the same posteriors (within 1e-5: the two
+  sweeps round differently) and the same log-likelihood (1e-7 relative), and both the oracle's
+  within the FP32 form's 1e-4;
+* every stitch agrees on these inputs, with its largest deviation far below the tolerance;
+* a batch whose stitches are all made to disagree (negative tolerance scale) re-runs every
+  segmented read unsegmented at download and returns exactly the unsegmented run's results;
+* per-read completion (the serving path) counts the stitches of a read before publishing it.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from signalalign_b200 import synth
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from signalalign_b200 import api as a
+    return a
+
+
+@pytest.fixture
+def policy(api):
+    saved = api.get_segment_policy()
+    yield
+    api.set_segment_policy(*saved)
+
+
+def _case(api, seed=61, n_reads=4, span=(4000, 9000)):
+    cfg = synth.config1(seed=seed, n_reads=n_reads, span=span)
+    m = W.gaussian_model(cfg)
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED)
+    inputs = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                            scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
+    return cfg, m, sm, inputs
+
+
+def _run(api, inputs, p, segment_diags, tol_scale=None):
+    api.set_segment_policy(segment_diags, 1024)
+    b = api.Batch(inputs, p)
+    b.upload()
+    if tol_scale is not None:
+        b.set_stitch_tolerance(tol_scale)
+    b.run()
+    b.download()
+    return b
+
+
+def test_segmented_equals_unsegmented_and_oracle(api, policy):
+    cfg, m, sm, inputs = _case(api)
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    seg = _run(api, inputs, p, 4096)
+    whole = _run(api, inputs, p, -1)
+    info = seg.segment_info()
+    assert info["segments"] > 2 * len(inputs), info
+    assert info["stitches"] == info["segments"] - len(inputs)
+    assert info["redone"] == 0, info
+    assert info["max_spread"] < 2e-5, info
+    assert whole.segment_info()["segments"] == len(inputs)
+    op = orc.params(threshold=p.threshold, expansion=p.diagonal_expansion)
+    for i, rd in enumerate(cfg["reads"]):
+        assert seg.status(i) == 0 and whole.status(i) == 0
+        assert W.max_posterior_error(whole.pairs(i), seg.pairs(i), p.threshold) <= 1e-5
+        assert abs(seg.log_likelihood(i) - whole.log_likelihood(i)) <= 1e-7 * abs(whole.log_likelihood(i))
+        om = W.oracle_model(m, orc.EMIT_DESCALED, rd)
+        want = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], op, True, True)
+        assert W.max_posterior_error(want, seg.pairs(i), p.threshold) <= FP32_TOL
+
+
+def test_disagreeing_stitches_rerun_unsegmented(api, policy):
+    cfg, m, sm, inputs = _case(api, seed=62, n_reads=3, span=(3000, 7000))
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    whole = _run(api, inputs, p, -1)
+    forced = _run(api, inputs, p, 4096, tol_scale=-1.0)
+    info = forced.segment_info()
+    assert info["stitches"] > 0
+    assert info["redone"] == len(inputs), info   # every read here has a stitch
+    for i in range(len(inputs)):
+        assert forced.status(i) == 0
+        assert np.array_equal(forced.pairs(i), whole.pairs(i))
+        assert forced.log_likelihood(i) == whole.log_likelihood(i)
+    # the same batch run again with the default tolerance: no re-run, results within rounding
+    forced.set_stitch_tolerance(1.0)
+    forced.run()
+    forced.download()
+    for i in range(len(inputs)):
+        assert W.max_posterior_error(whole.pairs(i), forced.pairs(i), p.threshold) <= 1e-5
+
+
+def test_served_reads_count_their_stitches(api, policy):
+    """the serving path publishes a segmented read only after its stitches were checked, with the
+    log-likelihood brought back to the first segment's frame"""
+    cfg, m, sm, inputs = _case(api, seed=63, n_reads=3, span=(5000, 8000))
+    p = api.pairwiseAlignmentBandingParameters_construct()
+    api.set_segment_policy(4096, 1024)
+    srv = api.Server(max_inflight_cells=500_000_000, max_batches=2)
+    try:
+        tickets = [srv.submit(r, p) for r in inputs]
+        for tk in tickets:
+            srv.wait(tk)
+        res = [srv.result(tk) for tk in tickets]
+        stats = srv.stats()
+    finally:
+        srv.close()
+    assert stats["reads_early"] == len(inputs)
+    whole = _run(api, inputs, p, -1)
+    for i in range(len(inputs)):
+        st, pairs, ll, _ = res[i]
+        assert st == 0
+        assert W.max_posterior_error(whole.pairs(i), pairs, p.threshold) <= 1e-5
+        assert abs(ll - whole.log_likelihood(i)) <= 1e-7 * abs(whole.log_likelihood(i))

@@ -119,6 +119,10 @@ def test_micro_batches_overlap_on_the_device(api):
     sm = W.gpu_model(api, W.gaussian_model(cfg), orc.EMIT_DESCALED)
     reads = _inputs(api, sm, cfg["reads"])
     p = api.pairwiseAlignmentBandingParameters_construct()
+    # whole (unsegmented) forward sweeps, so the first micro-batch is still running when the second
+    # is admitted
+    saved = api.get_segment_policy()
+    api.set_segment_policy(-1, saved[1])
     srv = api.Server(max_inflight_cells=1_000_000_000, max_batches=2)
     try:
         t0 = srv.submit(reads[0], p)
@@ -130,6 +134,7 @@ def test_micro_batches_overlap_on_the_device(api):
         log = srv.batch_log()
     finally:
         srv.close()
+        api.set_segment_policy(*saved)
     assert len(log) == 2 and all(b[2] == 1 for b in log), log
     (s0, e0, _), (s1, e1, _) = sorted(log)
     assert 0 <= s0 < e0 and 0 <= s1 < e1
