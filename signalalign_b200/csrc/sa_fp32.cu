@@ -746,9 +746,10 @@ void launch_worker(const sa_batch *b, const Args &a, const sa_launch_config &cfg
                                                                     (int64_t) cfg.grid_per_region * a.n_segs));
         kern<<<(unsigned) grid, kThreads, smem, s>>>(a);
     };
-    if (cls == 1) launch(worker_kernel<1>);
-    else if (cls == 2) launch(worker_kernel<2>);
-    else launch(worker_kernel<4>);
+    if (cls == 1 && cfg.ctas_per_sm >= 3) launch(worker_kernel<1, 3>);
+    else if (cls == 1) launch(worker_kernel<1, 2>);
+    else if (cls == 2) launch(worker_kernel<2, 1>);
+    else launch(worker_kernel<4, 1>);
 }
 
 // Reads whose stitch disagreed run again with every region as one segment (after the batch's
@@ -1177,11 +1178,11 @@ sa_status sa_tuneLaunchConfig(sa_batch *b, void *stream, int32_t repeats, sa_lau
     const int cpt = std::max(1, (b->max_width + kThreads - 1) / kThreads);
     const int wc = cpt <= 1 ? 1 : (cpt <= 2 ? 2 : 4);
     std::vector<sa_launch_config> cand;
-    for (int cps : {1, 2})
+    for (int cps : {1, 2, 3})
         for (int gpr : {2, 3, 4, 6})
             for (int ww : {1, 0})
                 for (int ecs : {8, 16, 32}) {
-                    if (wc != 1 && (ww == 0 || cps == 2)) continue;   // wider bands: CTA windows, one CTA per SM
+                    if (wc != 1 && (ww == 0 || cps >= 2)) continue;   // wider bands: CTA windows, one CTA per SM
                     cand.push_back(sa_launch_config{cps, gpr, ww, ecs});
                 }
     double best_t = 1e300;

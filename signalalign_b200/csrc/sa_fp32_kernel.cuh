@@ -1845,9 +1845,11 @@ __device__ void read_unit_done(const Args &A, int32_t r, int tid, Shared *sh) {
 
 // CPT: cells per thread of the forward sweep (128 threads per region).  The first claims are
 // forward sweeps, one per CTA; once none is left, windows are claimed: one per warp for bands up to
-// kWarpWindowWidth cells wide, one per CTA for wider bands.
-template <int CPT>
-__global__ void __launch_bounds__(kThreads, CPT == 1 ? 2 : 1) worker_kernel(const __grid_constant__ Args A) {
+// kWarpWindowWidth cells wide, one per CTA for wider bands.  MINB: CTAs per SM the registers are
+// budgeted for (2: 255 registers per thread; 3: 168, with some spilling, for batches bound by their
+// total work rather than by one forward chain).
+template <int CPT, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) worker_kernel(const __grid_constant__ Args A) {
     extern __shared__ float4 smem_raw[];
     Shared *sh = reinterpret_cast<Shared *>(smem_raw);
     float *area = reinterpret_cast<float *>(sh + 1);
