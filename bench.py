@@ -307,7 +307,7 @@ def run_serve(args):
 
         # untimed: the same arrival process for a while, so the memory pools hold the block sizes
         # of this load's micro-batches (a server in steady state allocates nothing)
-        warm = reqs[: max(16, n // 2)]
+        warm = reqs
         wt, _ = offer(warm, np.cumsum(r.exponential(1.0 / rate, len(warm))))
         for t, _, _ in wt:
             srv.wait(t, 600000.0)

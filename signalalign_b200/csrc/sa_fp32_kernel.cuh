@@ -289,14 +289,29 @@ __device__ __forceinline__ float warp_sum(float v) {
 
 // Sequential logAdd over vals[0..n) in index order, as dpDiagonal_dotProduct folds an
 // anti-diagonal one cell at a time (pairwiseAligner.c:1014-1027), run by one warp.
-//  * The running result never falls below the running maximum, so a value at least 7.5 below the
-//    maximum of the values before it leaves the result unchanged: only the others are folded, in
-//    index order (compacted into consecutive lanes first).
 //  * Values before the first one within kSeedGap of the overall maximum M enter as one exact
 //    log-sum-exp seed: the final result depends on the running result at that point with weight
 //    at most exp(-(kSeedGap - 0.7)) < 1e-6, so the reference's approximation error there (< 1e-3)
 //    cannot reach the final total.
+//  * From there on the running result r never falls below the running maximum, which is at least
+//    M - kSeedGap, and logAdd(r, v) is exactly r once r - v >= 7.5.  So a value at or below
+//    M - kSeedGap - 7.6 leaves the result unchanged: only the values above that bound are folded,
+//    in index order (compacted into consecutive lanes first).  Folding a few that would also have
+//    left r unchanged costs a step but changes nothing, so no running maximum is needed to pick them.
 constexpr float kSeedGap = 15.0f;
+constexpr float kFoldGap = kSeedGap + 7.6f;
+
+// lane-compacted values of vals[q .. q+32) above `lo` with index >= start, and their count
+__device__ __forceinline__ int fold_candidates(const float *vals, int q, int start, int n, float lo, float &packed) {
+    const int lane = threadIdx.x & 31;
+    const float v = q + lane < n ? vals[q + lane] : kNegInf;
+    const unsigned mask = __ballot_sync(0xffffffffu, q + lane >= start && v > lo);
+    const int nc = __popc(mask);
+    if (nc == 0) return 0;
+    const unsigned src = lane < nc ? __fns(mask, 0, lane + 1) : 0u;
+    packed = __shfl_sync(0xffffffffu, v, (int) (src & 31u));
+    return nc;
+}
 
 __device__ float ordered_fold(const float4 *tab, const float *vals, int n) {
     const int lane = threadIdx.x & 31;
@@ -310,32 +325,17 @@ __device__ float ordered_fold(const float4 *tab, const float *vals, int n) {
         const unsigned m = __ballot_sync(0xffffffffu, b + lane < n && vals[b + lane] >= mall - kSeedGap);
         if (m) { start = b + __ffs(m) - 1; break; }
     }
-    float seed = 0.0f, carry = kNegInf;
+    float seed = 0.0f;
     for (int b = 0; b < start; b += 32) {
         const float v = b + lane < start ? vals[b + lane] : kNegInf;
         seed += v > kNegInf ? __expf(v - mall) : 0.0f;
-        carry = fmaxf(carry, v);
     }
     seed = warp_sum(seed);
-    carry = warp_max(carry);
     float r = seed > 0.0f ? mall + __logf(seed) : kNegInf;
-    for (int b = start; b < n; b += 32) {
-        const float v = b + lane < n ? vals[b + lane] : kNegInf;
-        float incl = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const float t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl = fmaxf(incl, t);
-        }
-        incl = fmaxf(incl, carry);
-        float excl = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) excl = carry;
-        const unsigned mask = __ballot_sync(0xffffffffu, v > excl - 7.6f);
-        const int nc = __popc(mask);
-        const unsigned src = lane < nc ? __fns(mask, 0, lane + 1) : 0u;
-        const float packed = __shfl_sync(0xffffffffu, v, (int) (src & 31u));
+    for (int b = start & ~31; b < n; b += 32) {
+        float packed = kNegInf;
+        const int nc = fold_candidates(vals, b, start, n, mall - kFoldGap, packed);
         for (int k = 0; k < nc; ++k) r = lae(tab, r, __shfl_sync(0xffffffffu, packed, k));
-        carry = __shfl_sync(0xffffffffu, incl, 31);
     }
     return r;
 }
@@ -361,60 +361,23 @@ __device__ __forceinline__ float2 ordered_fold2(const float4 *tab, const float *
         const unsigned m = __ballot_sync(0xffffffffu, q + lane < nb && b[q + lane] >= mb - kSeedGap);
         if (m) { sb = q + __ffs(m) - 1; break; }
     }
-    float seed_a = 0.0f, seed_b = 0.0f, carry_a = kNegInf, carry_b = kNegInf;
+    float seed_a = 0.0f, seed_b = 0.0f;
     for (int q = 0; q < max(sa, sb); q += 32) {
         const float va = q + lane < sa ? a[q + lane] : kNegInf;
         const float vb = q + lane < sb ? b[q + lane] : kNegInf;
         seed_a += va > kNegInf ? __expf(va - ma) : 0.0f;
         seed_b += vb > kNegInf ? __expf(vb - mb) : 0.0f;
-        carry_a = fmaxf(carry_a, va);
-        carry_b = fmaxf(carry_b, vb);
     }
     seed_a = warp_sum(seed_a);
     seed_b = warp_sum(seed_b);
-    carry_a = warp_max(carry_a);
-    carry_b = warp_max(carry_b);
     float ra = ma > kNegInf && seed_a > 0.0f ? ma + __logf(seed_a) : kNegInf;
     float rb = mb > kNegInf && seed_b > 0.0f ? mb + __logf(seed_b) : kNegInf;
     const int ea = ma > kNegInf ? na : 0, eb = mb > kNegInf ? nb : 0;
     // chunk by chunk: candidates compacted, then both sequential chains side by side
-    for (int ca = sa, cb = sb; ca < ea || cb < eb; ca += 32, cb += 32) {
+    for (int ca = sa & ~31, cb = sb & ~31; ca < ea || cb < eb; ca += 32, cb += 32) {
         float pa = kNegInf, pb = kNegInf;
-        int nca = 0, ncb = 0;
-        if (ca < ea) {
-            const float v = ca + lane < ea ? a[ca + lane] : kNegInf;
-            float incl = v;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const float t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl = fmaxf(incl, t);
-            }
-            incl = fmaxf(incl, carry_a);
-            float excl = __shfl_up_sync(0xffffffffu, incl, 1);
-            if (lane == 0) excl = carry_a;
-            const unsigned mask = __ballot_sync(0xffffffffu, v > excl - 7.6f);
-            nca = __popc(mask);
-            const unsigned src = lane < nca ? __fns(mask, 0, lane + 1) : 0u;
-            pa = __shfl_sync(0xffffffffu, v, (int) (src & 31u));
-            carry_a = __shfl_sync(0xffffffffu, incl, 31);
-        }
-        if (cb < eb) {
-            const float v = cb + lane < eb ? b[cb + lane] : kNegInf;
-            float incl = v;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const float t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl = fmaxf(incl, t);
-            }
-            incl = fmaxf(incl, carry_b);
-            float excl = __shfl_up_sync(0xffffffffu, incl, 1);
-            if (lane == 0) excl = carry_b;
-            const unsigned mask = __ballot_sync(0xffffffffu, v > excl - 7.6f);
-            ncb = __popc(mask);
-            const unsigned src = lane < ncb ? __fns(mask, 0, lane + 1) : 0u;
-            pb = __shfl_sync(0xffffffffu, v, (int) (src & 31u));
-            carry_b = __shfl_sync(0xffffffffu, incl, 31);
-        }
+        const int nca = ca < ea ? fold_candidates(a, ca, sa, ea, ma - kFoldGap, pa) : 0;
+        const int ncb = cb < eb ? fold_candidates(b, cb, sb, eb, mb - kFoldGap, pb) : 0;
         for (int k = 0; k < max(nca, ncb); ++k) {
             const float xa = __shfl_sync(0xffffffffu, pa, k), xb = __shfl_sync(0xffffffffu, pb, k);
             if (k < nca) ra = lae(tab, ra, xa);
@@ -1384,9 +1347,8 @@ struct WarpWindow {
     int32_t off0, offp;           // first cells of d and d+1
     // look-ahead operands of a step's cells, by step parity: match emission of the match
     // successor, extra-event emission of the upper successor, skip emission of the lower
-    // successor, forward match value, path k-mer id; and the forward base and shift
+    // successor, forward match value; and the forward base and shift
     float qM[2][WCPT], qY[2][WCPT], qX[2][WCPT], qF[2][WCPT];
-    int32_t qK[2][WCPT];
     double qB[2];
     float qS[2];
     float mxD, mx_last, lm_prev, gamma1;
@@ -1411,7 +1373,6 @@ struct WarpWindow {
             qY[Q][j] = __ldg(E1 + SE_Y * m1.W + clampi((xmy - 1 - m1.L) >> 1, 0, max(m1.W - 1, 0)));
             qX[Q][j] = raw_gapx(c, x + 1);
             qF[Q][j] = __ldcg(Fm + ST_M * m.W + clampi(i, 0, max(m.W - 1, 0)));
-            qK[Q][j] = __ldg(A.kmer + R.kmer_base + clampi(x - 1, 0, max(R.lX - 1, 0)));
         }
         qB[Q] = __ldcg(A.base + db + max(dd, 0));
         qS[Q] = __ldcg(A.fshift + db + max(dd, 0));
@@ -1419,9 +1380,9 @@ struct WarpWindow {
 
     // Operands of a refresh at anti-diagonal dd (meta m, first cell off): its gap states, and for
     // the cells of dd+1 (m1, off1) the forward values of dd-1 (m_1, off_1) on their match
-    // predecessors and their match emissions.  load_refresh issues the loads one anti-diagonal
-    // early (forward values through L2: other CTAs wrote them during this launch);
-    // store_refresh puts them in this warp's staging rows at the end of that step.
+    // predecessors and their match emissions.  At the end of the step before the refresh,
+    // load_refresh loads them (forward values through L2: other CTAs wrote them during this
+    // launch) and store_refresh puts them in this warp's staging rows.
     struct RefreshOps {
         float x[WCPT], y[WCPT], m[WCPT], tx[WCPT], ty[WCPT], e[WCPT];
     };
@@ -1478,8 +1439,6 @@ struct WarpWindow {
         const int32_t offm = off0 - mm.W;
         prefetch<1 - K>(d - 1, mm, offm, m0, off0, mp, offp);
         const bool refresh_next = d - 1 > T && d - 1 <= from && (mm.flags & kFlagRefresh) != 0;
-        RefreshOps rops;
-        if (refresh_next) load_refresh(rops, mm, offm, m0, off0, mmm, offm - mmm.W, d - 2);
         // the recursion on d (D itself holds the end-state values); B of the cells kept in registers
         float lm = kNegInf;
         float bM[WCPT], bX[WCPT], bY[WCPT];
@@ -1607,7 +1566,7 @@ struct WarpWindow {
                         o.score = (int64_t) floor((double) fminf(p, 1.0f) * 10000000.0);
                         o.x = R.x1 + x - 1;
                         o.y = R.y1 + y - 1;
-                        o.kmer = qK[K][j];
+                        o.kmer = __ldg(A.kmer + R.kmer_base + x - 1);   // 1 <= x <= lX for a pair
                         A.out[wt.out_base + q] = o;
                     } else {
                         atomicMax(A.status + R.read, (int32_t) SA_E_OUTPUT);
@@ -1618,6 +1577,11 @@ struct WarpWindow {
             n_out = before;
         }
         if (refresh_next) {
+            // loaded here rather than a step early: held across the step, the 6 x WCPT operands
+            // pushed the 3-CTAs-per-SM build into spilling (312 B per thread; 16 B this way), and
+            // the latency is paid one step in ten
+            RefreshOps rops;
+            load_refresh(rops, mm, offm, m0, off0, mmm, offm - mmm.W, d - 2);
             __syncwarp();   // this step's refresh (if any) has read the staging rows
             store_refresh(rops);
         }
