@@ -54,6 +54,10 @@ def parse_args():
     ap.add_argument("--expectations", action="store_true",
                     help="EM expectations run instead: the reads' expectations in one batched call, against the CPU "
                          "oracle on a bounded sample")
+    ap.add_argument("--segments", type=int, default=None, metavar="DIAGS",
+                    help="forward-segment cap for the batches (sa_setSegmentPolicy: -1 whole regions, 0 automatic)")
+    ap.add_argument("--saturate", type=int, default=0, metavar="N",
+                    help="device throughput with N reads in one batch (the 256-read set repeated), no e2e legs")
     ap.add_argument("--serve", action="store_true",
                     help="serving run instead: Poisson arrivals at --load of the measured capacity, p50/p99 latency")
     ap.add_argument("--serve-requests", type=int, default=400)
@@ -380,6 +384,54 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_saturate(args):
+    """Device throughput of one batch of N reads (the bench's 256 reads repeated to N): many more
+    forward segments and windows than worker CTAs, so the worker runs at its throughput, not at a
+    chain's latency.  Device time of sa_batch_run by CUDA events; no host legs."""
+    import torch
+    from signalalign_b200 import api
+    torch.cuda.set_device(0)
+    cfg, text = model_and_reads(256, args.seed)
+    sm = load_product_model(text)
+    p = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=50, threshold=0.01)
+    base = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                          scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
+    reads = [base[i % len(base)] for i in range(args.saturate)]
+    b = api.Batch(reads, p)
+    b.upload()
+    cells = b.cells
+    for _ in range(max(3, args.warmup)):
+        b.run()
+    torch.cuda.synchronize()
+    ms, kern = [], []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.run()
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        kern.append(b.kernel_ms())
+    b.download()
+    bad = sum(1 for i in range(len(reads)) if b.status(i) != 0)
+    t = statistics.mean(ms)
+    wk = statistics.mean(k[1] for k in kern)
+    peak = api.measure_fp32_peak(0)
+    achieved = WORKER_FLOP_PER_CELL * cells / (wk / 1e3) / 1e12
+    line = {"metric": METRIC, "value": cells / (t / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": t, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": "%d reads (the 256-read bench set repeated), expansion 50"
+                                                   % len(reads), "cells_per_step": cells,
+                                            "launch_config": api.get_launch_config(0, 1),
+                                            "forward_segments": b.segment_info()},
+            "reads_per_sec": len(reads) / (t / 1e3), "read_errors": bad,
+            "kernels_ms": {"emission_kernel": statistics.mean(k[0] for k in kern), "worker_kernel": wk,
+                           "gather_pairs": statistics.mean(k[2] for k in kern)},
+            "roofline": {"kernel": "worker_kernel", "bound": "fp32", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak}}
+    print(json.dumps(line), flush=True)
+
+
 def run_config(args):
     """Configs 2 and 3 on one GPU: the device time of sa_batch_run over every alignment (config 3 in
     sub-batches of 512 alignments, which bounds the stores to ~40 GB), the end-to-end time of
@@ -538,11 +590,17 @@ def run_expectations(args):
 
 def main():
     args = parse_args()
+    if args.segments is not None:
+        from signalalign_b200 import api
+        api.set_segment_policy(args.segments, api.get_segment_policy()[1])
     if args.expectations:
         run_expectations(args)
         return
     if args.serve:
         run_serve(args)
+        return
+    if args.saturate:
+        run_saturate(args)
         return
     if args.config != 1 and args.impl == "ours":
         run_config(args)
