@@ -341,13 +341,15 @@ constexpr int64_t kSegMin = 4096;
 int32_t region_warm(const Region &rg, int32_t warm) { return std::max<int32_t>(warm, 10 * rg.max_width); }
 
 // Window indices (>= 1) whose T starts a new segment of region rg: k pieces of about equal sweep
-// time (L + warm each; the first piece owns L + warm anti-diagonals and needs no warm-up), each
-// cut at the first window start at or after its ideal place, none leaving less than L / 2 behind.
+// time (L + warm each; the first piece owns L + warm anti-diagonals and needs no warm-up, and L is
+// at least warm), each cut at the first window start at or after its ideal place, none leaving less
+// than L / 2 behind.
 void plan_cuts(const Region &rg, int64_t target, int32_t warm, std::vector<int32_t> &cuts) {
     cuts.clear();
     const int64_t n = rg.lX + rg.lY;
     if (target <= (int64_t) warm + 64 || n <= target) return;
-    const int64_t k = (n - warm + (target - warm) - 1) / (target - warm);
+    // pieces: sweeps of at most `target`, and none owning fewer anti-diagonals than its warm-up
+    const int64_t k = std::min((n - warm + (target - warm) - 1) / (target - warm), (n - warm) / warm);
     if (k < 2) return;
     const double L = (double) (n - warm) / (double) k;
     size_t j = 1;

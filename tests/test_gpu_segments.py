@@ -123,3 +123,41 @@ def test_served_reads_count_their_stitches(api, policy):
         assert st == 0
         assert W.max_posterior_error(whole.pairs(i), pairs, p.threshold) <= 1e-5
         assert abs(ll - whole.log_likelihood(i)) <= 1e-7 * abs(whole.log_likelihood(i))
+
+
+def test_segments_hdp_split_regions_and_wide_bands(api, policy):
+    """Segmented against whole sweeps where the segment planner meets the other paths: an HDP machine
+    (emissions in FP64 on the device), regions split by large anchor gaps, and a band wider than 128
+    cells (two cells per thread, CTA-wide windows)."""
+    from oracle import formats
+    cfg = synth.config2(seed=64, n_reads=2, span=(5000, 7000))
+    hdp = W.hdp_dict(cfg["hdp"], 5 ** 6)
+    m = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["table"]).split("\n")[:3])
+    sm_h = W.gpu_model(api, m, orc.EMIT_HDP, None, hdp)
+    hdp_inputs = [api.ReadInput(sm=sm_h, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                                scale=rd["scale"], shift=rd["shift"]) for rd in cfg["reads"]]
+    gcfg, _, sm_g, g_inputs = _case(api, seed=65, n_reads=2, span=(5000, 7000))
+    # anchors dropped over 150 reference positions in the middle: that gap (about 200 x 320 cells)
+    # is larger than the split limit (100 x 100), the others (about 50 x 80) are not, so each read
+    # becomes two long regions
+    split_inputs = []
+    for rd in gcfg["reads"]:
+        a = np.asarray(rd["anchors"]).reshape(-1, 2)
+        L = len(rd["reference"])
+        keep = (a[:, 0] < 0.5 * L - 75) | (a[:, 0] > 0.5 * L + 75)
+        split_inputs.append(api.ReadInput(sm=sm_g, reference=rd["reference"], events=rd["events"], anchors=a[keep],
+                                          scale=rd["scale"], shift=rd["shift"]))
+    cases = [(hdp_inputs, api.pairwiseAlignmentBandingParameters_construct()),
+             (split_inputs, api.pairwiseAlignmentBandingParameters_construct(split_matrix_bigger_than_this=100 * 100)),
+             (g_inputs, api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=200))]
+    for inputs, p in cases:
+        seg = _run(api, inputs, p, 4096)
+        whole = _run(api, inputs, p, -1)
+        info = seg.segment_info()
+        assert info["stitches"] > 0 and info["redone"] == 0, (p.diagonal_expansion, info)
+        if p.split_matrix_bigger_than_this == 100 * 100:
+            assert seg.regions > len(inputs)
+        for i in range(len(inputs)):
+            assert seg.status(i) == 0 and whole.status(i) == 0
+            assert W.max_posterior_error(whole.pairs(i), seg.pairs(i), p.threshold) <= 1e-5
+            assert abs(seg.log_likelihood(i) - whole.log_likelihood(i)) <= 1e-7 * abs(whole.log_likelihood(i))
