@@ -474,6 +474,7 @@ __device__ __forceinline__ void ring_init(float *base, int wmax) {
 // cell reads them from there; a chunk whose ranges exceed kEmitSpan reads global memory per cell.
 constexpr int kEmitWarps = 4;
 constexpr int kEmitSpan = 192;
+constexpr int kEmitCols = 4;   // column slots per lane of the column-stationary Gaussian path
 // The k-mer constants are staged as two float4 halves in separate arrays: lanes reading consecutive
 // columns then load 16-byte strides, which shared memory serves without bank conflicts (32-byte
 // records would put two lanes on every bank group).
@@ -551,7 +552,52 @@ __global__ void __launch_bounds__(32 * kEmitWarps) emission_kernel(const __grid_
             yhi = __reduce_max_sync(0xffffffffu, in ? (dk - Lk) >> 1 : INT32_MIN);
         }
         const bool staged = xhi - xlo < kEmitSpan && yhi - ylo < kEmitSpan;
-        if (staged) {
+        const bool by_column = staged && !c.hdp && xhi - xlo < 32 * kEmitCols;
+        if (by_column) {
+            // Gaussian emissions, column-stationary: lane l owns columns xlo + l + 32 q and keeps their
+            // k-mer constants in registers for the whole chunk, so a cell reads only its event from
+            // shared memory (16 B instead of 52 B with the constants staged too); on each
+            // anti-diagonal the lanes' columns are consecutive cells, so the stores coalesce
+            constexpr int kCols = kEmitCols;
+            const int nq = (xhi - xlo + 32) / 32;
+            KmerConst32 kk[kCols];
+            bool col_ok[kCols];
+#pragma unroll
+            for (int q = 0; q < kCols; ++q) {
+                const int32_t x = xlo + lane + 32 * q;
+                col_ok[q] = q < nq && x <= xhi && x >= 1 && x <= c.R.lX;
+                const int32_t kid = col_ok[q] ? __ldg(A.kmer + c.R.kmer_base + x - 1) : 0;
+                const float4 *kp = reinterpret_cast<const float4 *>(c.M->kc + kid);
+                const float4 ka = q < nq ? __ldg(kp) : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float4 kb = q < nq ? __ldg(kp + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
+                kk[q] = KmerConst32{ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
+            }
+            for (int q = lane; q <= yhi - ylo; q += 32) {
+                const int32_t yc = clampi(ylo + q - 1, 0, max(c.R.lY - 1, 0));
+                st.ev[q] = __ldg(reinterpret_cast<const float4 *>(A.events + c.R.event_base + yc));
+            }
+            __syncwarp();
+            for (int k = 0; k < C.nd; ++k) {
+                const int32_t d = C.d0 + k;
+                const int32_t L = __shfl_sync(0xffffffffu, mt.x, k);
+                const int32_t W = __shfl_sync(0xffffffffu, w, k);
+                float *Ed = A.E + 2 * (C.cell + __shfl_sync(0xffffffffu, off, k));
+                const int32_t xfirst = (d + L) >> 1;   // column of the anti-diagonal's cell 0
+#pragma unroll
+                for (int q = 0; q < kCols; ++q) {
+                    if (q >= nq) break;
+                    const int32_t x = xlo + lane + 32 * q, i = x - xfirst, y = d - x;
+                    if (i < 0 || i >= W) continue;
+                    float em = kNegInf, ey = kNegInf;
+                    if (col_ok[q] && y >= 1 && y <= c.R.lY) {
+                        const float4 v = st.ev[y - ylo];
+                        emit_gauss(kk[q], Event32{v.x, v.y, v.z, v.w}, c.rs, em, ey);
+                    }
+                    Ed[SE_M * W + i] = em;
+                    Ed[SE_Y * W + i] = ey;
+                }
+            }
+        } else if (staged) {
             for (int q = lane; q <= xhi - xlo; q += 32) {
                 const int32_t x = xlo + q;
                 const bool ok = x >= 1 && x <= c.R.lX;
@@ -570,7 +616,9 @@ __global__ void __launch_bounds__(32 * kEmitWarps) emission_kernel(const __grid_
             }
             __syncwarp();
         }
-        for (int k = 0; k < C.nd; ++k) {
+        // every other chunk (HDP emissions, or a chunk spanning more than 128 columns or the stage's
+        // rows): a lane per cell of each anti-diagonal
+        for (int k = 0; k < (by_column ? 0 : C.nd); ++k) {
             const int32_t d = C.d0 + k;
             const int32_t L = __shfl_sync(0xffffffffu, mt.x, k);
             const int32_t W = __shfl_sync(0xffffffffu, w, k);
