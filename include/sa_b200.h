@@ -280,6 +280,14 @@ sa_status sa_batch_set_wait_limit(sa_batch *b, int64_t cycles);
  * warmup_diags: default 1024, at least 64.  Applies to batches created afterwards. */
 sa_status sa_setSegmentPolicy(int32_t segment_diags, int32_t warmup_diags);
 sa_status sa_getSegmentPolicy(int32_t *segment_diags, int32_t *warmup_diags);
+/* The forward segments the batched form would plan for one read (host only, no device): per
+ * segment 6 int64 (region, first anti-diagonal b (exclusive unless 0), last anti-diagonal, warm-up
+ * anti-diagonals, region-relative index of the first window it publishes, region's widest
+ * anti-diagonal), for an explicit cap segment_diags > 0 (or < 0: regions whole).  Ragged ends as
+ * signalMachine passes them.  SA_E_OUTPUT with *n_segments set when capacity is too small. */
+sa_status sa_planForwardSegments(const int64_t *anchors, int64_t n_anchors, int64_t lX, int64_t lY,
+                                 const sa_params *p, int32_t segment_diags, int32_t warmup_diags, int64_t *out,
+                                 int64_t capacity, int64_t *n_segments);
 /* segments and stitches of a batch; after a download, reads re-run unsegmented and the largest
  * deviation from the constant over the agreeing stitches */
 sa_status sa_batch_segment_info(const sa_batch *b, int64_t *n_segments, int64_t *n_stitches, int64_t *n_redone,

@@ -151,6 +151,8 @@ def _bind(L):
         "sa_setSegmentPolicy": (C.c_int, [C.c_int32, C.c_int32]),
         "sa_getSegmentPolicy": (C.c_int, [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         "sa_batch_segment_info": (C.c_int, [vp, _i64p, _i64p, _i64p, _f64p]),
+        "sa_planForwardSegments": (C.c_int, [_i64p, C.c_int64, C.c_int64, C.c_int64, C.POINTER(Params), C.c_int32,
+                                             C.c_int32, _i64p, C.c_int64, _i64p]),
         "sa_batch_set_stitch_tolerance": (C.c_int, [vp, C.c_double]),
         "sa_getLaunchConfig": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(LaunchConfig)]),
         "sa_setLaunchConfig": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(LaunchConfig)]),
@@ -675,6 +677,19 @@ def set_segment_policy(segment_diags=0, warmup_diags=1024):
     """forward segments of later batches: segment_diags < 0 keeps regions whole, > 0 caps a segment's
     sweep, 0 picks the cap from the batch (sa_setSegmentPolicy)"""
     _check(lib().sa_setSegmentPolicy(int(segment_diags), int(warmup_diags)), "setSegmentPolicy")
+
+
+def plan_forward_segments(anchors, lX, lY, p, segment_diags, warmup_diags=1024):
+    """sa_planForwardSegments: (n, 6) int64 rows (region, first anti-diagonal, last, warm-up, first
+    window, region's widest anti-diagonal) for one read, host only"""
+    a = _anchors(anchors)
+    cap = 4 + (lX + lY) // 64
+    out = np.zeros((cap, 6), np.int64)
+    n = C.c_int64(0)
+    _check(lib().sa_planForwardSegments(a.ctypes.data_as(_i64p), len(a), lX, lY, C.byref(p), int(segment_diags),
+                                        int(warmup_diags), out.ctypes.data_as(_i64p), cap, C.byref(n)),
+           "planForwardSegments")
+    return out[:n.value].copy()
 
 
 def get_segment_policy():

@@ -1100,6 +1100,38 @@ sa_status sa_setSegmentPolicy(int32_t segment_diags, int32_t warmup_diags) {
     return SA_OK;
 }
 
+sa_status sa_planForwardSegments(const int64_t *anchors, int64_t n_anchors, int64_t lX, int64_t lY,
+                                 const sa_params *p, int32_t segment_diags, int32_t warmup_diags, int64_t *out,
+                                 int64_t capacity, int64_t *n_segments) {
+    if ((n_anchors > 0 && !anchors) || lX < 0 || lY < 0 || !p || !n_segments || capacity < 0 ||
+        (capacity > 0 && !out) || warmup_diags < 64 || segment_diags == 0)
+        return SA_E_ARG;
+    std::vector<Region> regs;
+    sa_status st = plan_regions(anchors, n_anchors, lX, lY, *p, true, true, regs);
+    if (st) return st;
+    int64_t k = 0;
+    std::vector<int32_t> cuts;
+    for (size_t g = 0; g < regs.size(); ++g) {
+        const Region &rg = regs[g];
+        const int32_t wr = region_warm(rg, warmup_diags);
+        cuts.clear();
+        if (segment_diags > 0) plan_cuts(rg, segment_diags, wr, cuts);
+        for (size_t q = 0; q <= cuts.size(); ++q, ++k) {
+            if (k >= capacity) continue;
+            const int64_t b = q == 0 ? 0 : rg.windows[cuts[q - 1]].T;
+            int64_t *o = out + 6 * k;
+            o[0] = (int64_t) g;
+            o[1] = b;
+            o[2] = q == cuts.size() ? rg.lX + rg.lY : rg.windows[cuts[q]].T;
+            o[3] = q == 0 ? 0 : wr + ((2 - wr) % 3 + 3) % 3;
+            o[4] = q == 0 ? 0 : cuts[q - 1];
+            o[5] = rg.max_width;
+        }
+    }
+    *n_segments = k;
+    return k > capacity ? SA_E_OUTPUT : SA_OK;
+}
+
 sa_status sa_getSegmentPolicy(int32_t *segment_diags, int32_t *warmup_diags) {
     if (!segment_diags || !warmup_diags) return SA_E_ARG;
     *segment_diags = g_seg_target.load();
