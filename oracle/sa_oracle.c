@@ -947,3 +947,67 @@ int64_t orc_expand_kmer(const char *kmer, int k, const char *options, char *out,
     }
     return np;
 }
+
+/* Forgetting of the forward start (test infrastructure for the GPU form's forward segments): the
+ * forward sweep of getPosteriorProbsWithBanding (pairwiseAligner.c:1310-1325) from anti-diagonal 0,
+ * and, for each start s in starts, the same sweep begun at s from a flat vector (anti-diagonals
+ * s-2 and s-1 all 0 in every state of every band cell).  logAdd depends only on the difference of
+ * its arguments, so a sweep's values shifted by a constant stay shifted by it.  steps_out[k] is the
+ * number of anti-diagonals after s from which on, up to s + horizon (or the end), both sweeps have
+ * the same -inf cells and every finite difference lies within tol of the others on the same
+ * anti-diagonal; -1 if that never holds. */
+int orc_flat_start_forgetting(const orc_model *m, const char *seq, int64_t lX, const double *events, int64_t lY,
+                              const int64_t *anchors, int64_t n_anchors, int64_t expansion, int ragged_left,
+                              const int64_t *starts, int64_t n_starts, int64_t horizon, double tol,
+                              int64_t *steps_out) {
+    int64_t n = lX + lY;
+    int64_t *xl = (int64_t *) malloc((size_t) (n + 1) * sizeof(int64_t));
+    int64_t *xr = (int64_t *) malloc((size_t) (n + 1) * sizeof(int64_t));
+    orc_paths P; memset(&P, 0, sizeof(P));
+    orc_dp dp; memset(&dp, 0, sizeof(dp));
+    int rc = !xl || !xr ? ORC_E_NOMEM : orc_band(anchors, n_anchors, lX, lY, expansion, xl, xr);
+    if (!rc) rc = orc_paths_build(&P, seq, lX, m->kmer_length, "", 0, m);
+    if (!rc) rc = orc_dp_init(&dp, m, &P, events, lY, xl, xr);
+    if (rc) goto done;
+    double s0[3];
+    orc_start_probs(m, ragged_left, s0);
+    orc_diag_fill(&dp.F[0], s0[0], s0[1], s0[2]);
+    dp.F[0].live = 1;
+    for (int64_t d = 1; d <= n; d++) {
+        orc_diag_fill(&dp.F[d], ORC_LOG_ZERO, ORC_LOG_ZERO, ORC_LOG_ZERO);
+        dp.F[d].live = 1;
+        orc_diag_calc(&dp, d, &dp.F[d], &dp.F[d - 1], d >= 2 ? &dp.F[d - 2] : NULL, 1);
+    }
+    /* the flat-start sweeps use the backward store */
+    for (int64_t k = 0; k < n_starts; k++) {
+        int64_t st = starts[k], last_bad = -1, end = st + horizon < n ? st + horizon : n;
+        steps_out[k] = -1;
+        if (st < 2 || st > n) continue;
+        orc_diag_fill(&dp.B[st - 2], 0, 0, 0); dp.B[st - 2].live = 1;
+        orc_diag_fill(&dp.B[st - 1], 0, 0, 0); dp.B[st - 1].live = 1;
+        for (int64_t d = st; d <= end; d++) {
+            orc_diag_fill(&dp.B[d], ORC_LOG_ZERO, ORC_LOG_ZERO, ORC_LOG_ZERO);
+            dp.B[d].live = 1;
+            orc_diag_calc(&dp, d, &dp.B[d], &dp.B[d - 1], &dp.B[d - 2], 1);
+            int64_t nv = 3 * dp.F[d].poff[dp.F[d].ncell];
+            double lo = INFINITY, hi = -INFINITY;
+            int bad = 0;
+            for (int64_t i = 0; i < nv; i++) {
+                double a = dp.F[d].v[i], b = dp.B[d].v[i];
+                int fa = a > -1e300, fb = b > -1e300;
+                if (fa != fb) { bad = 1; break; }
+                if (!fa) continue;
+                lo = a - b < lo ? a - b : lo;
+                hi = a - b > hi ? a - b : hi;
+            }
+            if (bad || hi - lo > tol) last_bad = d;
+        }
+        steps_out[k] = last_bad < end ? last_bad + 1 - st : -1;
+        for (int64_t d = st - 2; d <= end; d++) dp.B[d].live = 0;
+    }
+done:
+    orc_dp_free(&dp);
+    orc_paths_free(&P);
+    free(xl); free(xr);
+    return rc;
+}

@@ -88,3 +88,25 @@ def test_plan_arguments(api):
         api.plan_forward_segments(rd["anchors"], lX, lY, p, 0)        # 0 is the batch's automatic cap
     with pytest.raises(api.SAError):
         api.plan_forward_segments(rd["anchors"], lX, lY, p, 4096, 10)  # warm-up below 64
+
+
+@pytest.mark.parametrize("expansion", [50, 200])
+def test_flat_start_forgets_within_the_warmup(api, expansion):
+    """What forward segments rest on, on the FP64 oracle: a forward sweep begun from a flat vector
+    becomes the true sweep minus one constant (to 1e-9 on every finite cell, with the same -inf
+    cells) well within the warm-up the planner gives a segment (max(1024, 10 band widths))."""
+    import workloads as W
+    cfg = synth.config1(seed=95 + expansion, n_reads=3, span=(3000, 5000))
+    m = W.gaussian_model(cfg)
+    worst = 0
+    for rd in cfg["reads"]:
+        om = W.oracle_model(m, orc.EMIT_DESCALED, rd)
+        lX, lY = len(rd["reference"]) - 5, len(rd["events"])
+        _, maxw = window_starts(rd["anchors"], lX, lY, expansion)
+        warm = max(1024, 10 * maxw)
+        starts = list(range(warm + 2, lX + lY - warm, 2500))
+        steps = orc.flat_start_forgetting(om, rd["reference"], rd["events"], rd["anchors"], starts, expansion,
+                                          horizon=warm + 500, tol=1e-9)
+        assert (steps >= 0).all(), steps
+        worst = max(worst, int(steps.max()) / warm)
+    assert worst < 0.8, worst
