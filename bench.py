@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--expectations", action="store_true",
                     help="EM expectations run instead: the reads' expectations in one batched call, against the CPU "
                          "oracle on a bounded sample")
+    ap.add_argument("--route", default="substitute", choices=["substitute", "degenerate"],
+                    help="config 3: all-C and all-E references, or one reference with X (C or E) at the sites")
     ap.add_argument("--segments", type=int, default=None, metavar="DIAGS",
                     help="forward-segment cap for the batches (sa_setSegmentPolicy: -1 whole regions, 0 automatic)")
     ap.add_argument("--saturate", type=int, default=0, metavar="N",
@@ -100,7 +102,7 @@ def load_product_model(text, device=0):
         os.unlink(path)
 
 
-def accuracy_vs_oracle(m, reads, got_pairs, got_ll, threshold, threads, emission=None, hdp=None):
+def accuracy_vs_oracle(m, reads, got_pairs, got_ll, threshold, threads, emission=None, hdp=None, options="CEO"):
     """Every read's pairs and log-likelihood against the FP64 oracle, one read per host thread.
     Returns the largest posterior error over the union of each read's pairs (a pair on one side only
     counts as its posterior minus the threshold), the largest |log-likelihood| error (absolute and
@@ -114,7 +116,8 @@ def accuracy_vs_oracle(m, reads, got_pairs, got_ll, threshold, threads, emission
         rd = reads[i]
         om = orc.OracleModel(m if not isinstance(m, list) else m[i], emission, rd["scale"], rd["shift"],
                              rd.get("var", 1.0), hdp=hdp)
-        want, tps = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], p, with_total_probs=True)
+        want, tps = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], p, options=options,
+                                      with_total_probs=True)
         got = got_pairs(i)
         ma = {(int(r["x"]), int(r["y"])): r["score"] / 1e7 for r in want}
         mg = {(int(r["x"]), int(r["y"])): r["score"] / 1e7 for r in got}
@@ -454,7 +457,7 @@ def run_config(args):
         workload = "128 reads x U(5kb,15kb), 6-mer ACEGT HDP (15,625 k-mers, 2000-point grid), expansion 50"
         sub = len(als)
     else:
-        cfg = synth.config3(seed=args.seed + 2)
+        cfg = synth.config3(seed=args.seed + 2, route=args.route)
         hdp = W.hdp_dict(cfg["hdp"], 5 ** 6)
         gm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["gauss_table"]).split("\n")[:3])
         hm = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["hdp_table"]).split("\n")[:3])
@@ -462,12 +465,19 @@ def run_config(args):
                             orc.EMIT_DESCALED, None),
                   "hdp": (W.gpu_model(api, hm, orc.EMIT_HDP, None, hdp), hm, orc.EMIT_HDP, hdp)}
         als = cfg["alignments"]
-        workload = ("512 reads x U(1kb,30kb) x {template, complement} x {all-C, all-E} at CCWGG sites = 2048 "
-                    "alignments, 6-mer ACEGT Gaussian and HDP machines mixed")
+        if args.route == "substitute":
+            workload = ("512 reads x U(1kb,30kb) x {template, complement} x {all-C, all-E} at CCWGG sites = 2048 "
+                        "alignments, 6-mer ACEGT Gaussian and HDP machines mixed")
+        else:
+            workload = ("512 reads x U(1kb,30kb) x {template, complement}, X (C or E) at CCWGG sites = 1024 "
+                        "alignments with two-path cells over the sites (plain FP64 form), 6-mer ACEGT Gaussian "
+                        "and HDP machines mixed")
         sub = 512
     p = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=50, threshold=0.01)
+    degen = api.CYTOSINE_METHYLATION2 if args.config == 3 and args.route == "degenerate" else api.CYTOSINE_METHYLATION3
+    options = "CE" if degen == api.CYTOSINE_METHYLATION2 else "CEO"
     inputs = [api.ReadInput(sm=models[a["model"]][0], reference=a["reference"], events=a["events"],
-                            anchors=a["anchors"], scale=a["scale"], shift=a["shift"]) for a in als]
+                            anchors=a["anchors"], scale=a["scale"], shift=a["shift"], degenerate=degen) for a in als]
     groups = [inputs[i:i + sub] for i in range(0, len(inputs), sub)]
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
@@ -512,7 +522,8 @@ def run_config(args):
         if not idx:
             continue
         a_k = accuracy_vs_oracle(mm, [sub_reads[j] for j in idx], lambda q: bb.pairs(idx[q]),
-                                 lambda q: bb.log_likelihood(idx[q]), 0.01, os.cpu_count() or 1, emission=emis, hdp=hh)
+                                 lambda q: bb.log_likelihood(idx[q]), 0.01, os.cpu_count() or 1, emission=emis, hdp=hh,
+                                 options=options)
         acc[mk] = a_k
     del ms
     line = {"metric": METRIC, "value": cells / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
