@@ -892,6 +892,9 @@ sa_status sa_batch_run(sa_batch *b, void *stream) {
     // every run gets a new number (from 1), also one that launches nothing: a record counts for the
     // run whose number it holds
     if (b->d_done) ++b->run_seq;
+    // re-runs after a disagreeing stitch belong to one run's download
+    std::fill(b->redone.begin(), b->redone.end(), 0);
+    b->n_redone = 0;
     // what the kernels expect cleared: the results block (counters, per-read status and pair
     // ranges, log-likelihoods), the window pair counts, and the ready queue (-1 = empty)
     if (cudaMemsetAsync(b->dev_base + b->res_off, 0, b->res_bytes, s) != cudaSuccess ||

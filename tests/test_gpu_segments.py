@@ -97,8 +97,10 @@ def test_disagreeing_stitches_rerun_unsegmented(api, policy):
     forced.set_stitch_tolerance(1.0)
     forced.run()
     forced.download()
+    assert forced.segment_info()["redone"] == 0
     for i in range(len(inputs)):
         assert W.max_posterior_error(whole.pairs(i), forced.pairs(i), p.threshold) <= 1e-5
+        assert abs(forced.log_likelihood(i) - whole.log_likelihood(i)) <= 1e-7 * abs(whole.log_likelihood(i))
 
 
 def test_served_reads_count_their_stitches(api, policy):
