@@ -36,6 +36,9 @@ FLOP_PER_CELL = 74.0   # forward + backward + posterior incl. emissions, FP32 fo
 # emissions per cell (~2 x 10 FLOP per pass in the reference) are computed once by emission_kernel
 WORKER_FLOP_PER_CELL = 34.0
 EMISSION_BYTES_PER_CELL = 8.0   # emission_kernel writes match + extra-event emission per cell
+# the whole path's FP32 work per band cell in the scaled-probability accounting: both sweeps'
+# transitions (2 x 16), two emissions per sweep (2 x 2 x ~10) and the posterior (~2)
+PATH_FLOP_PER_CELL = 74.0
 WORKLOAD = "256 reads x U(2kb,20kb) spans, 6-mer ACGT Gaussian table, expansion 50, threshold 0.01"
 
 
@@ -830,6 +833,10 @@ def main():
                                           "it is cut into forward segments; alone_worker_ms is the worker kernel "
                                           "on the longest read alone (its segments on separate CTAs), frac = "
                                           "alone / batch worker time"},
+                "path_roofline": {"flop_per_cell": PATH_FLOP_PER_CELL, "bound_cells_per_sec": peak * 1e12 / PATH_FLOP_PER_CELL,
+                                  "achieved_cells_per_sec": value / world,
+                                  "frac": value / world / (peak * 1e12 / PATH_FLOP_PER_CELL),
+                                  "note": "all three kernels per band cell against the FP32 FMA probe"},
                 "gpu_launches": launches, "clocks": clocks}
     if world > 1:
         dist.barrier()
