@@ -827,7 +827,8 @@ sa_status sa_batch_create(const sa_read *reads, int64_t n_reads, const sa_params
         cudaSetDevice(prev);
     }
     if (!st && !b->plain_reads.empty()) {
-        st = plain_create(b->plain_reads.data(), (int64_t) b->plain_reads.size(), *p, kPlainBatchMaxBytes, &b->plain);
+        st = plain_create(b->plain_reads.data(), (int64_t) b->plain_reads.size(), *p, kPlainBatchMaxBytes, &b->plain,
+                          true);
         if (!st && plain_device(b->plain) != b->device) st = SA_E_ARG;
     }
     if (!st) st = mem_get(MemKind::Device, b->device, b->dev_bytes, b->dev);
@@ -1159,6 +1160,7 @@ sa_status sa_batch_segment_info(const sa_batch *b, int64_t *n_segments, int64_t 
 sa_status sa_batch_set_stitch_tolerance(sa_batch *b, double scale) {
     if (!b || !(scale == scale)) return SA_E_ARG;
     b->stitch_tol = (float) scale;
+    if (b->plain) plain_set_stitch_tolerance(b->plain, scale);
     return SA_OK;
 }
 
@@ -1279,6 +1281,17 @@ sa_status batch_plan_host(const sa_read *reads, int64_t n_reads, const sa_params
 }
 
 int batch_device(const sa_batch *b) { return b->device; }
+
+void segment_policy(int32_t &target, int32_t &warm) {
+    target = g_seg_target.load();
+    warm = g_seg_warm.load();
+}
+int64_t segment_min() { return kSegMin; }
+int32_t segment_warm(const Region &rg, int32_t warm) { return region_warm(rg, warm); }
+void segment_cuts(const Region &rg, int64_t target, int32_t warm, std::vector<int32_t> &cuts) {
+    plan_cuts(rg, target, warm, cuts);
+}
+
 
 bool batch_models_resident(const sa_batch *b) {
     // only the machines of reads the FP32 kernels run: reads routed to the plain form report

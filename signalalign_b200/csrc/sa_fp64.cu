@@ -45,6 +45,11 @@ struct Region64 {
     int32_t lX, lY, n, n_windows;
     int32_t ragged_left, ragged_right;
     int32_t model, ring, stride, pad;
+    // Forward segments of a long region (alignment runs): this task sweeps from anti-diagonal s0
+    // (1 for the region's first segment, which starts from the start probabilities; a later
+    // segment starts from a flat vector, every cell 0, on s0-2 and s0-1) and runs windows w0 .. w1-1;
+    // stitches where it meets its neighbours (-1: none); pairs are tagged with region `tag`
+    int32_t s0, w0, w1, tag, st_in, st_out;
     int64_t ev_base;              // the region's first event in the read (split regions start later)
     const int32_t *xl, *xr;
     const int32_t *pfirst, *pid, *ppre, *psuf;
@@ -59,11 +64,28 @@ struct Region64 {
     int32_t *status;
 };
 
+// where two forward segments of a region meet, at anti-diagonal b (the later one's first window's T):
+// the values of every path slot of b-1 and b, from both sides (4 blocks of stride x 3 doubles:
+// later b-1, later b, earlier b-1, earlier b), and the read it belongs to
+struct Stitch64 {
+    double *vals;
+    int32_t b, region, stride, pad;
+};
+struct Stitch64Res {        // cleared before every run
+    double delta;           // earlier-side value - later-side value (the constant)
+    double spread;          // largest deviation from it over the slots
+    int32_t arrive, result; // sides that wrote their values; 1 agreed, 2 disagreed
+};
+
 struct SetOut {
     sa_aligned_pair *out;
     int32_t *tag;
     unsigned long long *count;
     int64_t cap;
+    const Stitch64 *stitch;   // alignment runs with forward segments
+    Stitch64Res *stres;
+    int32_t *fail;            // per region: a stitch disagreed
+    double stitch_tol;        // tolerance scale (negative: every stitch disagrees)
 };
 
 // Expectations mode (getExpectationsUsingAnchors, pairwiseAligner.c:1983-2003): one CTA walks the
@@ -399,22 +421,155 @@ __device__ void expect_diagonal(const Model64 &M, const Region64 &R, const Expec
 
 // One region: forward sweep, windowed traceback, and per traceback window either the posterior
 // pairs or (expectations mode) the expectation updates.
+// path slots of anti-diagonal d: the first slot (of its first cell) and their number
+__device__ __forceinline__ void diag_slots(const Region64 &R, int32_t d, int32_t &first, int32_t &count) {
+    first = R.pfirst[(d + R.xl[d]) >> 1];
+    count = R.pfirst[((d + R.xr[d]) >> 1) + 1] - first;
+}
+
+// every path slot of anti-diagonal d set to `v` in all three states (whole CTA)
+__device__ void fill_diag(double *ring, const Region64 &R, int32_t d, double v) {
+    int32_t first, count;
+    diag_slots(R, d, first, count);
+    for (int32_t k = threadIdx.x; k < count; k += blockDim.x) {
+        double *c = slot(ring, R, d, first + k);
+        c[S_M] = v;
+        c[S_X] = v;
+        c[S_Y] = v;
+    }
+}
+
+// the forward values of anti-diagonal d into block `blk` of stitch st's values (whole CTA)
+__device__ void stitch_copy64(const Region64 &R, const SetOut &O, int32_t st, int32_t d, int blk) {
+    const Stitch64 S = O.stitch[st];
+    double *dst = S.vals + (int64_t) blk * 3 * S.stride;
+    int32_t first, count;
+    diag_slots(R, d, first, count);
+    for (int32_t k = threadIdx.x; k < count; k += blockDim.x) {
+        const double *c = slot(R.F, R, d, first + k);
+        dst[3 * k] = c[S_M];
+        dst[3 * k + 1] = c[S_X];
+        dst[3 * k + 2] = c[S_Y];
+    }
+}
+
+// Stitch st once both sides wrote their values (whole CTA, the side that arrives second): the same
+// -inf slots, and every difference (earlier - later) within 1e-9 + 1e-11 x (its distance below the
+// largest earlier value) of the difference at that value, which becomes the stitch's constant.
+// FP64 sweeps from different starts agree to rounding once the start is forgotten.
+__device__ void stitch_check64(const Region64 &R, const SetOut &O, int32_t st) {
+    __shared__ double red_a[32], red_d[32];
+    __shared__ int red_ok;
+    const Stitch64 S = O.stitch[st];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = (blockDim.x + 31) >> 5;
+    int32_t f0, c0, f1, c1;
+    diag_slots(R, S.b - 1, f0, c0);
+    diag_slots(R, S.b, f1, c1);
+    const int64_t stride3 = 3 * (int64_t) S.stride;
+    const double *later = S.vals, *earlier = S.vals + 2 * stride3;
+    auto at = [&](const double *base, int32_t q, double &v) {   // q over both anti-diagonals
+        v = q < 3 * c0 ? __ldcg(base + q) : __ldcg(base + stride3 + (q - 3 * c0));
+    };
+    const int32_t nq = 3 * (c0 + c1);
+    double amax = -INFINITY, dref = 0.0;
+    for (int32_t q = tid; q < nq; q += blockDim.x) {
+        double a, b;
+        at(earlier, q, a);
+        at(later, q, b);
+        if (a > kNegInf && b > kNegInf && a > amax) {
+            amax = a;
+            dref = a - b;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double a2 = __shfl_xor_sync(0xffffffffu, amax, o), d2 = __shfl_xor_sync(0xffffffffu, dref, o);
+        if (a2 > amax || (a2 == amax && d2 < dref)) { amax = a2; dref = d2; }
+    }
+    if (lane == 0) { red_a[warp] = amax; red_d[warp] = dref; }
+    if (tid == 0) red_ok = 1;
+    __syncthreads();
+    amax = red_a[0];
+    dref = red_d[0];
+    for (int w = 1; w < nw; ++w)
+        if (red_a[w] > amax || (red_a[w] == amax && red_d[w] < dref)) { amax = red_a[w]; dref = red_d[w]; }
+    bool ok = O.stitch_tol >= 0.0;
+    double spread = 0.0;
+    for (int32_t q = tid; q < nq; q += blockDim.x) {
+        double a, b;
+        at(earlier, q, a);
+        at(later, q, b);
+        const bool fa = a > kNegInf, fb = b > kNegInf;
+        if (fa != fb) {
+            ok = false;
+        } else if (fa) {
+            const double dev = fabs((a - b) - dref);
+            spread = fmax(spread, dev);
+            if (!(dev <= O.stitch_tol * (1e-9 + 1e-11 * (amax - a)))) ok = false;
+        }
+    }
+    __syncthreads();   // red_a / red_d read by every thread
+    if (!ok) red_ok = 0;
+    for (int o = 16; o > 0; o >>= 1) spread = fmax(spread, __shfl_xor_sync(0xffffffffu, spread, o));
+    if (lane == 0) red_a[warp] = spread;
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < nw; ++w) spread = fmax(spread, red_a[w]);
+        Stitch64Res &res = O.stres[st];
+        res.delta = dref;
+        res.spread = spread;
+        res.result = red_ok ? 1 : 2;
+        if (!red_ok) atomicExch(O.fail + S.region, 1);
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// one side of stitch st has written its values (whole CTA): the second to arrive checks it
+__device__ void stitch_arrive64(const Region64 &R, const SetOut &O, int32_t st) {
+    __shared__ int second;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        second = atomicAdd(&O.stres[st].arrive, 1) == 1;
+        __threadfence();
+    }
+    __syncthreads();
+    if (second) stitch_check64(R, O, st);
+    __syncthreads();
+}
+
 __device__ void run_region(const Model64 &M, const Region64 &R, int32_t region, const SetOut &O, const ExpectOut &X,
                            double (&acc)[10]) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    // startStateProb / raggedStartStateProb (stateMachine.c:1022-1032) on anti-diagonal 0
-    if (tid == 0) {
-        double *c = slot(R.F, R, 0, 0);
-        c[S_M] = R.ragged_left ? kNegInf : 0.0;
-        c[S_X] = R.ragged_left ? 0.0 : kNegInf;
-        c[S_Y] = R.ragged_left ? 0.0 : kNegInf;
+    if (R.s0 <= 1) {
+        // startStateProb / raggedStartStateProb (stateMachine.c:1022-1032) on anti-diagonal 0
+        if (tid == 0) {
+            double *c = slot(R.F, R, 0, 0);
+            c[S_M] = R.ragged_left ? kNegInf : 0.0;
+            c[S_X] = R.ragged_left ? 0.0 : kNegInf;
+            c[S_Y] = R.ragged_left ? 0.0 : kNegInf;
+        }
+    } else {
+        // a later forward segment: a flat start two anti-diagonals before its sweep
+        fill_diag(R.F, R, R.s0 - 2, 0.0);
+        fill_diag(R.F, R, R.s0 - 1, 0.0);
     }
     __syncthreads();
-    int32_t wi = 0;
-    Window W = R.win[0];
-    for (int32_t d = 1; d <= R.n; ++d) {
+    // anti-diagonals whose forward values go to a stitch: b-1 and b of each
+    const int32_t b_in = R.st_in >= 0 ? O.stitch[R.st_in].b : -10, b_out = R.st_out >= 0 ? O.stitch[R.st_out].b : -10;
+    int32_t wi = R.w0;
+    Window W = R.win[wi];
+    for (int32_t d = R.s0 <= 1 ? 1 : R.s0; d <= R.n; ++d) {
         for (int32_t xmy = R.xl[d] + 2 * tid; xmy <= R.xr[d]; xmy += 2 * nt) forward_cell(M, R, d, xmy);
         __syncthreads();
+        if (d == b_in - 1 || d == b_in) {
+            stitch_copy64(R, O, R.st_in, d, d - (b_in - 1));
+            __syncthreads();
+        }
+        if (d == b_out - 1 || d == b_out) {
+            stitch_copy64(R, O, R.st_out, d, 2 + d - (b_out - 1));
+            __syncthreads();
+        }
         if (d != W.D) continue;
         // endStateProb / raggedEndStateProb (stateMachine.c:1034-1061) on the traceback anti-diagonal
         const bool ragged_end = W.at_end && R.ragged_right;
@@ -468,7 +623,7 @@ __device__ void run_region(const Model64 &M, const Region64 &R, int32_t region, 
                             o.y = y - 1;
                             o.kmer = R.pid[r];
                             O.out[o_at] = o;
-                            O.tag[o_at] = region;
+                            O.tag[o_at] = R.tag;
                         } else {
                             atomicExch(R.status, (int32_t) SA_E_OUTPUT);
                         }
@@ -477,12 +632,15 @@ __device__ void run_region(const Model64 &M, const Region64 &R, int32_t region, 
             }
         }
         __syncthreads();
-        if (W.at_end) break;
+        if (W.at_end || wi + 1 >= R.w1) break;
         W = R.win[++wi];
     }
-    // the total probability of the last anti-diagonal is the region's log-likelihood
-    if (tid == 0) *R.loglik = R.P[R.n];
+    // the total probability of the last anti-diagonal is the region's log-likelihood (in the last
+    // segment's frame: the host adds the stitches' constants)
+    if (tid == 0 && R.w1 >= R.n_windows) *R.loglik = R.P[R.n];
     __syncthreads();
+    if (R.st_in >= 0) stitch_arrive64(R, O, R.st_in);
+    if (R.st_out >= 0) stitch_arrive64(R, O, R.st_out);
 }
 
 // Expectations mode (XS: one ExpectOut per read): CTA b walks read b's regions in order.
@@ -549,6 +707,8 @@ struct PlainRegion {
     std::vector<int32_t> xl, xr, pfirst, pid, ppre, psuf, row;
     int32_t ring = 3, stride = 1, max_paths = 1;
     size_t ev_off = 0;   // first event of the region in the set's event array
+    std::vector<int32_t> cuts;   // windows that start a later forward segment
+    int32_t warm = 0;            // their warm-up
 };
 
 }  // namespace
@@ -566,6 +726,17 @@ struct PlainSet {
     std::vector<double2> events;
     int64_t cells = 0, cap = 0;
     double threshold = 0.01;
+    // forward segments (alignment runs): per region its first task and first stitch
+    int64_t n_tasks = 0, n_stitch = 0, n_redone = 0;
+    std::vector<int64_t> task_first, stitch_first;
+    double stitch_tol = 1.0;
+    size_t res_stres = 0, res_fail = 0;
+    size_t o_redo = 0;
+    Region64 *d_tasks = nullptr, *d_redo = nullptr;
+    Stitch64 *d_stitch = nullptr;
+    Stitch64Res *d_stres = nullptr;
+    int32_t *d_fail = nullptr;
+    std::vector<Region64> whole;   // host copies of the regions' whole-sweep descriptors (re-runs)
     // device block: inputs (staged in `host_in` with the same layout), results, work
     MemBlock host_in, host_res, dev;
     size_t in_bytes = 0, res_off = 0, res_bytes = 0, dev_bytes = 0;
@@ -608,6 +779,8 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
     const size_t nreg = s->regs.size();
     const size_t o_regions = take(nreg * sizeof(Region64));
     const size_t o_models = take(s->models.size() * sizeof(Model64));
+    const size_t o_tasks = take((size_t) s->n_tasks * sizeof(Region64));
+    const size_t o_stitch = take((size_t) s->n_stitch * sizeof(Stitch64));
     std::vector<Region64> R(nreg);
     struct Off { size_t xl, xr, pfirst, pid, ppre, psuf, row, win; };
     std::vector<Off> off(nreg);
@@ -629,27 +802,44 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
     const size_t o_loglik = take(nreg * sizeof(double));
     const size_t o_status = take(nreg * sizeof(int32_t));
     const size_t o_count = take(sizeof(unsigned long long));
+    const size_t o_stres = take((size_t) s->n_stitch * sizeof(Stitch64Res));
+    const size_t o_fail = take(nreg * sizeof(int32_t));
     s->res_bytes = align256(at) - s->res_off;
     s->res_status = o_status - s->res_off;
     s->res_count = o_count - s->res_off;
+    s->res_stres = o_stres - s->res_off;
+    s->res_fail = o_fail - s->res_off;
     at = s->res_off + s->res_bytes;
     size_t p_total = 0;
     for (const PlainRegion &pr : s->regs) p_total += (size_t) (pr.rg.lX + pr.rg.lY + 1);
     const size_t o_P = take(p_total * sizeof(double));
     s->p_bytes = p_total * sizeof(double);
-    std::vector<size_t> o_F(nreg), o_B(nreg), o_E(nreg);
+    // rings per task: a region's first segment (or its whole sweep) uses the region's, every later
+    // segment its own; stitch values 4 x stride x 3 doubles each
+    std::vector<size_t> o_F(s->n_tasks), o_B(s->n_tasks), o_E(s->n_tasks), o_sv(s->n_stitch);
     for (size_t i = 0; i < nreg; ++i) {
         const size_t ring_bytes = 3 * sizeof(double) * (size_t) s->regs[i].ring * (size_t) s->regs[i].stride;
-        o_F[i] = take(ring_bytes);
-        o_B[i] = take(ring_bytes);
-        o_E[i] = take(ring_bytes / 3 * 2);
+        for (size_t q = 0; q <= s->regs[i].cuts.size(); ++q) {
+            const size_t t = (size_t) s->task_first[i] + q;
+            o_F[t] = take(ring_bytes);
+            o_B[t] = take(ring_bytes);
+            o_E[t] = take(ring_bytes / 3 * 2);
+        }
+        for (size_t q = 0; q < s->regs[i].cuts.size(); ++q)
+            o_sv[(size_t) s->stitch_first[i] + q] = take(4 * 3 * sizeof(double) * (size_t) s->regs[i].stride);
     }
+    s->o_redo = take(nreg * sizeof(Region64));
     const size_t o_out = take((size_t) s->cap * sizeof(sa_aligned_pair));
     const size_t o_tag = take((size_t) s->cap * sizeof(int32_t));
     s->dev_bytes = align256(at);
     if (dev) {
         s->d_regions = reinterpret_cast<Region64 *>(dev + o_regions);
         s->d_models = reinterpret_cast<Model64 *>(dev + o_models);
+        s->d_tasks = reinterpret_cast<Region64 *>(dev + o_tasks);
+        s->d_stitch = reinterpret_cast<Stitch64 *>(dev + o_stitch);
+        s->d_stres = reinterpret_cast<Stitch64Res *>(dev + o_stres);
+        s->d_fail = reinterpret_cast<int32_t *>(dev + o_fail);
+        s->d_redo = reinterpret_cast<Region64 *>(dev + s->o_redo);
         s->d_loglik = reinterpret_cast<double *>(dev + o_loglik);
         s->d_status = reinterpret_cast<int32_t *>(dev + o_status);
         s->d_count = reinterpret_cast<unsigned long long *>(dev + o_count);
@@ -694,15 +884,52 @@ size_t plain_layout(PlainSet *s, unsigned char *host, unsigned char *dev) {
             r.row = reinterpret_cast<const int32_t *>(dev + off[i].row);
             r.ev = reinterpret_cast<const double2 *>(dev + o_events) + pr.ev_off;
             r.win = reinterpret_cast<const Window *>(dev + off[i].win);
-            r.F = reinterpret_cast<double *>(dev + o_F[i]);
-            r.B = reinterpret_cast<double *>(dev + o_B[i]);
-            r.E = reinterpret_cast<double *>(dev + o_E[i]);
+            const size_t t0 = (size_t) s->task_first[i];
+            r.F = reinterpret_cast<double *>(dev + o_F[t0]);
+            r.B = reinterpret_cast<double *>(dev + o_B[t0]);
+            r.E = reinterpret_cast<double *>(dev + o_E[t0]);
+            r.s0 = 1;
+            r.w0 = 0;
+            r.w1 = r.n_windows;
+            r.tag = (int32_t) i;
+            r.st_in = r.st_out = -1;
             r.P = s->d_P + p_at;
             p_at += (size_t) r.n + 1;
             r.loglik = s->d_loglik + i;
             r.status = s->d_status + i;
         }
         std::memcpy(host + o_regions, R.data(), nreg * sizeof(Region64));
+        s->whole = R;
+        // tasks: per region its segments (one, the whole sweep, when it has no cuts), and the stitches
+        std::vector<Region64> T((size_t) s->n_tasks);
+        std::vector<Stitch64> ST((size_t) s->n_stitch);
+        for (size_t i = 0; i < nreg; ++i) {
+            const PlainRegion &pr = s->regs[i];
+            const std::vector<int32_t> &cuts = pr.cuts;
+            for (size_t q = 0; q <= cuts.size(); ++q) {
+                const size_t t = (size_t) s->task_first[i] + q;
+                Region64 r = R[i];
+                r.F = reinterpret_cast<double *>(dev + o_F[t]);
+                r.B = reinterpret_cast<double *>(dev + o_B[t]);
+                r.E = reinterpret_cast<double *>(dev + o_E[t]);
+                r.w0 = q == 0 ? 0 : cuts[q - 1];
+                r.w1 = q == cuts.size() ? r.n_windows : cuts[q];
+                r.s0 = q == 0 ? 1 : pr.rg.windows[cuts[q - 1]].T - pr.warm;
+                r.st_in = q == 0 ? -1 : (int32_t) (s->stitch_first[i] + (int64_t) q - 1);
+                r.st_out = q == cuts.size() ? -1 : (int32_t) (s->stitch_first[i] + (int64_t) q);
+                T[t] = r;
+            }
+            for (size_t q = 0; q < cuts.size(); ++q) {
+                Stitch64 &st = ST[(size_t) s->stitch_first[i] + q];
+                std::memset(&st, 0, sizeof(st));
+                st.vals = reinterpret_cast<double *>(dev + o_sv[(size_t) s->stitch_first[i] + q]);
+                st.b = pr.rg.windows[cuts[q]].T;
+                st.region = (int32_t) i;
+                st.stride = pr.stride;
+            }
+        }
+        if (!T.empty()) std::memcpy(host + o_tasks, T.data(), T.size() * sizeof(Region64));
+        if (!ST.empty()) std::memcpy(host + o_stitch, ST.data(), ST.size() * sizeof(Stitch64));
         for (size_t m = 0; m < s->models.size(); ++m) {
             const sa_state_machine *sm = s->models[m].sm;
             Model64 M;
@@ -782,7 +1009,8 @@ void plan_region(const PathTable &pt, int32_t asz, int64_t kpow, PlainRegion &pr
 
 // Plans a set of reads for the plain form.  Reads that fail planning keep their status and get no
 // regions.  `max_bytes` bounds the device block (SA_E_CAPACITY above it).
-sa_status plain_create(const sa_read *reads, int64_t n_reads, const sa_params &p, size_t max_bytes, PlainSet **out) {
+sa_status plain_create(const sa_read *reads, int64_t n_reads, const sa_params &p, size_t max_bytes, PlainSet **out,
+                       bool segments) {
     *out = nullptr;
     auto *s = new (std::nothrow) PlainSet();
     if (!s) return SA_E_NOMEM;
@@ -847,6 +1075,38 @@ sa_status plain_create(const sa_read *reads, int64_t n_reads, const sa_params &p
     }
     s->device = device < 0 ? 0 : device;
     s->cap = cap;
+    // Forward segments (alignment runs): long regions cut at window starts like the batched form's,
+    // the automatic cap from twice the set's anti-diagonals per CTA slot (four plain CTAs per SM)
+    int32_t policy = -1, warm0 = 1024;
+    if (segments) segment_policy(policy, warm0);
+    int64_t target = policy;
+    if (segments && policy == 0) {
+        int64_t diags = 0;
+        for (const PlainRegion &pr : s->regs) diags += pr.rg.lX + pr.rg.lY + 1;
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess) {
+            cudaGetLastError();
+            sms = 0;
+        }
+        if (sms <= 0) sms = 148;
+        target = std::max<int64_t>(segment_min(), 2 * diags / ((int64_t) sms * 4));
+    }
+    s->task_first.assign(s->regs.size(), 0);
+    s->stitch_first.assign(s->regs.size(), 0);
+    for (size_t i = 0; i < s->regs.size(); ++i) {
+        PlainRegion &pr = s->regs[i];
+        pr.cuts.clear();
+        pr.warm = 0;
+        if (segments && policy >= 0) {
+            const int32_t wr = segment_warm(pr.rg, warm0);
+            segment_cuts(pr.rg, target, wr, pr.cuts);
+            pr.warm = wr;
+        }
+        s->task_first[i] = s->n_tasks;
+        s->stitch_first[i] = s->n_stitch;
+        s->n_tasks += 1 + (int64_t) pr.cuts.size();
+        s->n_stitch += (int64_t) pr.cuts.size();
+    }
     plain_layout(s, nullptr, nullptr);
     if (s->dev_bytes > max_bytes) {
         delete s;
@@ -876,11 +1136,17 @@ sa_status plain_run(PlainSet *s, cudaStream_t stream) {
         return SA_E_CUDA;
     if (s->regs.empty()) return SA_OK;
     SetOut O;
+    std::memset(&O, 0, sizeof(O));
     O.out = s->d_out;
     O.tag = s->d_tag;
     O.count = s->d_count;
     O.cap = s->cap;
-    region_kernel<<<(unsigned) s->regs.size(), 128, 0, stream>>>(s->d_models, s->d_regions, O, nullptr);
+    O.stitch = s->d_stitch;
+    O.stres = s->d_stres;
+    O.fail = s->d_fail;
+    O.stitch_tol = s->stitch_tol;
+    s->n_redone = 0;
+    region_kernel<<<(unsigned) s->n_tasks, 128, 0, stream>>>(s->d_models, s->d_tasks, O, nullptr);
     count_launch();
     return cudaGetLastError() == cudaSuccess ? SA_OK : SA_E_CUDA;
 }
@@ -896,6 +1162,40 @@ sa_status plain_download(PlainSet *s, cudaStream_t stream) {
     const auto *res = static_cast<const unsigned char *>(s->host_res.ptr);
     const auto *loglik = reinterpret_cast<const double *>(res);
     const auto *rstatus = reinterpret_cast<const int32_t *>(res + s->res_status);
+    const auto *stres = reinterpret_cast<const Stitch64Res *>(res + s->res_stres);
+    const auto *fail = reinterpret_cast<const int32_t *>(res + s->res_fail);
+    // regions whose stitch disagreed run again as whole sweeps (their rings are their first
+    // segment's); the pairs of that second launch follow the first launch's in the output
+    const size_t nreg = s->regs.size();
+    std::vector<char> redone(nreg, 0);
+    unsigned long long count0 = *reinterpret_cast<const unsigned long long *>(res + s->res_count);
+    {
+        std::vector<Region64> redo;
+        for (size_t i = 0; i < nreg; ++i)
+            if (fail[i]) {
+                redone[i] = 1;
+                redo.push_back(s->whole[i]);
+            }
+        if (!redo.empty()) {
+            SetOut O;
+            std::memset(&O, 0, sizeof(O));
+            O.out = s->d_out;
+            O.tag = s->d_tag;
+            O.count = s->d_count;
+            O.cap = s->cap;
+            if (cudaMemcpyAsync(s->d_redo, redo.data(), redo.size() * sizeof(Region64), cudaMemcpyHostToDevice,
+                                stream) != cudaSuccess)
+                return SA_E_CUDA;
+            region_kernel<<<(unsigned) redo.size(), 128, 0, stream>>>(s->d_models, s->d_redo, O, nullptr);
+            count_launch();
+            if (cudaGetLastError() != cudaSuccess ||
+                cudaMemcpyAsync(s->host_res.ptr, static_cast<unsigned char *>(s->dev.ptr) + s->res_off, s->res_bytes,
+                                cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+                cudaStreamSynchronize(stream) != cudaSuccess)
+                return SA_E_CUDA;
+            s->n_redone = (int64_t) redo.size();
+        }
+    }
     const auto count = *reinterpret_cast<const unsigned long long *>(res + s->res_count);
     const size_t npairs = (size_t) std::min<unsigned long long>(count, (unsigned long long) s->cap);
     std::vector<sa_aligned_pair> got(npairs);
@@ -910,6 +1210,7 @@ sa_status plain_download(PlainSet *s, cudaStream_t stream) {
     std::vector<std::vector<Emitted>> per_read(n_reads);
     for (size_t i = 0; i < npairs; ++i) {
         const int32_t ri = tag[i];
+        if (i < count0 && redone[ri]) continue;   // superseded by the whole sweep's pairs
         const PlainRegion &pr = s->regs[ri];
         const sa_aligned_pair &g = got[i];
         Emitted e;
@@ -935,6 +1236,9 @@ sa_status plain_download(PlainSet *s, cudaStream_t stream) {
             const int64_t ri = s->read_first[r] + i;
             if (rstatus[ri] && !s->status[r]) s->status[r] = rstatus[ri];
             s->ll[r] += loglik[ri];
+            // the last segment's total is in its own frame: the stitches' constants bring it back
+            if (!redone[ri])
+                for (size_t q = 0; q < s->regs[ri].cuts.size(); ++q) s->ll[r] += stres[s->stitch_first[ri] + q].delta;
         }
         if (count > (unsigned long long) s->cap && s->read_count[r] && !s->status[r]) s->status[r] = SA_E_OUTPUT;
         auto &v = per_read[r];
@@ -957,6 +1261,12 @@ sa_status plain_read_status(const PlainSet *s, int64_t r) { return (sa_status) s
 const std::vector<sa_aligned_pair> &plain_pairs(const PlainSet *s, int64_t r) { return s->pairs[r]; }
 double plain_log_likelihood(const PlainSet *s, int64_t r) { return s->ll[r]; }
 void plain_destroy(PlainSet *s) { delete s; }
+void plain_set_stitch_tolerance(PlainSet *s, double scale) { s->stitch_tol = scale; }
+void plain_segment_info(const PlainSet *s, int64_t *n_tasks, int64_t *n_stitches, int64_t *n_redone) {
+    *n_tasks = s->n_tasks;
+    *n_stitches = s->n_stitch;
+    *n_redone = s->n_redone;
+}
 
 }  // namespace sa
 
@@ -1000,7 +1310,7 @@ extern "C" sa_status sa_getAlignedPairsUsingAnchors(const sa_state_machine *sm_c
     rd.ragged_right = ragged_right;
     rd.degenerate = degenerate;
     PlainSet *s = nullptr;
-    st = plain_create(&rd, 1, *p, kPlainMaxBytes, &s);
+    st = plain_create(&rd, 1, *p, kPlainMaxBytes, &s, true);
     if (st) return st;
     if (s->read_status[0]) {
         st = (sa_status) s->read_status[0];

@@ -155,6 +155,13 @@ struct MemBlock {
 sa_status mem_get(MemKind kind, int device, size_t bytes, MemBlock &out);
 void mem_put(MemBlock &b);
 
+// forward-segment planning shared by both forms (sa_fp32.cu): the policy (cap, -1 off, 0 automatic;
+// warm-up), the automatic cap's floor, a region's warm-up and its cuts (window indices)
+void segment_policy(int32_t &target, int32_t &warm);
+int64_t segment_min();
+int32_t segment_warm(const Region &rg, int32_t warm);
+void segment_cuts(const Region &rg, int64_t target, int32_t warm, std::vector<int32_t> &cuts);
+
 // batches bound to one caller-provided device area instead of their own allocations (sa_fp32.cu)
 sa_status batch_plan_host(const sa_read *reads, int64_t n_reads, const sa_params *p, sa_batch **out);
 int batch_device(const sa_batch *b);
@@ -194,7 +201,13 @@ bool batch_run_events(const sa_batch *b, cudaEvent_t *start, cudaEvent_t *end);
 // B in rings of the longest traceback window.  Used by the single-read entry and, inside batches,
 // for reads whose references have degenerate ('X') positions.
 struct PlainSet;
-sa_status plain_create(const sa_read *reads, int64_t n_reads, const sa_params &p, size_t max_bytes, PlainSet **out);
+// segments: cut long regions into forward segments (alignment runs; not the expectations mode)
+sa_status plain_create(const sa_read *reads, int64_t n_reads, const sa_params &p, size_t max_bytes, PlainSet **out,
+                       bool segments = false);
+// scale of the set's stitch tolerance (negative: every stitch disagrees and its region re-runs whole)
+void plain_set_stitch_tolerance(PlainSet *s, double scale);
+// forward segments of the plain form in use: stitches and regions re-run whole at the last download
+void plain_segment_info(const PlainSet *s, int64_t *n_tasks, int64_t *n_stitches, int64_t *n_redone);
 sa_status plain_upload(PlainSet *s, cudaStream_t stream);
 sa_status plain_run(PlainSet *s, cudaStream_t stream);
 sa_status plain_download(PlainSet *s, cudaStream_t stream);

@@ -163,3 +163,40 @@ def test_segments_hdp_split_regions_and_wide_bands(api, policy):
             assert seg.status(i) == 0 and whole.status(i) == 0
             assert W.max_posterior_error(whole.pairs(i), seg.pairs(i), p.threshold) <= 1e-5
             assert abs(seg.log_likelihood(i) - whole.log_likelihood(i)) <= 1e-7 * abs(whole.log_likelihood(i))
+
+
+def test_plain_form_segments(api, policy):
+    """The plain FP64 form (the single-read entry and a batch's X reads) with forward segments: a
+    long read with degenerate X (C or E) sites, two paths over each, against the whole sweep (FP64
+    sweeps agree to rounding once the start is forgotten) and the oracle (1e-5); and a batch whose
+    plain-form stitches are all made to disagree re-runs those regions whole, with the whole
+    sweep's results exactly."""
+    from oracle import formats
+    cfg = synth.config3(seed=66, n_reads=1, span=(6000, 7000), grid_length=200, route="degenerate")
+    rd = [a for a in cfg["alignments"] if a["model"] == "gauss"][0]
+    m = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["gauss_table"]).split("\n")[:3])
+    sm = W.gpu_model(api, m, orc.EMIT_DESCALED, rd)
+    p = api.pairwiseAlignmentBandingParameters_construct(diagonal_expansion=50)
+    call = lambda: api.getAlignedPairsUsingAnchors(sm, rd["reference"], rd["events"], rd["anchors"], p,
+                                                   degenerate=api.CYTOSINE_METHYLATION2, with_log_likelihood=True)
+    api.set_segment_policy(4096, 1024)
+    seg, ll_seg = call()
+    api.set_segment_policy(-1, 1024)
+    whole, ll_whole = call()
+    assert len(whole) > 100
+    assert W.max_posterior_error(whole, seg, p.threshold) <= 1e-7
+    assert abs(ll_seg - ll_whole) <= 1e-9 * abs(ll_whole)
+    om = W.oracle_model(m, orc.EMIT_DESCALED, rd)
+    op = orc.params(threshold=p.threshold, expansion=p.diagonal_expansion)
+    want = orc.aligned_pairs(om, rd["reference"], rd["events"], rd["anchors"], op, True, True, options="CE")
+    assert W.max_posterior_error(want, seg, p.threshold) <= 1e-5
+    # the same read inside a batch (routed to the plain form), stitches forced to disagree
+    inp = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
+                         scale=rd["scale"], shift=rd["shift"], degenerate=api.CYTOSINE_METHYLATION2)]
+    forced = _run(api, inp, p, 4096, tol_scale=-1.0)
+    assert forced.status(0) == 0
+    assert np.array_equal(forced.pairs(0), whole)
+    assert forced.log_likelihood(0) == ll_whole
+    agreed = _run(api, inp, p, 4096)
+    assert W.max_posterior_error(whole, agreed.pairs(0), p.threshold) <= 1e-7
+    assert abs(agreed.log_likelihood(0) - ll_whole) <= 1e-9 * abs(ll_whole)
