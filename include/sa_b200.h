@@ -266,14 +266,16 @@ sa_status sa_batch_set_wait_limit(sa_batch *b, int64_t cycles);
 
 /* ---- forward segments (no counterpart in signalAlign, whose forward sweep runs once per region) ----
  * A region's forward sweep is sequential over its anti-diagonals, so the longest read of a batch
- * bounds the batch.  The batched form cuts it at traceback-window starts into segments that run at
- * the same time on different CTAs.  Each segment after the first sweeps max(warmup_diags, 10 x the
+ * bounds the batch.  Both forms (the batched FP32 form and the plain FP64 form behind
+ * sa_getAlignedPairsUsingAnchors and a batch's X reads; not the expectations calls) cut it at
+ * traceback-window starts into segments that run at the same time on different CTAs.  Each segment after the first sweeps max(warmup_diags, 10 x the
  * region's widest anti-diagonal) anti-diagonals before its own from a flat start; its values then
  * equal the true ones minus one constant (the recursion depends only on differences of log values,
  * and the start's influence dies out within a few band widths).  Where two segments meet, the kernel checks that on two
- * anti-diagonals (every cell within 2e-5 + 1e-6 x its distance below the anti-diagonal's maximum);
+ * anti-diagonals (FP32: every cell within 2e-5 + 1e-6 x its distance below the anti-diagonal's
+ * maximum; FP64: 1e-9 + 1e-11 x that distance);
  * posteriors do not depend on the constant, and the log-likelihood adds it back.  A read whose
- * check disagrees is re-run unsegmented in sa_batch_download, so results never depend on it.
+ * check disagrees is re-run unsegmented at download, so results never depend on it.
  * segment_diags: < 0 keeps every region whole; > 0 caps a segment's sweep (warm-up included);
  * 0 (default) picks twice the batch's forward anti-diagonals per worker CTA, at least 4096 (a large
  * batch, bound by its total work, then keeps nearly every region whole; a small one splits).
