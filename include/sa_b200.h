@@ -290,8 +290,9 @@ sa_status sa_getSegmentPolicy(int32_t *segment_diags, int32_t *warmup_diags);
 sa_status sa_planForwardSegments(const int64_t *anchors, int64_t n_anchors, int64_t lX, int64_t lY,
                                  const sa_params *p, int32_t segment_diags, int32_t warmup_diags, int64_t *out,
                                  int64_t capacity, int64_t *n_segments);
-/* segments and stitches of a batch; after a download, reads re-run unsegmented and the largest
- * deviation from the constant over the agreeing stitches */
+/* segments and stitches of a batch (both forms); after a download, reads (FP32 form) and regions
+ * (plain form) re-run unsegmented, and the largest deviation from the constant over the FP32 form's
+ * agreeing stitches */
 sa_status sa_batch_segment_info(const sa_batch *b, int64_t *n_segments, int64_t *n_stitches, int64_t *n_redone,
                                 double *max_spread);
 /* scale of the stitch tolerance for the batch's next runs (default 1; a negative scale makes every

@@ -1149,6 +1149,13 @@ sa_status sa_batch_segment_info(const sa_batch *b, int64_t *n_segments, int64_t 
     *n_segments = b->n_segs;
     *n_stitches = b->n_stitch;
     *n_redone = b->downloaded ? b->n_redone : 0;
+    if (b->plain) {   // the batch's reads in the plain FP64 form (regions re-run whole)
+        int64_t t = 0, st = 0, rd = 0;
+        plain_segment_info(b->plain, &t, &st, &rd);
+        *n_segments += t;
+        *n_stitches += st;
+        if (b->downloaded) *n_redone += rd;
+    }
     double m = 0.0;
     if (b->downloaded)
         for (int64_t q = 0; q < b->n_stitch; ++q)

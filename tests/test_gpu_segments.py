@@ -194,6 +194,8 @@ def test_plain_form_segments(api, policy):
     inp = [api.ReadInput(sm=sm, reference=rd["reference"], events=rd["events"], anchors=rd["anchors"],
                          scale=rd["scale"], shift=rd["shift"], degenerate=api.CYTOSINE_METHYLATION2)]
     forced = _run(api, inp, p, 4096, tol_scale=-1.0)
+    info = forced.segment_info()
+    assert info["stitches"] > 0 and info["redone"] == 1, info
     assert forced.status(0) == 0
     assert np.array_equal(forced.pairs(0), whole)
     assert forced.log_likelihood(0) == ll_whole
