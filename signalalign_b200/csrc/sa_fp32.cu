@@ -855,6 +855,17 @@ sa_status sa_batch_upload(sa_batch *b, void *stream) {
         std::memset(&m, 0, sizeof(m));
         m.kc = sm->dev.kc32;
         m.emission = sm->emission;
+        // a skip emission the same for every k-mer (log 0.1 for HDP machines and .model files)
+        // is passed as a value instead of loaded per column
+        if (sm->emission == SA_EMIT_HDP) {
+            m.gapx_uniform = 1;
+            m.gapx_value = (float) kLogPointOne;
+        } else {
+            bool uni = !sm->gapx.empty();
+            for (size_t q = 1; q < sm->gapx.size() && uni; ++q) uni = (float) sm->gapx[q] == (float) sm->gapx[0];
+            m.gapx_uniform = uni ? 1 : 0;
+            m.gapx_value = uni ? (float) sm->gapx[0] : 0.0f;
+        }
         for (int j = 0; j < 9; ++j) m.t[j] = (float) sm->t[j];
         if (sm->emission == SA_EMIT_HDP) {
             const HdpTables &h = sm->hdp;

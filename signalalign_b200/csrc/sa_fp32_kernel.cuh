@@ -79,9 +79,9 @@ struct ModelDesc {
     const KmerConst32 *kc;
     Hdp64 hdp64;
     int32_t emission;
-    int32_t pad;
+    int32_t gapx_uniform;   // every k-mer's skip emission is gapx_value (log 0.1 in .model machines)
     float t[9];
-    float pad2;
+    float gapx_value;
 };
 
 // per-read FP64 descaling parameters (HDP emissions)
@@ -410,6 +410,8 @@ struct Ctx {
     ReadScale32 rs;
     float t[9];
     bool hdp;
+    bool gx_uniform;   // the skip emission is gx for every column: no per-column load
+    float gx;
 };
 
 __device__ __forceinline__ void ctx_init(Ctx &c, const Args &A, int32_t region) {
@@ -419,6 +421,8 @@ __device__ __forceinline__ void ctx_init(Ctx &c, const Args &A, int32_t region) 
     c.M = A.models + c.R.model;
     c.rs = A.read_scale[c.R.read];
     c.hdp = c.M->emission == SA_EMIT_HDP;
+    c.gx_uniform = c.M->gapx_uniform != 0;
+    c.gx = c.M->gapx_value;
 #pragma unroll
     for (int i = 0; i < 9; ++i) c.t[i] = c.M->t[i];
 }
@@ -428,6 +432,7 @@ __device__ __forceinline__ int32_t clampi(int32_t v, int32_t lo, int32_t hi) { r
 // Raw loads: always from a valid address (indices clamped into the region's arrays); validity is
 // computed from indices alone and applied where the value is consumed.
 __device__ __forceinline__ float raw_gapx(const Ctx &c, int32_t x) {
+    if (c.gx_uniform) return c.gx;
     const int64_t at = c.R.lX > 0 ? c.R.kmer_base + clampi(x - 1, 0, c.R.lX - 1) : 0;
     return __ldg(c.A->gapx + at);
 }
