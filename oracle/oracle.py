@@ -68,8 +68,8 @@ def lib():
                                         C.c_void_p, C.c_int64, _i64p, _f64p, C.c_int64, _i64p]
         L.orc_flat_start_forgetting.restype = C.c_int
         L.orc_flat_start_forgetting.argtypes = [C.POINTER(_Model), C.c_char_p, C.c_int64, _f64p, C.c_int64, _i64p,
-                                                C.c_int64, C.c_int64, C.c_int, _i64p, C.c_int64, C.c_int64,
-                                                C.c_double, _i64p]
+                                                C.c_int64, C.c_int64, C.c_int, C.c_char_p, _i64p, C.c_int64,
+                                                C.c_int64, C.c_double, _i64p]
         L.orc_full_matrix.restype = C.c_int
         L.orc_full_matrix.argtypes = [C.POINTER(_Model), C.c_char_p, C.c_int64, _f64p, C.c_int64, C.c_double,
                                       C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_void_p, C.c_int64, _i64p,
@@ -283,7 +283,8 @@ def expand_kmer(kmer, options, max_paths=100000):
     return [raw[i * len(kmer):(i + 1) * len(kmer)].decode() for i in range(n)]
 
 
-def flat_start_forgetting(om, ref, events, anchors, starts, expansion=50, horizon=4000, tol=1e-9, ragged_left=True):
+def flat_start_forgetting(om, ref, events, anchors, starts, expansion=50, horizon=4000, tol=1e-9, ragged_left=True,
+                          options="CEO"):
     """orc_flat_start_forgetting: per start, the anti-diagonals after which a forward sweep begun
     there from a flat vector equals the true forward sweep minus one constant (within tol), or -1"""
     k = om.model["kmer_length"]
@@ -293,8 +294,8 @@ def flat_start_forgetting(om, ref, events, anchors, starts, expansion=50, horizo
     st = np.ascontiguousarray(np.asarray(starts, dtype=np.int64))
     out = np.zeros(len(st), np.int64)
     rc = lib().orc_flat_start_forgetting(C.byref(om.s), ref.encode(), lX, _p(ev, C.c_double), len(ev),
-                                         _p(a, C.c_int64), len(a), expansion, int(ragged_left), _p(st, C.c_int64),
-                                         len(st), horizon, tol, _p(out, C.c_int64))
+                                         _p(a, C.c_int64), len(a), expansion, int(ragged_left), options.encode(),
+                                         _p(st, C.c_int64), len(st), horizon, tol, _p(out, C.c_int64))
     if rc:
         raise OracleError("orc_flat_start_forgetting rc=%d" % rc)
     return out

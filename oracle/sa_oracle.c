@@ -958,15 +958,15 @@ int64_t orc_expand_kmer(const char *kmer, int k, const char *options, char *out,
  * anti-diagonal; -1 if that never holds. */
 int orc_flat_start_forgetting(const orc_model *m, const char *seq, int64_t lX, const double *events, int64_t lY,
                               const int64_t *anchors, int64_t n_anchors, int64_t expansion, int ragged_left,
-                              const int64_t *starts, int64_t n_starts, int64_t horizon, double tol,
-                              int64_t *steps_out) {
+                              const char *options, const int64_t *starts, int64_t n_starts, int64_t horizon,
+                              double tol, int64_t *steps_out) {
     int64_t n = lX + lY;
     int64_t *xl = (int64_t *) malloc((size_t) (n + 1) * sizeof(int64_t));
     int64_t *xr = (int64_t *) malloc((size_t) (n + 1) * sizeof(int64_t));
     orc_paths P; memset(&P, 0, sizeof(P));
     orc_dp dp; memset(&dp, 0, sizeof(dp));
     int rc = !xl || !xr ? ORC_E_NOMEM : orc_band(anchors, n_anchors, lX, lY, expansion, xl, xr);
-    if (!rc) rc = orc_paths_build(&P, seq, lX, m->kmer_length, "", 0, m);
+    if (!rc) rc = orc_paths_build(&P, seq, lX, m->kmer_length, options, (int) strlen(options), m);
     if (!rc) rc = orc_dp_init(&dp, m, &P, events, lY, xl, xr);
     if (rc) goto done;
     double s0[3];

@@ -110,3 +110,27 @@ def test_flat_start_forgets_within_the_warmup(api, expansion):
         assert (steps >= 0).all(), steps
         worst = max(worst, int(steps.max()) / warm)
     assert worst < 0.8, worst
+
+
+def test_flat_start_forgets_with_two_path_cells(api):
+    """The same with degenerate X (C or E) sites, whose cells hold two paths (the plain FP64 form's
+    forward segments): every path slot of the flat-start sweep becomes the true one minus the
+    constant within the warm-up."""
+    from oracle import formats
+    import workloads as W
+    cfg = synth.config3(seed=97, n_reads=2, span=(3000, 4000), grid_length=200, route="degenerate")
+    m = formats.parse_model_lines(*synth.model_text("ACEGT", 6, cfg["gauss_table"]).split("\n")[:3])
+    worst, sites = 0, 0
+    for rd in [a for a in cfg["alignments"] if a["model"] == "gauss"]:
+        sites += rd["reference"].count("X")
+        om = W.oracle_model(m, orc.EMIT_DESCALED, rd)
+        lX, lY = len(rd["reference"]) - 5, len(rd["events"])
+        _, maxw = window_starts(rd["anchors"], lX, lY)
+        warm = max(1024, 10 * maxw)
+        starts = list(range(warm + 2, lX + lY - warm, 2000))
+        steps = orc.flat_start_forgetting(om, rd["reference"], rd["events"], rd["anchors"], starts, 50,
+                                          horizon=warm + 500, tol=1e-9, options="CE")
+        assert (steps >= 0).all(), steps
+        worst = max(worst, int(steps.max()) / warm)
+    assert sites > 10
+    assert worst < 0.8, worst
